@@ -1,0 +1,231 @@
+// Fused PageRank: algorithms::simple_pagerank
+// (include/graphblas/algorithms/simple_pagerank.hpp:146-533) as ONE
+// persistent cooperative launch with one bounded grid barrier per iteration.
+//
+// Per iteration the reference pre-scales pr by alpha / outdegree (keeping
+// the dangling mass apart), runs vxm over L (a gather over L's CCS), adds the
+// teleport + dangling term and measures the L1 change.  Here the CCS gather
+// runs on merge-path tiles and its row epilogue does all of the rest for the
+// column it just finished: new pr_j, |new - old|, and already the pre-scaled
+// input of the NEXT iteration (pr_next, double-buffered) with its dangling
+// mass, so the next gather can start right after the barrier.
+#include "common.cuh"
+#include "merge.cuh"
+#include "persist.cuh"
+#include "spmv.cuh"
+
+#include <cmath>
+
+namespace alpb {
+
+using RF = RingPlusTimesF64;
+
+struct PrState {
+	GridSync gs;
+	int64_t iterations;
+	double residual;
+};
+
+struct PrArgs {
+	MergeTables mt;                // over the CCS
+	const int64_t *ccs_ptr;
+	const uint32_t *ccs_row;
+	const double *ccs_val;
+	const int64_t *crs_ptr;
+	const double *crs_val;
+	double *pr, *rs, *next0, *next1;
+	double *own_res, *span_res, *own_dang, *span_dang;  // [ntiles]
+	double *blk;                                        // [grid]
+	int64_t n, max_iter;
+	double alpha, conv;
+	int init_given;
+	PrState *st;
+};
+
+struct PrEpi {
+	const PrArgs *a;
+	double *next_out;
+	double d;
+	double acc_res = 0.0, acc_dang = 0.0;
+	__device__ __forceinline__ void terms(int64_t j, double v, bool has, double &res, double &dang) {
+		const double nn = has ? 0.0 + v : 0.0;       // pr_nextnext = 0; += pr_next L
+		const double old = __ldcg(a->pr + j);
+		const double nw = nn + d;                    // pr = pr_nextnext + dangling
+		a->pr[j] = nw;
+		res = old > nw ? old - nw : nw - old;
+		const double rsj = __ldg(a->rs + j);
+		if (rsj == 0.0) {                            // input of the next iteration
+			next_out[j] = 0.0;
+			dang = nw;
+		} else {
+			next_out[j] = nw * rsj;
+			dang = 0.0;
+		}
+	}
+	__device__ __forceinline__ void row(int64_t j, double v, bool has) {
+		double r, dg;
+		terms(j, v, has, r, dg);
+		acc_res += r;
+		acc_dang += dg;
+	}
+	__device__ __forceinline__ void row_span(int64_t first, int64_t j, double v, bool has) {
+		double r, dg;
+		terms(j, v, has, r, dg);
+		a->span_res[first] = r;
+		a->span_dang[first] = dg;
+	}
+};
+
+struct GatherL2 {
+	const double *x;
+	__device__ __forceinline__ double operator()(uint32_t j) const { return __ldcg(x + j); }
+};
+
+__global__ void __launch_bounds__(MP_BLOCK) k_pagerank(PrArgs a) {
+	__shared__ MergeSmem<RF> sm;
+	__shared__ double red[33];
+	PrState *st = a.st;
+	const int64_t G = gridDim.x, n = a.n, nt = a.mt.ntiles;
+	const int lane = threadIdx.x & 31;
+	// setup: out-degree counts of nonzero-valued entries (the pattern ring of
+	// :224-237), alpha / count (:281-289), initial guess, pre-scaled input
+	double dang = 0.0;
+	for (int64_t t = blockIdx.x; t < nt; t += G) {
+		a.span_res[t] = 0.0;
+		a.span_dang[t] = 0.0;
+	}
+	{
+		const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+		const int64_t nw = (G * blockDim.x) >> 5;
+		for (int64_t i = warp; i < n; i += nw) {
+			const int64_t b = a.crs_ptr[i], e = a.crs_ptr[i + 1];
+			double cnt = 0.0;
+			for (int64_t k = b + lane; k < e; k += 32)
+				cnt += (a.crs_val == nullptr || a.crs_val[k] != 0.0) ? 1.0 : 0.0;
+			for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+			if (lane == 0) {
+				const double rsi = cnt > 0.0 ? a.alpha / cnt : 0.0;
+				a.rs[i] = rsi;
+				const double p = a.init_given ? a.pr[i] : 1.0 / double(n);
+				a.pr[i] = p;
+				if (rsi == 0.0) {
+					a.next0[i] = 0.0;
+					dang += p;
+				} else {
+					a.next0[i] = p * rsi;
+				}
+			}
+		}
+	}
+	dang = block_sum(dang, red);
+	if (threadIdx.x == 0) a.blk[blockIdx.x] = dang;
+	if (!grid_sync(&st->gs)) return;
+	dang = block_sum_array(a.blk, G, red);
+
+	int64_t iter = 0;
+	double residual = 0.0;
+	double *cur = a.next0, *nxt = a.next1;
+	for (;;) {
+		const double d = (a.alpha * dang + 1 - a.alpha) / double(n);  // (:390)
+		PrEpi epi{&a, nxt, d};
+		GatherL2 xl{cur};
+		for (int64_t t = blockIdx.x; t < nt; t += G) {
+			epi.acc_res = epi.acc_dang = 0.0;
+			merge_tile<RF>(t, a.mt, a.ccs_ptr, a.ccs_row, a.ccs_val, xl, epi, 1, sm);
+			const double s1 = block_sum(epi.acc_res, red);
+			const double s2 = block_sum(epi.acc_dang, red);
+			if (threadIdx.x == 0) {
+				a.own_res[t] = s1;
+				a.own_dang[t] = s2;
+			}
+		}
+		if (!grid_sync(&st->gs)) return;
+		residual = block_sum_array(a.own_res, nt, red) + block_sum_array(a.span_res, nt, red);
+		dang = block_sum_array(a.own_dang, nt, red) + block_sum_array(a.span_dang, nt, red);
+		++iter;
+		if (a.conv != 0.0 && residual <= a.conv) break;   // (:490)
+		if (iter >= a.max_iter) break;
+		double *tmp = cur;
+		cur = nxt;
+		nxt = tmp;
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		st->iterations = iter;
+		st->residual = residual;
+	}
+}
+
+} // namespace alpb
+
+using namespace alpb;
+
+extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32_t *crs_col_idx,
+	const double *crs_values, const int64_t *ccs_col_ptr, const uint32_t *ccs_row_idx,
+	const double *ccs_values, double *pr, int init_given, double alpha, double conv,
+	int64_t max_iter, int64_t *iterations, double *residual, void *stream) {
+	(void) crs_col_idx;
+	ALPB_CHECK(alpha > 0 && alpha < 1, ALPB_ILLEGAL, "alpb_pagerank: alpha must be in (0, 1)");
+	ALPB_CHECK(max_iter > 0, ALPB_ILLEGAL, "alpb_pagerank: max must be positive");
+	ALPB_CHECK(iterations && residual, ALPB_ILLEGAL, "alpb_pagerank: null output");
+	ALPB_CHECK(n > 0, ALPB_ILLEGAL, "alpb_pagerank: empty graph");
+	cudaStream_t s = as_stream(stream);
+	int64_t nnz = 0;
+	ALPB_CUDA(cudaMemcpyAsync(&nnz, ccs_col_ptr + n, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	alpb_spmv_plan plan = nullptr;
+	int rc = alpb_spmv_plan_create(&plan, n, nnz, ccs_col_ptr, ALPB_SCHED_MERGE_PATH, 0, stream);
+	if (rc != ALPB_SUCCESS) return rc;
+	const int64_t nt = plan->ntiles;
+	int grid = cooperative_grid(k_pagerank, MP_BLOCK, 0, 0);
+	if (grid > 2 * sm_count()) grid = 2 * sm_count();
+	if (grid <= 0) {
+		alpb_spmv_plan_destroy(plan);
+		set_error("alpb_pagerank: no cooperative occupancy");
+		return ALPB_PANIC;
+	}
+	double *scratch = nullptr;
+	PrState *st = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&scratch, size_t(3 * n + 4 * nt + grid) * 8, s));
+	ALPB_CUDA(cudaMallocAsync(&st, sizeof(PrState), s));
+	ALPB_CUDA(cudaMemsetAsync(st, 0, sizeof(PrState), s));
+	PrArgs a;
+	a.mt = merge_tables(*plan);
+	a.ccs_ptr = ccs_col_ptr;
+	a.ccs_row = ccs_row_idx;
+	a.ccs_val = ccs_values;
+	a.crs_ptr = crs_row_ptr;
+	a.crs_val = crs_values;
+	a.pr = pr;
+	a.rs = scratch;
+	a.next0 = scratch + n;
+	a.next1 = scratch + 2 * n;
+	a.own_res = scratch + 3 * n;
+	a.span_res = a.own_res + nt;
+	a.own_dang = a.span_res + nt;
+	a.span_dang = a.own_dang + nt;
+	a.blk = a.span_dang + nt;
+	a.n = n;
+	a.max_iter = max_iter;
+	a.alpha = alpha;
+	a.conv = conv;
+	a.init_given = init_given;
+	a.st = st;
+	void *args[] = {&a};
+	ALPB_CUDA(cudaLaunchCooperativeKernel((void *) k_pagerank, dim3(grid), dim3(MP_BLOCK), args, 0, s));
+	ALPB_LAUNCHED();
+	PrState h;
+	ALPB_CUDA(cudaMemcpyAsync(&h, st, sizeof(PrState), cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaFreeAsync(scratch, s));
+	ALPB_CUDA(cudaFreeAsync(st, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	alpb_spmv_plan_destroy(plan);
+	ALPB_CHECK(h.gs.err == 0, ALPB_PANIC, "alpb_pagerank: grid barrier timed out");
+	*iterations = h.iterations;
+	*residual = h.residual;
+	if (!(h.residual <= conv)) {
+		set_error("alpb_pagerank: not converged after %lld iterations (residual %g)",
+			(long long) h.iterations, h.residual);
+		return ALPB_FAILED;
+	}
+	return ALPB_SUCCESS;
+}

@@ -1,0 +1,86 @@
+// Persistent (cooperative) kernel support: a grid barrier whose every wait is
+// bounded, and a deterministic block reduction.
+#pragma once
+#include "common.cuh"
+
+namespace alpb {
+
+// Barrier state in device memory; zero-initialise before the launch.
+struct GridSync {
+	unsigned int count;
+	unsigned int gen;
+	int err;    // 1: a barrier wait gave up (the kernel exits; host reports PANIC)
+	int pad;
+};
+
+// ~1 s at the sleep granularity below: far beyond any legitimate wait of a
+// co-resident grid, short enough to keep the context usable on a fault.
+constexpr long long kSpinLimit = 1ll << 24;
+
+// All blocks of a cooperative launch call this the same number of times.
+// Returns false once any block has timed out; callers then leave their loop.
+__device__ __forceinline__ bool grid_sync(GridSync *gs) {
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		volatile unsigned int *vgen = &gs->gen;
+		volatile int *verr = &gs->err;
+		const unsigned int g = *vgen;
+		__threadfence();
+		const unsigned int arrived = atomicAdd(&gs->count, 1u);
+		if (arrived == gridDim.x - 1) {
+			gs->count = 0;
+			__threadfence();
+			atomicExch(&gs->gen, g + 1);
+		} else {
+			long long spins = 0;
+			while (*vgen == g && *verr == 0) {
+				if (++spins > kSpinLimit) {
+					atomicExch(&gs->err, 1);
+					break;
+				}
+				__nanosleep(64);
+			}
+		}
+		__threadfence();
+	}
+	__syncthreads();
+	return *((volatile int *) &gs->err) == 0;
+}
+
+// Sum over the block in a fixed order (warp trees, then warp 0 over the warp
+// sums); the result is returned to every thread.
+__device__ __forceinline__ double block_sum(double v, double *smem /* >= 33 */) {
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+	__syncthreads();
+	if (lane == 0) smem[wid] = v;
+	__syncthreads();
+	if (wid == 0) {
+		const int nw = (blockDim.x + 31) >> 5;
+		double w = lane < nw ? smem[lane] : 0.0;
+		for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+		if (lane == 0) smem[32] = w;
+	}
+	__syncthreads();
+	return smem[32];
+}
+
+// Every block sums the same array in the same order (same value everywhere).
+__device__ __forceinline__ double block_sum_array(const double *a, int64_t n, double *smem) {
+	double v = 0.0;
+	for (int64_t k = threadIdx.x; k < n; k += blockDim.x) v += ((const volatile double *) a)[k];
+	return block_sum(v, smem);
+}
+
+// Largest grid of `kernel` whose blocks are all co-resident.
+template <class K>
+int cooperative_grid(K kernel, int block, size_t smem, int64_t want) {
+	int per_sm = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess)
+		return 0;
+	int64_t g = int64_t(per_sm) * sm_count();
+	if (want > 0 && want < g) g = want;
+	return int(g);
+}
+
+} // namespace alpb

@@ -1,0 +1,633 @@
+// Sparse matrix times dense/sparse vector over a semiring: the replacement of
+// internal::vxm_generic + vxm_inner_kernel_gather
+// (include/graphblas/reference/blas2.hpp:283-551, 835-1528).
+//
+// Two schedules gather over a compressed storage whose outer dimension is the
+// output (CRS for mxv, CCS for vxm, as the reference does):
+//
+//  * merge path (dense fast path, merge.cuh): the (rows + nonzeroes) merge
+//    list is cut in equal tiles (Merrill & Garland, "Merge-based parallel
+//    sparse matrix-vector multiplication", SC'16), so power-law rows cost the
+//    same as uniform ones; one launch, sums in a fixed order (deterministic).
+//  * vector (general path): W lanes per row, lane-strided loads and a
+//    warp-shuffle tree; carries every ALP semantic of the reference gather:
+//    output/input masks (value or structural, inverted), sparse input and
+//    output vectors with assigned flags, add_identity, use_index,
+//    explicit_zero and the immutable-nonzero shortcut of lor.
+#include "common.cuh"
+#include "spmv.cuh"
+#include "merge.cuh"
+
+#include <algorithm>
+
+namespace alpb {
+
+// ------------------------------------------------------------ plan layout --
+// merge-path split of diagonal d: rows consumed i, nonzeroes consumed d - i
+__device__ __forceinline__ int64_t merge_search_global(const int64_t *offsets, int64_t m,
+	int64_t nnz, int64_t d) {
+	int64_t lo = d - nnz > 0 ? d - nnz : 0;
+	int64_t hi = d < m ? d : m;
+	while (lo < hi) {
+		const int64_t pivot = (lo + hi) >> 1;
+		// row end of row `pivot` is offsets[pivot + 1]
+		if (offsets[pivot + 1] <= d - pivot - 1) lo = pivot + 1; else hi = pivot;
+	}
+	return lo;
+}
+
+__global__ void k_merge_tiles(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
+	int64_t *tile_row) {
+	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t <= ntiles;
+		 t += int64_t(gridDim.x) * blockDim.x) {
+		int64_t d = t * MP_TILE;
+		if (d > m + nnz) d = m + nnz;
+		tile_row[t] = merge_search_global(offsets, m, nnz, d);
+	}
+}
+
+__global__ void k_row_stats(const int64_t *offsets, int64_t m, unsigned long long *maxlen,
+	double *sumsq) {
+	int64_t lmax = 0;
+	double lsq = 0.0;
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m;
+		 i += int64_t(gridDim.x) * blockDim.x) {
+		const int64_t len = offsets[i + 1] - offsets[i];
+		lmax = len > lmax ? len : lmax;
+		lsq += double(len) * double(len);
+	}
+	for (int o = 16; o > 0; o >>= 1) {
+		const int64_t om = __shfl_down_sync(0xffffffffu, lmax, o);
+		lmax = om > lmax ? om : lmax;
+		lsq += __shfl_down_sync(0xffffffffu, lsq, o);
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicMax(maxlen, (unsigned long long) lmax);
+		atomicAdd(sumsq, lsq);
+	}
+}
+
+// Spanning-row tables of the merge path (see merge.cuh): for each tile, the
+// first tile of its head / tail row when that row crosses tiles, and for the
+// first tile of a spanning row the number of tiles it covers.
+__global__ void k_merge_tables(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
+	const int64_t *tile_row, int64_t *head_first, int64_t *tail_first, int32_t *span_len) {
+	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < ntiles;
+		 t += int64_t(gridDim.x) * blockDim.x) {
+		const int64_t i0 = tile_row[t], i1 = tile_row[t + 1];
+		const int64_t d0 = t * MP_TILE;
+		int64_t d1 = d0 + MP_TILE;
+		if (d1 > m + nnz) d1 = m + nnz;
+		const int64_t j0 = d0 - i0, j1 = d1 - i1;
+		head_first[t] = (i1 > i0 && offsets[i0] < j0) ? (i0 + offsets[i0]) / MP_TILE : -1;
+		int64_t tf = -1;
+		if (i1 < m) {
+			const int64_t start = offsets[i1] > j0 ? offsets[i1] : j0;
+			if (j1 > start) tf = (i1 + offsets[i1]) / MP_TILE;
+		}
+		tail_first[t] = tf;
+		span_len[t] = (tf == t) ? int32_t((i1 + offsets[i1 + 1]) / MP_TILE - t + 1) : 0;
+	}
+}
+
+MergeTables merge_tables(const alpb_spmv_plan_s &p) {
+	MergeTables t;
+	t.m = p.m;
+	t.nnz = p.nnz;
+	t.ntiles = p.ntiles;
+	t.tile_row = p.tile_row;
+	t.head_first = p.head_first;
+	t.tail_first = p.tail_first;
+	t.span_len = p.span_len;
+	t.counter = p.counter;
+	t.head_val = p.head_val;
+	t.tail_val = p.tail_val;
+	t.head_has = p.head_has;
+	t.tail_has = p.tail_has;
+	return t;
+}
+
+// ------------------------------------------------------- merge-path SpMV --
+template <class R>
+struct AccumulateY {
+	typename R::T *__restrict__ y;
+	__device__ __forceinline__ void row(int64_t r, typename R::T v, bool has) {
+		if (has) y[r] = R::add(y[r], v);  // foldl( y_r, row sum ), blas2.hpp:534-549
+	}
+	__device__ __forceinline__ void row_span(int64_t, int64_t r, typename R::T v, bool has) {
+		row(r, v, has);
+	}
+};
+
+template <class R>
+__global__ void __launch_bounds__(MP_BLOCK)
+k_spmv_merge(MergeTables mt, const int64_t *__restrict__ offsets,
+	const uint32_t *__restrict__ indices, const typename R::T *__restrict__ values,
+	const typename R::T *__restrict__ x, typename R::T *__restrict__ y, int left) {
+	__shared__ MergeSmem<R> sm;
+	PlainX<typename R::T> xl{x};
+	AccumulateY<R> epi{y};
+	for (int64_t t = blockIdx.x; t < mt.ntiles; t += gridDim.x)
+		merge_tile<R>(t, mt, offsets, indices, values, xl, epi, left, sm);
+}
+
+// ------------------------------------------------------ vector schedules --
+// Rows are handed out per warp (32/W rows at a time) so that every lane of a
+// warp runs the same number of outer iterations and the width-W shuffles
+// below always see the full warp.
+template <class R, int W>
+__global__ void __launch_bounds__(256)
+k_spmv_vector_dense(const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
+	const typename R::T *__restrict__ values, const typename R::T *__restrict__ x,
+	typename R::T *__restrict__ y, int64_t m, int left) {
+	using T = typename R::T;
+	constexpr int RPW = 32 / W;  // rows per warp step
+	const int lane = threadIdx.x & (W - 1);
+	const int sub = (threadIdx.x & 31) / W;
+	const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+	const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	for (int64_t base = warp * RPW; base < m; base += nwarps * RPW) {
+		const int64_t i = base + sub;
+		T acc = R::zero();
+		int64_t b = 0, e = 0;
+		if (i < m) {
+			b = offsets[i];
+			e = offsets[i + 1];
+			for (int64_t k = b + lane; k < e; k += W) {
+				const T a = values ? __ldcs(values + k) : R::one();
+				const T xv = __ldg(x + __ldcs(indices + k));
+				acc = R::add(acc, left ? R::mull(xv, a) : R::mulr(a, xv));
+			}
+		}
+#pragma unroll
+		for (int o = W / 2; o > 0; o >>= 1) acc = R::add(acc, __shfl_down_sync(0xffffffffu, acc, o, W));
+		if (i < m && lane == 0 && e > b) y[i] = R::add(y[i], acc);
+	}
+}
+
+// General path, all ALP semantics; see the file comment.
+template <class R, int W>
+__global__ void __launch_bounds__(256)
+k_spmv_vector_general(SpmvArgs a) {
+	using T = typename R::T;
+	constexpr int RPW = 32 / W;
+	const T *__restrict__ values = reinterpret_cast<const T *>(a.values);
+	const T *__restrict__ x = reinterpret_cast<const T *>(a.v);
+	T *__restrict__ y = reinterpret_cast<T *>(a.u);
+	const bool dense_hint = (a.descr & ALPB_DESC_DENSE) != 0;
+	const bool add_identity = (a.descr & ALPB_DESC_ADD_IDENTITY) != 0;
+	const bool use_index = (a.descr & ALPB_DESC_USE_INDEX) != 0;
+	const bool explicit_zero = (a.descr & ALPB_DESC_EXPLICIT_ZERO) != 0;
+	const int lane = threadIdx.x & (W - 1);
+	const int sub = (threadIdx.x & 31) / W;
+	const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+	const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	int64_t newly = 0;
+	for (int64_t base = warp * RPW; base < a.m_out; base += nwarps * RPW) {
+		const int64_t i = base + sub;
+		const bool in_range = i < a.m_out;
+		bool row_ok = in_range;
+		if (row_ok && a.masked)
+			row_ok = a.mask_by_structure
+				? (a.u_mask_assigned == nullptr || a.u_mask_assigned[i] != 0)
+				: eval_mask(a.u_mask, a.u_mask_assigned, a.u_mask_type, a.descr, i);
+		const bool id_row = in_range && add_identity && (a.scatter_sem || row_ok);
+		const bool u_has = in_range && (a.u_assigned == nullptr || a.u_assigned[i] != 0);
+		// immutable-nonzero shortcut of the gather (blas2.hpp:351-357)
+		if (R::immutable && !a.scatter_sem && row_ok && u_has && y[i] != R::zero()) row_ok = false;
+		const bool active = row_ok || id_row;
+		T acc = R::zero();
+		bool set = false;
+		if (active) {
+			if (id_row && lane == 0 && i < a.n_in) {
+				const bool vm_ok = !a.input_masked ||
+					eval_mask(a.v_mask, a.v_mask_assigned, a.v_mask_type, a.descr, i);
+				if (vm_ok && (dense_hint || a.v_assigned == nullptr || a.v_assigned[i])) {
+					acc = a.left ? R::mull(x[i], R::one()) : R::mulr(R::one(), x[i]);
+					set = true;
+				}
+			}
+			const int64_t b = row_ok ? a.offsets[i] : 0, e = row_ok ? a.offsets[i + 1] : 0;
+			for (int64_t k = b + lane; k < e; k += W) {
+				const uint32_t j = a.indices[k];
+				if (a.input_masked &&
+					!eval_mask(a.v_mask, a.v_mask_assigned, a.v_mask_type, a.descr, j))
+					continue;
+				if (!dense_hint && a.v_assigned != nullptr && !a.v_assigned[j]) continue;
+				const T av = values ? values[k] : R::one();
+				const T xv = use_index ? T(j) : x[j];
+				acc = R::add(a.left ? R::mull(xv, av) : R::mulr(av, xv), acc);
+				set = true;
+				if (R::immutable && acc != R::zero()) break;
+			}
+		}
+#pragma unroll
+		for (int o = W / 2; o > 0; o >>= 1) {
+			acc = R::add(acc, __shfl_down_sync(0xffffffffu, acc, o, W));
+			set = set | (__shfl_down_sync(0xffffffffu, int(set), o, W) != 0);
+		}
+		const bool ez = explicit_zero && !a.scatter_sem && row_ok;
+		if (active && lane == 0 && (ez || set)) {
+			if (u_has || dense_hint) {
+				y[i] = R::add(y[i], acc);
+			} else {
+				y[i] = acc;
+			}
+			if (!u_has && a.u_assigned) {
+				a.u_assigned[i] = 1;
+				++newly;
+			}
+		}
+	}
+	if (a.u_nnz) {
+		// warp-aggregated count of newly assigned entries
+		for (int o = 16; o > 0; o >>= 1) newly += __shfl_down_sync(0xffffffffu, newly, o);
+		if ((threadIdx.x & 31) == 0 && newly) atomicAdd((unsigned long long *) a.u_nnz,
+			(unsigned long long) newly);
+	}
+}
+
+// Trivial case of blas2.hpp:1001-1037: the output keeps its values; with
+// explicit_zero every unassigned entry becomes the additive identity.
+template <class R>
+__global__ void k_spmv_trivial(SpmvArgs a) {
+	using T = typename R::T;
+	T *y = reinterpret_cast<T *>(a.u);
+	int64_t newly = 0;
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < a.m_out;
+		 i += int64_t(gridDim.x) * blockDim.x) {
+		if (a.u_assigned && !a.u_assigned[i]) {
+			y[i] = R::zero();
+			a.u_assigned[i] = 1;
+			++newly;
+		}
+	}
+	if (a.u_nnz) {
+		for (int o = 16; o > 0; o >>= 1) newly += __shfl_down_sync(0xffffffffu, newly, o);
+		if ((threadIdx.x & 31) == 0 && newly) atomicAdd((unsigned long long *) a.u_nnz,
+			(unsigned long long) newly);
+	}
+}
+
+// --------------------------------------------------------------- drivers --
+template <class R>
+int launch_merge(const SpmvArgs &a, const alpb_spmv_plan_s &p, cudaStream_t s) {
+	using T = typename R::T;
+	if (p.ntiles == 0) return ALPB_SUCCESS;
+	k_spmv_merge<R><<<unsigned(p.ntiles), MP_BLOCK, 0, s>>>(merge_tables(p), a.offsets, a.indices,
+		reinterpret_cast<const T *>(a.values), reinterpret_cast<const T *>(a.v),
+		reinterpret_cast<T *>(a.u), a.left);
+	ALPB_LAUNCHED();
+	return ALPB_SUCCESS;
+}
+
+template <class R, int W>
+int launch_vector_dense_w(const SpmvArgs &a, cudaStream_t s) {
+	using T = typename R::T;
+	const int64_t threads = a.m_out * W;
+	k_spmv_vector_dense<R, W><<<grid_for(threads, 256, 8), 256, 0, s>>>(a.offsets, a.indices,
+		reinterpret_cast<const T *>(a.values), reinterpret_cast<const T *>(a.v),
+		reinterpret_cast<T *>(a.u), a.m_out, a.left);
+	ALPB_LAUNCHED();
+	return ALPB_SUCCESS;
+}
+
+template <class R, int W>
+int launch_vector_general_w(const SpmvArgs &a, cudaStream_t s) {
+	const int64_t threads = a.m_out * W;
+	k_spmv_vector_general<R, W><<<grid_for(threads, 256, 8), 256, 0, s>>>(a);
+	ALPB_LAUNCHED();
+	return ALPB_SUCCESS;
+}
+
+template <class R>
+int launch_vector(const SpmvArgs &a, int W, bool dense, cudaStream_t s) {
+	if (dense) {
+		switch (W) {
+		case 1: return launch_vector_dense_w<R, 1>(a, s);
+		case 2: return launch_vector_dense_w<R, 2>(a, s);
+		case 4: return launch_vector_dense_w<R, 4>(a, s);
+		case 8: return launch_vector_dense_w<R, 8>(a, s);
+		case 16: return launch_vector_dense_w<R, 16>(a, s);
+		default: return launch_vector_dense_w<R, 32>(a, s);
+		}
+	}
+	switch (W) {
+	case 1: return launch_vector_general_w<R, 1>(a, s);
+	case 2: return launch_vector_general_w<R, 2>(a, s);
+	case 4: return launch_vector_general_w<R, 4>(a, s);
+	case 8: return launch_vector_general_w<R, 8>(a, s);
+	case 16: return launch_vector_general_w<R, 16>(a, s);
+	default: return launch_vector_general_w<R, 32>(a, s);
+	}
+}
+
+static int default_width(double mean) {
+	int w = 1;
+	while (w < 32 && w * 2 <= mean * 0.75 + 1) w *= 2;
+	return w;
+}
+
+template <class R>
+int run_spmv(const SpmvArgs &a, const alpb_spmv_plan_s *p, int force_sched, cudaStream_t s) {
+	if (a.trivial) {
+		if (a.descr & ALPB_DESC_EXPLICIT_ZERO) {
+			k_spmv_trivial<R><<<grid_for(a.m_out, 256), 256, 0, s>>>(a);
+			ALPB_LAUNCHED();
+		}
+		return ALPB_SUCCESS;
+	}
+	const bool fast = a.dense_all && !a.masked && !a.input_masked &&
+		!(a.descr & (ALPB_DESC_ADD_IDENTITY | ALPB_DESC_USE_INDEX));
+	int sched = force_sched ? force_sched : (p ? p->sched : ALPB_SCHED_VECTOR);
+	int W = p ? p->vw : default_width(a.m_out ? double(a.nnz) / double(a.m_out) : 1.0);
+	if (fast && sched == ALPB_SCHED_MERGE_PATH && p && p->tile_row)
+		return launch_merge<R>(a, *p, s);
+	return launch_vector<R>(a, W, fast, s);
+}
+
+int dispatch_spmv(int ring, const SpmvArgs &a, const alpb_spmv_plan_s *p, int force_sched,
+	cudaStream_t s) {
+	switch (ring) {
+	case ALPB_RING_PLUS_TIMES_F64: return run_spmv<RingPlusTimesF64>(a, p, force_sched, s);
+	case ALPB_RING_LOR_LAND_BOOL: return run_spmv<RingLorLandBool>(a, p, force_sched, s);
+	case ALPB_RING_MIN_PLUS_I32: return run_spmv<RingMinPlusI32>(a, p, force_sched, s);
+	case ALPB_RING_PLUS_PATTERN_F64: return run_spmv<RingPlusPatternF64>(a, p, force_sched, s);
+	case ALPB_RING_PLUS_TIMES_I32: return run_spmv<RingPlusTimesI32>(a, p, force_sched, s);
+	}
+	set_error("alpb_mxv: semiring %d is not instantiated on the device", ring);
+	return ALPB_UNSUPPORTED;
+}
+
+int ring_value_type(int ring) {
+	switch (ring) {
+	case ALPB_RING_PLUS_TIMES_F64: return ALPB_FP64;
+	case ALPB_RING_LOR_LAND_BOOL: return ALPB_BOOL;
+	case ALPB_RING_MIN_PLUS_I32: return ALPB_INT32;
+	case ALPB_RING_PLUS_PATTERN_F64: return ALPB_FP64;
+	case ALPB_RING_PLUS_TIMES_I32: return ALPB_INT32;
+	}
+	return -1;
+}
+
+int plan_build(alpb_spmv_plan_s *p, const int64_t *offsets, cudaStream_t s) {
+	// row-length profile
+	unsigned long long *d_max = nullptr;
+	double *d_sq = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&d_max, 8, s));
+	ALPB_CUDA(cudaMallocAsync(&d_sq, 8, s));
+	ALPB_CUDA(cudaMemsetAsync(d_max, 0, 8, s));
+	ALPB_CUDA(cudaMemsetAsync(d_sq, 0, 8, s));
+	if (p->m > 0) {
+		k_row_stats<<<grid_for(p->m, 256, 4), 256, 0, s>>>(offsets, p->m, d_max, d_sq);
+		ALPB_LAUNCHED();
+	}
+	unsigned long long hmax = 0;
+	double hsq = 0;
+	ALPB_CUDA(cudaMemcpyAsync(&hmax, d_max, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaMemcpyAsync(&hsq, d_sq, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaFreeAsync(d_max, s));
+	ALPB_CUDA(cudaFreeAsync(d_sq, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	p->maxlen = double(hmax);
+	p->mean = p->m ? double(p->nnz) / double(p->m) : 0.0;
+	const double var = p->m ? hsq / double(p->m) - p->mean * p->mean : 0.0;
+	p->cv = p->mean > 0 ? sqrt(var > 0 ? var : 0.0) / p->mean : 0.0;
+	// merge-path tile table
+	p->ntiles = (p->m + p->nnz + MP_TILE - 1) / MP_TILE;
+	if (p->ntiles > 0) {
+		ALPB_CHECK(p->nnz + MP_TILE < (int64_t(1) << 31), ALPB_OVERFLW,
+			"alpb_spmv_plan_create: merge path tiles use 32-bit offsets (nnz %lld)",
+			(long long) p->nnz);
+		const size_t nt = size_t(p->ntiles);
+		ALPB_CUDA(cudaMalloc(&p->tile_row, (nt + 1) * 8));
+		ALPB_CUDA(cudaMalloc(&p->head_first, nt * 8));
+		ALPB_CUDA(cudaMalloc(&p->tail_first, nt * 8));
+		ALPB_CUDA(cudaMalloc(&p->span_len, nt * 4));
+		ALPB_CUDA(cudaMalloc(&p->counter, nt * 4));
+		ALPB_CUDA(cudaMalloc(&p->head_val, nt * 8));
+		ALPB_CUDA(cudaMalloc(&p->tail_val, nt * 8));
+		ALPB_CUDA(cudaMalloc(&p->head_has, nt));
+		ALPB_CUDA(cudaMalloc(&p->tail_has, nt));
+		ALPB_CUDA(cudaMemsetAsync(p->counter, 0, nt * 4, s));
+		k_merge_tiles<<<grid_for(p->ntiles + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz,
+			p->ntiles, p->tile_row);
+		ALPB_LAUNCHED();
+		k_merge_tables<<<grid_for(p->ntiles, 256), 256, 0, s>>>(offsets, p->m, p->nnz, p->ntiles,
+			p->tile_row, p->head_first, p->tail_first, p->span_len);
+		ALPB_LAUNCHED();
+	}
+	return ALPB_SUCCESS;
+}
+
+} // namespace alpb
+
+using namespace alpb;
+
+extern "C" {
+
+int alpb_spmv_plan_create(alpb_spmv_plan *plan, int64_t m, int64_t nnz, const int64_t *offsets,
+	int sched, int vector_width, void *stream) {
+	ALPB_CHECK(plan != nullptr, ALPB_ILLEGAL, "alpb_spmv_plan_create: null plan");
+	*plan = nullptr;
+	ALPB_CHECK(m >= 0 && nnz >= 0, ALPB_ILLEGAL, "alpb_spmv_plan_create: negative size");
+	ALPB_CHECK(sched >= ALPB_SCHED_AUTO && sched <= ALPB_SCHED_VECTOR, ALPB_ILLEGAL,
+		"alpb_spmv_plan_create: schedule %d", sched);
+	auto *p = new alpb_spmv_plan_s();
+	p->m = m;
+	p->nnz = nnz;
+	p->offsets = offsets;
+	cudaGetDevice(&p->device);
+	int rc = plan_build(p, offsets, as_stream(stream));
+	if (rc != ALPB_SUCCESS) {
+		alpb_spmv_plan_destroy(p);
+		return rc;
+	}
+	if (vector_width > 0) {
+		int w = 1;
+		while (w < vector_width && w < 32) w *= 2;
+		p->vw = w;
+	} else {
+		p->vw = default_width(p->mean);
+	}
+	if (sched == ALPB_SCHED_AUTO) {
+		// profile heuristic: regular rows -> vector, skewed rows -> merge path
+		sched = (p->cv < 0.5 && p->maxlen <= 4.0 * p->mean + 32) ? ALPB_SCHED_VECTOR
+																	 : ALPB_SCHED_MERGE_PATH;
+	}
+	p->sched = sched;
+	*plan = p;
+	return ALPB_SUCCESS;
+}
+
+int alpb_spmv_plan_destroy(alpb_spmv_plan p) {
+	if (!p) return ALPB_SUCCESS;
+	cudaFree(p->tile_row);
+	cudaFree(p->head_first);
+	cudaFree(p->tail_first);
+	cudaFree(p->span_len);
+	cudaFree(p->counter);
+	cudaFree(p->head_val);
+	cudaFree(p->tail_val);
+	cudaFree(p->head_has);
+	cudaFree(p->tail_has);
+	delete p;
+	return ALPB_SUCCESS;
+}
+
+int alpb_spmv_plan_info(alpb_spmv_plan p, int *sched, int *vw, int64_t *tiles) {
+	ALPB_CHECK(p != nullptr, ALPB_ILLEGAL, "alpb_spmv_plan_info: null plan");
+	if (sched) *sched = p->sched;
+	if (vw) *vw = p->vw;
+	if (tiles) *tiles = p->ntiles;
+	return ALPB_SUCCESS;
+}
+
+int alpb_spmv_autotune(alpb_spmv_plan p, int ring, int64_t n, const uint32_t *indices,
+	const void *values, int value_type, const void *x, void *y_scratch, void *stream) {
+	ALPB_CHECK(p != nullptr, ALPB_ILLEGAL, "alpb_spmv_autotune: null plan");
+	ALPB_CHECK(value_type == ALPB_VOID || value_type == ring_value_type(ring), ALPB_UNSUPPORTED,
+		"alpb_spmv_autotune: value type %d with ring %d", value_type, ring);
+	cudaStream_t s = as_stream(stream);
+	SpmvArgs a{};
+	a.m_out = p->m;
+	a.n_in = n;
+	a.nnz = p->nnz;
+	a.offsets = nullptr;
+	a.indices = indices;
+	a.values = value_type == ALPB_VOID ? nullptr : values;
+	a.v = x;
+	a.u = y_scratch;
+	a.dense_all = true;
+	cudaEvent_t e0, e1;
+	ALPB_CUDA(cudaEventCreate(&e0));
+	ALPB_CUDA(cudaEventCreate(&e1));
+	// candidates: merge path, and vector widths around the mean row length
+	struct Cand { int sched, w; } cands[8];
+	int nc = 0;
+	cands[nc++] = {ALPB_SCHED_MERGE_PATH, p->vw};
+	for (int w = 2; w <= 32; w *= 2) cands[nc++] = {ALPB_SCHED_VECTOR, w};
+	float best = 1e30f;
+	int best_i = 0;
+	const int saved_vw = p->vw;
+	a.offsets = p->offsets;
+	for (int c = 0; c < nc; ++c) {
+		p->vw = cands[c].w;
+		float total = 0;
+		for (int rep = 0; rep < 4; ++rep) {
+			ALPB_CUDA(cudaEventRecord(e0, s));
+			int rc = dispatch_spmv(ring, a, p, cands[c].sched, s);
+			if (rc != ALPB_SUCCESS) { p->vw = saved_vw; return rc; }
+			ALPB_CUDA(cudaEventRecord(e1, s));
+			ALPB_CUDA(cudaEventSynchronize(e1));
+			float ms = 0;
+			ALPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+			if (rep > 0) total += ms;  // first run warms caches
+		}
+		if (total < best) { best = total; best_i = c; }
+	}
+	ALPB_CUDA(cudaEventDestroy(e0));
+	ALPB_CUDA(cudaEventDestroy(e1));
+	p->sched = cands[best_i].sched;
+	p->vw = cands[best_i].sched == ALPB_SCHED_VECTOR ? cands[best_i].w : saved_vw;
+	p->tuned_ms = best / 3.0f;
+	return ALPB_SUCCESS;
+}
+
+int alpb_mxv(int ring, uint32_t descr, int form, int64_t m_out, int64_t n_in, int64_t nnz,
+	const int64_t *offsets, const uint32_t *indices, const void *values, int value_type,
+	void *u, uint8_t *u_assigned, int64_t *u_nnz,
+	const void *u_mask, const uint8_t *u_mask_assigned, int u_mask_type, int64_t u_mask_count,
+	const void *v, const uint8_t *v_assigned, int64_t v_count,
+	const void *v_mask, const uint8_t *v_mask_assigned, int v_mask_type, int64_t v_mask_count,
+	alpb_spmv_plan plan, void *stream) {
+	ALPB_CHECK(ring_value_type(ring) >= 0, ALPB_UNSUPPORTED,
+		"alpb_mxv: semiring %d is not instantiated on the device", ring);
+	ALPB_CHECK(value_type == ALPB_VOID || value_type == ring_value_type(ring), ALPB_UNSUPPORTED,
+		"alpb_mxv: matrix value type %d does not match semiring %d", value_type, ring);
+	ALPB_CHECK(m_out >= 0 && n_in >= 0 && nnz >= 0, ALPB_ILLEGAL, "alpb_mxv: negative size");
+	ALPB_CHECK(descr <= 16383u, ALPB_ILLEGAL, "alpb_mxv: descriptor out of range");
+	ALPB_CHECK(!(descr & ALPB_DESC_TRANSPOSE_MATRIX), ALPB_ILLEGAL,
+		"alpb_mxv: transpose_matrix must be resolved by the caller (storage + handedness)");
+	const bool masked = u_mask_count >= 0;
+	const bool input_masked = v_mask_count >= 0;
+	const bool dense_hint = (descr & ALPB_DESC_DENSE) != 0;
+	// dense descriptor on a sparse container is ILLEGAL (blas2.hpp:950-971)
+	if (dense_hint) {
+		ALPB_CHECK(v_count == n_in, ALPB_ILLEGAL,
+			"alpb_mxv: dense descriptor with a sparse input vector");
+		ALPB_CHECK(!masked || u_mask_count == m_out, ALPB_ILLEGAL,
+			"alpb_mxv: dense descriptor with a sparse output mask");
+		ALPB_CHECK(!input_masked || v_mask_count == n_in, ALPB_ILLEGAL,
+			"alpb_mxv: dense descriptor with a sparse input mask");
+	}
+	ALPB_CHECK(m_out == 0 || u != nullptr, ALPB_ILLEGAL, "alpb_mxv: null output");
+	ALPB_CHECK(n_in == 0 || v != nullptr || (descr & ALPB_DESC_USE_INDEX), ALPB_ILLEGAL,
+		"alpb_mxv: null input");
+	ALPB_CHECK(u_assigned == nullptr || u_nnz != nullptr, ALPB_ILLEGAL,
+		"alpb_mxv: sparse output needs its nnz counter");
+	// overlap checks (blas2.hpp:1040-1052)
+	ALPB_CHECK((descr & ALPB_DESC_SAFE_OVERLAP) || u != v || u == nullptr, ALPB_OVERLAP,
+		"alpb_mxv: output and input vectors overlap");
+	ALPB_CHECK(!masked || u_mask == nullptr || u != u_mask, ALPB_OVERLAP,
+		"alpb_mxv: output and mask vectors overlap");
+	if (plan) {
+		ALPB_CHECK(plan->m == m_out && plan->nnz == nnz, ALPB_MISMATCH,
+			"alpb_mxv: plan was made for another storage (%lld x nnz %lld)",
+			(long long) plan->m, (long long) plan->nnz);
+	}
+	SpmvArgs a{};
+	a.m_out = m_out;
+	a.n_in = n_in;
+	a.nnz = nnz;
+	a.offsets = offsets;
+	a.indices = indices;
+	a.values = value_type == ALPB_VOID ? nullptr : values;
+	a.u = u;
+	a.u_assigned = u_assigned;
+	a.u_nnz = u_nnz;
+	a.u_mask = u_mask;
+	a.u_mask_assigned = u_mask_assigned;
+	a.u_mask_type = u_mask == nullptr ? ALPB_VOID : u_mask_type;
+	a.v = v;
+	a.v_assigned = v_assigned;
+	a.v_mask = v_mask;
+	a.v_mask_assigned = v_mask_assigned;
+	a.v_mask_type = v_mask == nullptr ? ALPB_VOID : v_mask_type;
+	a.descr = descr;
+	a.left = (form & ALPB_FORM_LEFT) ? 1 : 0;
+	a.masked = masked;
+	a.input_masked = input_masked;
+	a.dense_all = u_assigned == nullptr && (v_assigned == nullptr || dense_hint);
+	const bool invert = (descr & ALPB_DESC_INVERT_MASK) != 0;
+	a.trivial = v_count == 0 || n_in == 0 || m_out == 0 || nnz == 0 ||
+		(masked && u_mask_count == 0 && !invert) || (input_masked && v_mask_count == 0 && !invert);
+	// The reference picks its loop by size (blas2.hpp:1108-1132, 1311-1334, the
+	// sequential backend's rule): the gather over the output's storage, or the
+	// scatter over the input's nonzeroes when that loop is shorter.  The two
+	// differ observably, so the same rule selects the semantics here:
+	//  - gather with a non-inverted output mask walks the mask's assigned set
+	//    and never reads its values (:1256-1301): the mask acts structurally;
+	//  - scatter (:617-745, :1135-1213) reads the mask by value, adds the
+	//    identity (add_identity) to every processed input index whatever the
+	//    mask, and never writes explicit zeroes.
+	{
+		const int64_t gather_loop = masked ? std::min(m_out, 2 * u_mask_count) : m_out;
+		int64_t scatter_loop = dense_hint ? n_in
+			: std::min(n_in, (input_masked && !invert) ? 2 * std::min(v_mask_count, v_count)
+													   : 2 * v_count);
+		if (descr & 8192u) scatter_loop = gather_loop + 1;  // force_row_major
+		a.scatter_sem = scatter_loop < gather_loop;
+		a.mask_by_structure = masked && !invert && !a.scatter_sem && (form & ALPB_FORM_ROWS);
+		if (a.mask_by_structure && u_mask_assigned == nullptr) {
+			// a dense mask read by structure selects every row
+			a.masked = false;
+			a.mask_by_structure = false;
+		}
+		if (a.scatter_sem) a.dense_all = false;
+	}
+	if (m_out == 0) return ALPB_SUCCESS;
+	return dispatch_spmv(ring, a, plan, 0, as_stream(stream));
+}
+
+} // extern "C"

@@ -1,0 +1,66 @@
+// Internal interface of the SpMV engine, shared by the solvers.
+#pragma once
+#include "common.cuh"
+
+// Schedule chosen for one compressed storage, with the merge-path tile table
+// and carry table (the scratch memory of the merge-path kernel).
+struct alpb_spmv_plan_s {
+	int64_t m = 0, nnz = 0;
+	const int64_t *offsets = nullptr;  // storage the plan was made for
+	int sched = ALPB_SCHED_VECTOR;
+	int vw = 8;
+	int device = 0;
+	int64_t ntiles = 0;
+	// merge-path tables (the scratch memory of the merge-path schedule)
+	int64_t *tile_row = nullptr;    // ntiles + 1 merge-path row splits
+	int64_t *head_first = nullptr;  // ntiles
+	int64_t *tail_first = nullptr;  // ntiles
+	int32_t *span_len = nullptr;    // ntiles
+	int32_t *counter = nullptr;     // ntiles (zero between products)
+	uint64_t *head_val = nullptr;   // ntiles
+	uint64_t *tail_val = nullptr;   // ntiles
+	uint8_t *head_has = nullptr;    // ntiles
+	uint8_t *tail_has = nullptr;    // ntiles
+	double mean = 0, maxlen = 0, cv = 0;
+	float tuned_ms = 0;
+};
+
+namespace alpb {
+
+struct SpmvArgs {
+	int64_t m_out, n_in, nnz;
+	const int64_t *offsets;
+	const uint32_t *indices;
+	const void *values;  // nullptr: pattern matrix
+	void *u;
+	uint8_t *u_assigned;
+	int64_t *u_nnz;
+	const void *u_mask;
+	const uint8_t *u_mask_assigned;
+	int u_mask_type;
+	const void *v;
+	const uint8_t *v_assigned;
+	const void *v_mask;
+	const uint8_t *v_mask_assigned;
+	int v_mask_type;
+	uint32_t descr;
+	int left;
+	bool masked, input_masked, dense_all, trivial;
+	// Path semantics of the reference (see alpb_mxv): the output mask is read
+	// by structure only when the reference walks the mask's assigned set, and
+	// the scatter path applies add_identity outside the output mask and
+	// ignores explicit_zero.
+	bool mask_by_structure, scatter_sem;
+};
+
+// Run one SpMV with the plan's schedule (force_sched != 0 overrides it).
+int dispatch_spmv(int ring, const SpmvArgs &a, const alpb_spmv_plan_s *p, int force_sched,
+	cudaStream_t s);
+int ring_value_type(int ring);
+
+// merge-path geometry, shared with the fused solvers
+constexpr int MP_BLOCK = 256;
+constexpr int MP_IPT = 8;
+constexpr int MP_TILE = MP_BLOCK * MP_IPT;
+
+} // namespace alpb

@@ -1,0 +1,323 @@
+/*
+ * alp_b200.h -- C-ABI of the B200 backend for the ALP/GraphBLAS hot path.
+ *
+ * Every entry point takes plain device pointers, sizes, small integer codes
+ * and a cudaStream_t passed as `void *` (NULL = legacy default stream).  No
+ * C++ or torch type appears in a signature, so C, C++ (the grb::b200
+ * template backend under include/graphblas/b200/), ctypes and any other FFI
+ * bind it the same way.
+ *
+ * Status: every function returns an `int` whose values are numerically equal
+ * to grb::RC (reference: include/graphblas/rc.hpp:47-155), so the C++ backend
+ * returns them unchanged.  On a non-SUCCESS return the output containers are
+ * unchanged, except for ALPB_PANIC (the grb::RC contract of
+ * include/graphblas/base/blas2.hpp:208-223).  alpb_last_error() returns a
+ * thread-local human-readable message for the last failing call.
+ *
+ * Storage conventions (mirroring internal::Compressed_Storage,
+ * include/graphblas/reference/compressed_storage.hpp:48-797):
+ *   - offsets   int64[m+1]   (NonzeroIndexType = size_t in the reference)
+ *   - indices   uint32[nnz]  (RowIndexType = ColIndexType = unsigned int,
+ *                             include/graphblas/base/config.hpp:436-475)
+ *   - values    D[nnz] or NULL for a pattern (void) matrix.
+ *   A CCS is passed through the same arguments: (col_start, row_index, values)
+ *   of the transposed orientation, exactly as the reference stores both.
+ *
+ * Vector conventions (mirroring Vector<D,reference> + Coordinates,
+ * include/graphblas/reference/vector.hpp:280-289, coordinates.hpp:61-1500):
+ *   - values    D[n]
+ *   - assigned  uint8[n] (1 = entry present) or NULL for a dense vector
+ *   - nnz       int64 device counter of assigned entries, updated by kernels
+ *               that assign new entries (may be NULL iff assigned is NULL).
+ */
+#ifndef ALP_B200_H
+#define ALP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALPB_API __attribute__((visibility("default")))
+
+/* ---- status codes: identical numbering to grb::RC (rc.hpp:47-155) ---- */
+enum alpb_status {
+	ALPB_SUCCESS = 0,
+	ALPB_PANIC = 1,
+	ALPB_OUTOFMEM = 2,
+	ALPB_MISMATCH = 3,
+	ALPB_OVERLAP = 4,
+	ALPB_OVERFLW = 5,
+	ALPB_UNSUPPORTED = 6,
+	ALPB_ILLEGAL = 7,
+	ALPB_FAILED = 8
+};
+
+/* ---- descriptor bits: identical to grb::descriptors (descriptors.hpp:63-267) ---- */
+#define ALPB_DESC_NONE             0u
+#define ALPB_DESC_INVERT_MASK      1u
+#define ALPB_DESC_TRANSPOSE_MATRIX 2u
+#define ALPB_DESC_NO_DUPLICATES    4u
+#define ALPB_DESC_STRUCTURAL       8u
+#define ALPB_DESC_DENSE           16u
+#define ALPB_DESC_ADD_IDENTITY    32u
+#define ALPB_DESC_USE_INDEX       64u
+#define ALPB_DESC_NO_CASTING     256u
+#define ALPB_DESC_EXPLICIT_ZERO  512u
+#define ALPB_DESC_SAFE_OVERLAP  1024u
+
+/* ---- element type codes ---- */
+enum alpb_type {
+	ALPB_VOID = 0,   /* pattern: no value array                      */
+	ALPB_BOOL = 1,   /* uint8 holding 0 or 1                          */
+	ALPB_INT32 = 2,
+	ALPB_FP64 = 3,
+	ALPB_UINT32 = 4,
+	ALPB_INT64 = 5
+};
+
+/*
+ * ---- semirings instantiated on the device ----
+ * Each is an ALP grb::Semiring< add, mul, zero-identity, one-identity >:
+ *   PLUS_TIMES_F64   <operators::add<double>, operators::mul<double>,
+ *                     identities::zero, identities::one>       (ops.hpp:175,208)
+ *   LOR_LAND_BOOL    <operators::logical_or<bool>, operators::logical_and<bool>,
+ *                     identities::logical_false, identities::logical_true>
+ *                                                             (ops.hpp:462,490)
+ *   MIN_PLUS_I32     <operators::min<int>, operators::add<int>,
+ *                     identities::infinity, identities::zero>  (ops.hpp:274,175)
+ *   PLUS_PATTERN_F64 <operators::add<double>,
+ *                     operators::left_assign_if<double,bool,double>,
+ *                     identities::zero, identities::logical_true>
+ *                     -- the out-degree ring of simple_pagerank.hpp:224-237
+ *   PLUS_TIMES_I32   <operators::add<int>, operators::mul<int>, zero, one>
+ * Any other semiring is not instantiated and returns ALPB_UNSUPPORTED.
+ */
+enum alpb_ring {
+	ALPB_RING_PLUS_TIMES_F64 = 0,
+	ALPB_RING_LOR_LAND_BOOL = 1,
+	ALPB_RING_MIN_PLUS_I32 = 2,
+	ALPB_RING_PLUS_PATTERN_F64 = 3,
+	ALPB_RING_PLUS_TIMES_I32 = 4
+};
+
+/* SpMV schedules (the autotuner chooses among them per sparsity profile) */
+enum alpb_schedule {
+	ALPB_SCHED_AUTO = 0,
+	ALPB_SCHED_MERGE_PATH = 1,   /* nnz+rows balanced tiles, deterministic carries */
+	ALPB_SCHED_VECTOR = 2        /* W lanes per row, W in {1,2,4,8,16,32}      */
+};
+
+typedef struct alpb_spmv_plan_s *alpb_spmv_plan;
+
+/* ======================================================================
+ * Runtime (replaces grb::init / grb::finalize,
+ * src/graphblas/reference/init.cpp:45-113, include/graphblas/base/init.hpp)
+ * ====================================================================== */
+ALPB_API int alpb_init(int device);
+ALPB_API int alpb_finalize(void);
+ALPB_API const char *alpb_last_error(void);
+ALPB_API int alpb_version(void);
+/* Number of kernels this library has launched since load (all entry points). */
+ALPB_API int64_t alpb_launch_count(void);
+
+/* device memory for the container classes (reference: utils::AutoDeleter /
+ * reference/alloc.hpp allocation modes); bytes are rounded up to 256 B. */
+ALPB_API int alpb_malloc(void **ptr, size_t bytes);
+ALPB_API int alpb_free(void *ptr);
+ALPB_API int alpb_memcpy_h2d(void *dst, const void *src, size_t bytes, void *stream);
+ALPB_API int alpb_memcpy_d2h(void *dst, const void *src, size_t bytes, void *stream);
+ALPB_API int alpb_memcpy_d2d(void *dst, const void *src, size_t bytes, void *stream);
+ALPB_API int alpb_memset(void *dst, int byte, size_t bytes, void *stream);
+ALPB_API int alpb_stream_sync(void *stream);
+
+/* ======================================================================
+ * Synthetic generators, seeded counter-based (same integer hash as the
+ * oracle, so CPU and GPU produce identical inputs).
+ * ====================================================================== */
+/* 64-bit mix used by every generator: out[k] = hash(seed, stream, k). */
+ALPB_API int alpb_gen_hash_u64(uint64_t *out, int64_t count, uint64_t seed,
+	uint64_t stream_id, void *stream);
+/* fill a value array from the hash: FP64 -> U[0,1); INT32 -> lo + h % (hi-lo+1);
+ * BOOL -> 1 with probability p (p only used for BOOL). */
+ALPB_API int alpb_gen_values(void *out, int type, int64_t count, uint64_t seed,
+	uint64_t stream_id, int32_t lo, int32_t hi, double p, void *stream);
+/* R-MAT edge keys ((uint64)row << 32 | col), 2^scale vertices, quadrant
+ * probabilities a, b, c (d = 1-a-b-c); no deduplication. */
+ALPB_API int alpb_gen_rmat_keys(uint64_t *keys, int64_t n_draws, int scale,
+	double a, double b, double c, uint64_t seed, void *stream);
+/* edge values keyed by (row, col): identical for the same edge whatever its
+ * position; FP64 -> U[0,1), INT32 -> lo + h % (hi-lo+1). */
+ALPB_API int alpb_gen_edge_values(void *values, int type, const int64_t *row_ptr,
+	const uint32_t *col_idx, int64_t m, int64_t nnz, uint64_t seed,
+	int32_t lo, int32_t hi, void *stream);
+
+/* ======================================================================
+ * Matrix construction (replaces Matrix<D,reference>::buildMatrixUnique,
+ * include/graphblas/reference/matrix.hpp:1820-2030, on the device)
+ * ====================================================================== */
+/* Sort keys ascending and remove duplicates in place; *n_unique receives the
+ * count (synchronises `stream`). */
+ALPB_API int alpb_keys_sort_unique(uint64_t *keys, int64_t n, int64_t *n_unique,
+	void *stream);
+/* Row offsets and column indices from sorted unique keys. */
+ALPB_API int alpb_crs_from_sorted_keys(const uint64_t *keys, int64_t nnz, int64_t m,
+	int64_t *row_ptr, uint32_t *col_idx, void *stream);
+/* General COO -> CRS with the reference's in-row order (reverse of input
+ * order, matrix.hpp:1921-1930).  I, J uint32[nnz]; values of `type` or NULL. */
+ALPB_API int alpb_coo_to_crs(int64_t m, int64_t n, int64_t nnz, const uint32_t *I,
+	const uint32_t *J, const void *values, int type, int64_t *row_ptr,
+	uint32_t *col_idx, void *out_values, void *stream);
+/* CCS (= CRS of the transpose) from CRS; stable, so within a column entries
+ * appear in increasing row order. */
+ALPB_API int alpb_crs_transpose(int64_t m, int64_t n, int64_t nnz,
+	const int64_t *row_ptr, const uint32_t *col_idx, const void *values, int type,
+	int64_t *col_ptr, uint32_t *row_idx, void *t_values, void *stream);
+/* n-dimensional box stencil of halo 1 (hpcg/ndim_matrix_builders.hpp:198-394,
+ * build_ndims_system_matrix, hpcg/matrix_building_utils.hpp:61-110): rows in
+ * natural order, dimension 0 fastest; diag value on i==j else off value.  With
+ * ref_order != 0 the in-row order is that of the reference build (decreasing
+ * column); else increasing.  Call with row_ptr only (col_idx = NULL) to get
+ * *nnz first. */
+ALPB_API int alpb_gen_stencil_crs(int dims, const int64_t *sizes, double diag,
+	double off, int ref_order, int64_t *row_ptr, uint32_t *col_idx, double *values,
+	int64_t *nnz, void *stream);
+/* 2-D 5-point Poisson on an L x L grid (Dirichlet), diag 4+shift, off -1. */
+ALPB_API int alpb_gen_poisson2d_crs(int64_t L, double shift, int64_t *row_ptr,
+	uint32_t *col_idx, double *values, void *stream);
+
+/* ======================================================================
+ * SpMV (replaces internal::vxm_generic + vxm_inner_kernel_gather,
+ * include/graphblas/reference/blas2.hpp:283-551, 835-1528, and the public
+ * grb::mxv / grb::vxm overloads, blas2.hpp:1532-2230)
+ * ====================================================================== */
+/* Analyse a compressed storage (row lengths: mean, max, CV), choose a
+ * schedule (sched = ALPB_SCHED_AUTO) and precompute its tile table. */
+ALPB_API int alpb_spmv_plan_create(alpb_spmv_plan *plan, int64_t m, int64_t nnz,
+	const int64_t *offsets, int sched, int vector_width, void *stream);
+ALPB_API int alpb_spmv_plan_destroy(alpb_spmv_plan plan);
+/* Time the candidate schedules on this matrix/ring and keep the fastest. */
+ALPB_API int alpb_spmv_autotune(alpb_spmv_plan plan, int ring, int64_t n,
+	const uint32_t *indices, const void *values, int value_type, const void *x,
+	void *y_scratch, void *stream);
+/* chosen schedule and vector width (for reporting). */
+ALPB_API int alpb_spmv_plan_info(alpb_spmv_plan plan, int *sched, int *vector_width,
+	int64_t *tiles);
+
+/* `form` bits of alpb_mxv */
+#define ALPB_FORM_LEFT 1  /* vector on the left: mul(v_i, A_ij) (vxm)            */
+#define ALPB_FORM_ROWS 2  /* the gather storage is the matrix's CRS              */
+
+/*
+ * u = u (+) A (x) v over `ring`, gathering over the compressed storage
+ * (offsets, indices, values) whose outer dimension is the output:
+ *   mxv(u, A, v)          : pass A's CRS, form = ROWS         (mul(A_ij, v_j))
+ *   vxm(u, v, A)          : pass A's CCS, form = LEFT         (mul(v_i, A_ij))
+ *   mxv<transpose_matrix> : pass A's CCS, form = 0
+ *   vxm<transpose_matrix> : pass A's CRS, form = LEFT | ROWS
+ * m_out = length of u, n_in = length of v.  Masks: u_mask on the output,
+ * v_mask on the input, evaluated as utils::interpretMask (utils.hpp:318-341)
+ * under `descr` (structural / invert_mask).  mask values of mask_type
+ * (BOOL/INT32/FP64/VOID).  Descriptor bits honoured: invert_mask, structural,
+ * dense, add_identity, use_index, explicit_zero, safe_overlap.  The
+ * transpose_matrix bit must already be resolved by the caller (choice of
+ * storage and form), as the reference does at blas2.hpp:1848.
+ * The reference's observable semantics depend on which loop it runs, and
+ * alpb_mxv applies the same choice (the sequential backend's rule,
+ * blas2.hpp:1108-1132, 1311-1334): when the scatter over the input's
+ * nonzeroes is the shorter loop, add_identity reaches every processed input
+ * index whatever the output mask and explicit_zero writes nothing
+ * (blas2.hpp:617-745); on the CRS gather (form & ROWS) a non-inverted output
+ * mask is read by structure, not by value (blas2.hpp:1256-1301).
+ * Host-side entry counts (the Coordinates::nonzeroes() the reference reads on
+ * the host) drive the trivial cases (blas2.hpp:1001-1037) and the dense
+ * checks (blas2.hpp:950-971): v_count = nnz(v); u_mask_count = nnz(u_mask)
+ * or -1 for "no output mask"; v_mask_count likewise for the input mask.
+ * `plan` may be NULL (vector schedule, no scratch).
+ */
+ALPB_API int alpb_mxv(int ring, uint32_t descr, int form,
+	int64_t m_out, int64_t n_in, int64_t nnz,
+	const int64_t *offsets, const uint32_t *indices, const void *values,
+	int value_type,
+	void *u, uint8_t *u_assigned, int64_t *u_nnz,
+	const void *u_mask, const uint8_t *u_mask_assigned, int u_mask_type,
+	int64_t u_mask_count,
+	const void *v, const uint8_t *v_assigned, int64_t v_count,
+	const void *v_mask, const uint8_t *v_mask_assigned, int v_mask_type,
+	int64_t v_mask_count,
+	alpb_spmv_plan plan, void *stream);
+
+/* ======================================================================
+ * BLAS1 (replaces reference/blas1.hpp: dot 9262-9681, eWiseMul 8610-9172,
+ * eWiseMulAdd 6347-6770, foldl/foldr 1069-2897, eWiseApply 2966-5343, set in
+ * reference/io.hpp).  FP64 unless stated; dense vectors unless an assigned
+ * array is passed.
+ * ====================================================================== */
+enum alpb_op {
+	ALPB_OP_ADD = 0, ALPB_OP_SUB = 1, ALPB_OP_MUL = 2, ALPB_OP_DIV = 3,
+	ALPB_OP_MIN = 4, ALPB_OP_MAX = 5, ALPB_OP_ABS_DIFF = 6,
+	ALPB_OP_LEFT_ASSIGN = 7, ALPB_OP_RIGHT_ASSIGN = 8,
+	ALPB_OP_LOR = 9, ALPB_OP_LAND = 10
+};
+/* *result = *result (+) sum_i x_i (*) y_i with (+) = add_op, (*) = mul_op,
+ * over entries assigned in both; result is a HOST double (synchronises). */
+ALPB_API int alpb_dot_f64(double *result, int add_op, int mul_op, int64_t n,
+	const double *x, const uint8_t *x_assigned, const double *y,
+	const uint8_t *y_assigned, void *stream);
+/* same, result left on the device (no synchronisation). */
+ALPB_API int alpb_dot_f64_device(double *d_result, int add_op, int mul_op, int64_t n,
+	const double *x, const double *y, void *stream);
+/* x[i] = value for all i (dense result); if assigned != NULL it is set to 1
+ * and *nnz = n. */
+ALPB_API int alpb_set_scalar(void *x, int type, int64_t n, double value,
+	uint8_t *assigned, int64_t *nnz, void *stream);
+/* z = alpha (*) x (+) y style elementwise: out[i] = op(a[i], b[i]) for dense
+ * FP64 vectors; a or b may be NULL to use the scalar sa / sb instead. */
+ALPB_API int alpb_ewise_apply_f64(double *out, int op, int64_t n, const double *a,
+	double sa, const double *b, double sb, void *stream);
+/* out[i] = out[i] (+) (a[i] (*) b[i]) (eWiseMulAdd / eWiseMul in-place accumulate);
+ * a or b NULL -> scalar. */
+ALPB_API int alpb_ewise_muladd_f64(double *out, int add_op, int mul_op, int64_t n,
+	const double *a, double sa, const double *b, double sb, void *stream);
+/* foldl: x[i] = x[i] op y[i] (y NULL -> scalar sy); foldr: y[i] = x op y[i]. */
+ALPB_API int alpb_foldl_f64(double *x, int op, int64_t n, const double *y, double sy,
+	void *stream);
+/* reduce a dense vector to a host scalar: *result = *result op fold(x). */
+ALPB_API int alpb_reduce_f64(double *result, int op, int64_t n, const double *x,
+	const uint8_t *assigned, void *stream);
+
+/* ======================================================================
+ * Solvers
+ * ====================================================================== */
+/* Conjugate gradient with the numerics of
+ * algorithms::preconditioned_conjugate_gradient (conjugate_gradient.hpp:
+ * 191-483, unpreconditioned branch): relative tolerance tol*||b||, stops when
+ * sqrt(r.r) < tol or after max_iter; *residual = r.r (not its root).  All
+ * FP64.  Fused: two passes over HBM per iteration (SpMV + dot, then the
+ * x/r/u updates + r.r), device-side scalars, no host sync per iteration.
+ * x holds the initial guess on entry.  `work` is 4*n doubles of scratch or
+ * NULL (allocated internally).  Returns ALPB_FAILED when not converged.  */
+ALPB_API int alpb_cg_solve(int64_t n, const int64_t *row_ptr, const uint32_t *col_idx,
+	const double *values, const double *b, double *x, int64_t max_iter, double tol,
+	int64_t *iterations, double *residual, double *work, alpb_spmv_plan plan,
+	void *stream);
+
+/* Power-iteration PageRank with the numerics of algorithms::simple_pagerank
+ * (simple_pagerank.hpp:146-533): pr_j <- alpha * sum_i L_ij pr_i / outdeg_i
+ * + (alpha * dangling + 1 - alpha) / n, L1 residual, stop at residual <= conv.
+ * Takes L's CCS (col_ptr, row_idx, values; values NULL = pattern of ones) and
+ * the CRS offsets for the out-degrees.  pr holds the initial guess if
+ * init_given != 0, else 1/n. */
+ALPB_API int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr,
+	const uint32_t *crs_col_idx, const double *crs_values,
+	const int64_t *ccs_col_ptr, const uint32_t *ccs_row_idx, const double *ccs_values,
+	double *pr, int init_given, double alpha, double conv, int64_t max_iter,
+	int64_t *iterations, double *residual, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALP_B200_H */
