@@ -54,6 +54,8 @@ PROTOS: dict[str, list] = {
     "alpb_launch_count": [],
     "alpb_malloc": [C.POINTER(P), C.c_size_t],
     "alpb_free": [P],
+    "alpb_malloc_managed": [C.POINTER(P), C.c_size_t],
+    "alpb_prefetch": [P, C.c_size_t, I32, P],
     "alpb_memcpy_h2d": [P, P, C.c_size_t, P],
     "alpb_memcpy_d2h": [P, P, C.c_size_t, P],
     "alpb_memcpy_d2d": [P, P, C.c_size_t, P],
@@ -69,6 +71,9 @@ PROTOS: dict[str, list] = {
     "alpb_crs_transpose": [I64, I64, I64, P, P, P, I32, P, P, P, P],
     "alpb_gen_stencil_crs": [I32, PI64, D, D, I32, P, P, P, PI64, P],
     "alpb_gen_poisson2d_crs": [I64, D, P, P, P, P],
+    "alpb_gen_poisson2d_batch": [I64, P, P, P, P, I64, P, P, P, P],
+    "alpb_gen_normal": [P, I64, U64, U64, P],
+    "alpb_gen_sym_dd_values": [P, P, I64, U64, D, D, D, P, P],
     "alpb_spmv_plan_create": [C.POINTER(P), I64, I64, P, I32, I32, P],
     "alpb_spmv_plan_destroy": [P],
     "alpb_spmv_autotune": [P, I32, I64, P, P, I32, P, P, P],
@@ -86,8 +91,21 @@ PROTOS: dict[str, list] = {
     "alpb_ewise_muladd_f64": [P, I32, I32, I64, P, D, P, D, P],
     "alpb_foldl_f64": [P, I32, I64, P, D, P],
     "alpb_reduce_f64": [PD, I32, I64, P, P, P],
+    "alpb_vec_op": [I32, I32, I32, D, I32, U32, I64, P, I32, P, P, P, P, I32, I32,
+                    P, I32, P, D, P, I32, P, D, P],
+    "alpb_count_assigned": [P, I64, PI64, P],
+    "alpb_vec_reduce": [PD, I32, D, I32, U32, I64, P, I32, P, P, I32, P, P, P, I32, I32, P],
     "alpb_cg_solve": [I64, P, P, P, P, P, I64, D, PI64, PD, P, P, P],
     "alpb_pagerank": [I64, P, P, P, P, P, P, P, I32, D, D, I64, PI64, PD, P],
+    "alpb_sddmm": [P, I64, I64, P, P, P, P, D, P, P],
+    "alpb_cg_adjoint": [I64, P, P, P, P, P, P, P, P, P, P, I64, D, PI64, PD, P, P, P],
+    "alpb_cg_grad": [I64, P, P, P, P, P, P, P, P, P, P, P, P, I64, D, PD, PI64, PI64, P, P, P],
+    "alpb_batched_cg_create": [C.POINTER(P), I64, I64, P, P, P, I64, P, P],
+    "alpb_batched_cg_destroy": [P],
+    "alpb_batched_cg_solve": [P, P, P, I64, D, P],
+    "alpb_batched_cg_capture": [P, P, P, I64, D, P],
+    "alpb_batched_cg_replay": [P, P],
+    "alpb_batched_cg_results": [P, P, P, P, P],
 }
 _RESTYPE = {"alpb_last_error": C.c_char_p, "alpb_launch_count": C.c_int64}
 

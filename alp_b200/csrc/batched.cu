@@ -1,0 +1,571 @@
+// Batched conjugate gradient: many independent SPD systems of uneven size,
+// solved together in ONE persistent cooperative launch.
+//
+// The instances are stored as one block-diagonal CRS (instance i owns rows
+// [seg_rows[i], seg_rows[i+1])).  The merge-path tiles are cut per instance
+// (merge_plan_segmented), so every tile belongs to exactly one instance and
+// every instance scalar (beta, alpha, r.r, gamma, sigma) is a sum over that
+// instance's tiles.  Each iteration has the two phases of the single-system
+// solver (cg.cu) and two grid barriers for the whole batch; the per-instance
+// reductions are finished by the last tile of the instance to arrive
+// (atomic arrival counter, sum in tile order: deterministic), so no extra
+// barrier is spent on them.  An instance that converges (its own relative
+// tolerance, as algorithms::conjugate_gradient tests it,
+// conjugate_gradient.hpp:377-378, :437) or exhausts the iteration budget is
+// masked out; the launch ends when no instance is active.
+#include "common.cuh"
+#include "merge.cuh"
+#include "persist.cuh"
+#include "spmv.cuh"
+
+#include <cub/device/device_scan.cuh>
+
+#include <cmath>
+#include <vector>
+
+namespace alpb {
+
+using RF = RingPlusTimesF64;
+
+// ------------------------------------------------------ segmented tables --
+__global__ void k_seg_tile_counts(const int64_t *offsets, const int64_t *seg_rows, int64_t nseg,
+	int64_t *counts) {
+	for (int64_t s = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s <= nseg;
+		 s += int64_t(gridDim.x) * blockDim.x) {
+		if (s == nseg) { counts[s] = 0; continue; }
+		const int64_t r0 = seg_rows[s], r1 = seg_rows[s + 1];
+		const int64_t items = (r1 - r0) + (offsets[r1] - offsets[r0]);
+		counts[s] = (items + MP_TILE - 1) / MP_TILE;
+	}
+}
+
+__global__ void k_seg_tile_d(const int64_t *offsets, const int64_t *seg_rows, const int64_t *seg_tile,
+	int64_t nseg, int64_t m, int64_t nnz, int64_t *tile_d, int32_t *tile_seg) {
+	for (int64_t s = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < nseg;
+		 s += int64_t(gridDim.x) * blockDim.x) {
+		const int64_t r0 = seg_rows[s];
+		const int64_t base = r0 + offsets[r0];
+		for (int64_t t = seg_tile[s]; t < seg_tile[s + 1]; ++t) {
+			tile_d[t] = base + (t - seg_tile[s]) * MP_TILE;
+			tile_seg[t] = int32_t(s);
+		}
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) tile_d[seg_tile[nseg]] = m + nnz;
+}
+
+__device__ __forceinline__ int64_t merge_search_d(const int64_t *offsets, int64_t m, int64_t nnz,
+	int64_t d) {
+	int64_t lo = d - nnz > 0 ? d - nnz : 0;
+	int64_t hi = d < m ? d : m;
+	while (lo < hi) {
+		const int64_t pivot = (lo + hi) >> 1;
+		if (offsets[pivot + 1] <= d - pivot - 1) lo = pivot + 1; else hi = pivot;
+	}
+	return lo;
+}
+
+__global__ void k_seg_tile_rows(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
+	const int64_t *tile_d, int64_t *tile_row) {
+	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t <= ntiles;
+		 t += int64_t(gridDim.x) * blockDim.x)
+		tile_row[t] = merge_search_d(offsets, m, nnz, tile_d[t]);
+}
+
+// tile containing diagonal d: last t with tile_d[t] <= d
+__device__ __forceinline__ int64_t tile_of(const int64_t *tile_d, int64_t ntiles, int64_t d) {
+	int64_t lo = 0, hi = ntiles - 1;
+	while (lo < hi) {
+		const int64_t mid = (lo + hi + 1) >> 1;
+		if (tile_d[mid] <= d) lo = mid; else hi = mid - 1;
+	}
+	return lo;
+}
+
+__global__ void k_seg_tables(const int64_t *offsets, int64_t m, int64_t ntiles,
+	const int64_t *tile_d, const int64_t *tile_row, int64_t *head_first, int64_t *tail_first,
+	int32_t *span_len) {
+	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < ntiles;
+		 t += int64_t(gridDim.x) * blockDim.x) {
+		const int64_t i0 = tile_row[t], i1 = tile_row[t + 1];
+		const int64_t d0 = tile_d[t], d1 = tile_d[t + 1];
+		const int64_t j0 = d0 - i0, j1 = d1 - i1;
+		head_first[t] = (i1 > i0 && offsets[i0] < j0) ? tile_of(tile_d, ntiles, i0 + offsets[i0]) : -1;
+		int64_t tf = -1;
+		if (i1 < m) {
+			const int64_t start = offsets[i1] > j0 ? offsets[i1] : j0;
+			if (j1 > start) tf = tile_of(tile_d, ntiles, i1 + offsets[i1]);
+		}
+		tail_first[t] = tf;
+		span_len[t] = (tf == t)
+			? int32_t(tile_of(tile_d, ntiles, i1 + offsets[i1 + 1]) - t + 1) : 0;
+	}
+}
+
+int merge_plan_segmented(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t nseg,
+	const int64_t *seg_rows, SegmentedTiles *st, cudaStream_t s) {
+	st->nseg = nseg;
+	ALPB_CUDA(cudaMalloc(&st->seg_tile, size_t(nseg + 1) * 8));
+	int64_t *counts = nullptr;
+	void *tmp = nullptr;
+	size_t tb = 0;
+	ALPB_CUDA(cudaMallocAsync(&counts, size_t(nseg + 1) * 8, s));
+	k_seg_tile_counts<<<grid_for(nseg + 1, 256), 256, 0, s>>>(offsets, seg_rows, nseg, counts);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, counts, st->seg_tile, nseg + 1, s));
+	ALPB_CUDA(cudaMallocAsync(&tmp, tb, s));
+	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, counts, st->seg_tile, nseg + 1, s));
+	g_launches.fetch_add(1);
+	int64_t nt = 0;
+	ALPB_CUDA(cudaMemcpyAsync(&nt, st->seg_tile + nseg, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaFreeAsync(counts, s));
+	ALPB_CUDA(cudaFreeAsync(tmp, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	ALPB_CHECK(nt > 0, ALPB_ILLEGAL, "segmented plan: no work");
+	p->ntiles = nt;
+	const size_t n = size_t(nt);
+	ALPB_CUDA(cudaMalloc(&st->tile_d, (n + 1) * 8));
+	ALPB_CUDA(cudaMalloc(&st->tile_seg, n * 4));
+	ALPB_CUDA(cudaMalloc(&p->tile_row, (n + 1) * 8));
+	ALPB_CUDA(cudaMalloc(&p->head_first, n * 8));
+	ALPB_CUDA(cudaMalloc(&p->tail_first, n * 8));
+	ALPB_CUDA(cudaMalloc(&p->span_len, n * 4));
+	ALPB_CUDA(cudaMalloc(&p->counter, n * 4));
+	ALPB_CUDA(cudaMalloc(&p->head_val, n * 8));
+	ALPB_CUDA(cudaMalloc(&p->tail_val, n * 8));
+	ALPB_CUDA(cudaMalloc(&p->head_has, n));
+	ALPB_CUDA(cudaMalloc(&p->tail_has, n));
+	ALPB_CUDA(cudaMemsetAsync(p->counter, 0, n * 4, s));
+	k_seg_tile_d<<<grid_for(nseg, 256), 256, 0, s>>>(offsets, seg_rows, st->seg_tile, nseg, p->m,
+		p->nnz, st->tile_d, st->tile_seg);
+	ALPB_LAUNCHED();
+	k_seg_tile_rows<<<grid_for(nt + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz, nt, st->tile_d,
+		p->tile_row);
+	ALPB_LAUNCHED();
+	k_seg_tables<<<grid_for(nt, 256), 256, 0, s>>>(offsets, p->m, nt, st->tile_d, p->tile_row,
+		p->head_first, p->tail_first, p->span_len);
+	ALPB_LAUNCHED();
+	st->seg_rows = const_cast<int64_t *>(seg_rows);
+	return ALPB_SUCCESS;
+}
+
+void segmented_free(SegmentedTiles *st) {
+	cudaFree(st->seg_tile);
+	cudaFree(st->tile_d);
+	cudaFree(st->tile_seg);
+	st->seg_tile = st->tile_d = nullptr;
+	st->tile_seg = nullptr;
+}
+
+// ------------------------------------------------------------ batched CG --
+struct BcgInst {       // per-instance device state
+	double sigma, gamma, alpha, tol_abs, rr;
+	int64_t iterations;
+	int32_t done, converged;
+	int32_t cnt;       // arrival counter of the instance's tiles (zero between phases)
+	int32_t pad;
+};
+
+struct BcgArgs {
+	MergeTables mt;
+	const int64_t *offsets;
+	const uint32_t *indices;
+	const double *values;
+	const double *b;
+	double *x, *r, *u0, *u1, *temp;
+	double *own, *span, *own2, *span2;  // [ntiles]
+	const int32_t *tile_seg;           // [ntiles]
+	const int64_t *seg_tile;           // [nseg+1]
+	BcgInst *inst;                     // [nseg]
+	int64_t nseg, max_iter;
+	double tol;
+	int32_t *active;                   // instances still iterating
+	GridSync *gs;
+};
+
+struct BcgPrelude {
+	const BcgArgs *a;
+	double acc_rr = 0.0, acc_bb = 0.0;
+	__device__ __forceinline__ void terms(int64_t i, double v, bool has, double &rr, double &bb) {
+		const double t = has ? 0.0 + v : 0.0;
+		const double bi = a->b[i];
+		const double ri = (0.0 + bi) - t;
+		a->r[i] = ri;
+		a->u0[i] = 0.0;
+		rr = ri * ri;
+		bb = bi * bi;
+	}
+	__device__ __forceinline__ void row(int64_t i, double v, bool has) {
+		double rr, bb;
+		terms(i, v, has, rr, bb);
+		acc_rr += rr;
+		acc_bb += bb;
+	}
+	__device__ __forceinline__ void row_span(int64_t first, int64_t i, double v, bool has) {
+		double rr, bb;
+		terms(i, v, has, rr, bb);
+		a->span[first] = rr;
+		a->span2[first] = bb;
+	}
+};
+
+struct BcgGather {
+	const double *r, *u_old;
+	double gamma;
+	__device__ __forceinline__ double operator()(uint32_t j) const {
+		return __ldcg(r + j) + gamma * __ldcg(u_old + j);
+	}
+};
+
+struct BcgIter {
+	const BcgArgs *a;
+	const double *u_old;
+	double *u_new;
+	double gamma;
+	double acc = 0.0;
+	__device__ __forceinline__ double term(int64_t i, double v, bool has) {
+		const double t = has ? 0.0 + v : 0.0;
+		a->temp[i] = t;
+		const double un = __ldcg(a->r + i) + gamma * __ldcg(u_old + i);
+		u_new[i] = un;
+		return t * un;
+	}
+	__device__ __forceinline__ void row(int64_t i, double v, bool has) { acc += term(i, v, has); }
+	__device__ __forceinline__ void row_span(int64_t first, int64_t i, double v, bool has) {
+		a->span[first] = term(i, v, has);
+	}
+};
+
+// The last of instance s's tiles to arrive gets true; the caller then sums
+// the instance's tile partials.  Called by thread 0 after the tile's
+// partials are stored.
+__device__ __forceinline__ bool inst_arrive(BcgInst *in, int64_t ntiles_inst) {
+	__threadfence();
+	const int32_t prev = atomicAdd(&in->cnt, 1);
+	if (prev != ntiles_inst - 1) return false;
+	__threadfence();
+	in->cnt = 0;
+	return true;
+}
+
+__device__ __forceinline__ double sum_tiles(const double *own, const double *span, int64_t t0,
+	int64_t t1) {
+	double v = 0.0;
+	for (int64_t t = t0; t < t1; ++t)
+		v += ((const volatile double *) own)[t] + (span ? ((const volatile double *) span)[t] : 0.0);
+	return v;
+}
+
+__global__ void __launch_bounds__(MP_BLOCK) k_batched_cg(BcgArgs a) {
+	__shared__ MergeSmem<RF> sm;
+	__shared__ double red[33];
+	const int64_t G = gridDim.x, nt = a.mt.ntiles;
+	for (int64_t t = blockIdx.x; t < nt; t += G) {
+		a.span[t] = 0.0;
+		a.span2[t] = 0.0;
+	}
+	if (!grid_sync(a.gs)) return;
+
+	// prelude per instance: r = b - A x, sigma = r.r, tol * ||b||
+	{
+		BcgPrelude epi{&a};
+		PlainX<double> xl{a.x};
+		for (int64_t t = blockIdx.x; t < nt; t += G) {
+			epi.acc_rr = epi.acc_bb = 0.0;
+			merge_tile<RF>(t, a.mt, a.offsets, a.indices, a.values, xl, epi, 0, sm);
+			const double s1 = block_sum(epi.acc_rr, red);
+			const double s2 = block_sum(epi.acc_bb, red);
+			if (threadIdx.x == 0) {
+				a.own[t] = s1;
+				a.own2[t] = s2;
+			}
+		}
+	}
+	if (!grid_sync(a.gs)) return;  // spanning terms of every instance are in place
+	for (int64_t s = blockIdx.x; s < a.nseg; s += G) {
+		if (threadIdx.x != 0) continue;
+		BcgInst *in = a.inst + s;
+		const double sigma = sum_tiles(a.own, a.span, a.seg_tile[s], a.seg_tile[s + 1]);
+		const double bnorm = sum_tiles(a.own2, a.span2, a.seg_tile[s], a.seg_tile[s + 1]);
+		in->sigma = sigma;
+		in->gamma = 0.0;
+		in->tol_abs = a.tol * sqrt(bnorm);
+		in->iterations = 0;
+		in->done = 0;
+		in->converged = 0;
+		in->cnt = 0;
+	}
+	if (!grid_sync(a.gs)) return;
+
+	int64_t iter = 0;
+	double *u_old = a.u0, *u_new = a.u1;
+	for (;;) {
+		++iter;
+		// phase A over the tiles of active instances
+		for (int64_t t = blockIdx.x; t < nt; t += G) {
+			const int32_t s = a.tile_seg[t];
+			BcgInst *in = a.inst + s;
+			if (((volatile int32_t *) &in->done)[0]) continue;
+			const double gamma = ((volatile double *) &in->gamma)[0];
+			BcgIter epi{&a, u_old, u_new, gamma};
+			BcgGather xl{a.r, u_old, gamma};
+			merge_tile<RF>(t, a.mt, a.offsets, a.indices, a.values, xl, epi, 0, sm);
+			const double sum = block_sum(epi.acc, red);
+			if (threadIdx.x == 0) {
+				a.own[t] = sum;
+				const int64_t t0 = a.seg_tile[s], t1 = a.seg_tile[s + 1];
+				if (inst_arrive(in, t1 - t0)) {
+					const double beta = sum_tiles(a.own, a.span, t0, t1);
+					in->alpha = in->sigma / beta;
+				}
+			}
+		}
+		if (!grid_sync(a.gs)) return;
+		// phase B: the rows owned by each active tile
+		for (int64_t t = blockIdx.x; t < nt; t += G) {
+			const int32_t s = a.tile_seg[t];
+			BcgInst *in = a.inst + s;
+			if (((volatile int32_t *) &in->done)[0]) continue;
+			const double alpha = ((volatile double *) &in->alpha)[0];
+			double part = 0.0;
+			for (int64_t i = a.mt.tile_row[t] + threadIdx.x; i < a.mt.tile_row[t + 1];
+				 i += blockDim.x) {
+				a.x[i] = a.x[i] + alpha * __ldcg(u_new + i);
+				const double ri = __ldcg(a.r + i) - alpha * __ldcg(a.temp + i);
+				a.r[i] = ri;
+				part += ri * ri;
+			}
+			part = block_sum(part, red);
+			if (threadIdx.x == 0) {
+				a.own[t] = part;
+				const int64_t t0 = a.seg_tile[s], t1 = a.seg_tile[s + 1];
+				if (inst_arrive(in, t1 - t0)) {
+					const double rr = sum_tiles(a.own, nullptr, t0, t1);
+					in->rr = rr;
+					in->iterations = iter;
+					if (sqrt(rr) < in->tol_abs || iter >= a.max_iter) {
+						in->converged = sqrt(rr) < in->tol_abs ? 1 : 0;
+						__threadfence();
+						in->done = 1;
+						atomicSub(a.active, 1);
+					} else {
+						in->gamma = rr / in->sigma;
+						in->sigma = rr;
+					}
+				}
+			}
+		}
+		if (!grid_sync(a.gs)) return;
+		if (((volatile int32_t *) a.active)[0] == 0) break;
+		double *tmp = u_old;
+		u_old = u_new;
+		u_new = tmp;
+	}
+}
+
+} // namespace alpb
+
+using namespace alpb;
+
+struct alpb_batched_cg_s {
+	alpb_spmv_plan_s plan;
+	SegmentedTiles st;
+	int64_t n = 0, nnz = 0, nseg = 0;
+	const int64_t *offsets = nullptr;
+	const uint32_t *indices = nullptr;
+	const double *values = nullptr;
+	double *work = nullptr;     // r, u0, u1, temp
+	double *scratch = nullptr;  // own, span, own2, span2
+	BcgInst *inst = nullptr;
+	int32_t *active = nullptr;
+	GridSync *gs = nullptr;
+	int grid = 0;
+	cudaGraphExec_t graph = nullptr;
+	const double *g_b = nullptr;
+	double *g_x = nullptr;
+	int64_t g_max = 0;
+	double g_tol = 0;
+};
+
+__global__ void k_bcg_reset(GridSync *gs, int32_t *active, int32_t nseg) {
+	gs->count = 0;
+	gs->gen = 0;
+	gs->err = 0;
+	*active = nseg;
+}
+
+static int bcg_launch(alpb_batched_cg_s *h, const double *b, double *x, int64_t max_iter,
+	double tol, cudaStream_t s) {
+	const int64_t nt = h->plan.ntiles;
+	// kernels only (no host-memory copies), so the solve can be captured
+	k_bcg_reset<<<1, 1, 0, s>>>(h->gs, h->active, int32_t(h->nseg));
+	ALPB_LAUNCHED();
+	BcgArgs a;
+	a.mt = merge_tables(h->plan);
+	a.mt.tile_d = h->st.tile_d;
+	a.offsets = h->offsets;
+	a.indices = h->indices;
+	a.values = h->values;
+	a.b = b;
+	a.x = x;
+	a.r = h->work;
+	a.u0 = h->work + h->n;
+	a.u1 = h->work + 2 * h->n;
+	a.temp = h->work + 3 * h->n;
+	a.own = h->scratch;
+	a.span = h->scratch + nt;
+	a.own2 = h->scratch + 2 * nt;
+	a.span2 = h->scratch + 3 * nt;
+	a.tile_seg = h->st.tile_seg;
+	a.seg_tile = h->st.seg_tile;
+	a.inst = h->inst;
+	a.nseg = h->nseg;
+	a.max_iter = max_iter;
+	a.tol = tol;
+	a.active = h->active;
+	a.gs = h->gs;
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(h->grid);
+	cfg.blockDim = dim3(MP_BLOCK);
+	cfg.stream = s;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeCooperative;
+	attr[0].val.cooperative = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	ALPB_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg, a));
+	ALPB_LAUNCHED();
+	return ALPB_SUCCESS;
+}
+
+extern "C" {
+
+int alpb_batched_cg_create(alpb_batched_cg *out, int64_t n, int64_t nnz, const int64_t *row_ptr,
+	const uint32_t *col_idx, const double *values, int64_t nseg, const int64_t *seg_rows,
+	void *stream) {
+	ALPB_CHECK(out != nullptr, ALPB_ILLEGAL, "alpb_batched_cg_create: null handle");
+	*out = nullptr;
+	ALPB_CHECK(n > 0 && nnz >= 0 && nseg > 0 && nseg < (int64_t(1) << 31), ALPB_ILLEGAL,
+		"alpb_batched_cg_create: bad sizes");
+	ALPB_CHECK(n + nnz < (int64_t(1) << 31) * 1024, ALPB_OVERFLW, "alpb_batched_cg_create: too large");
+	cudaStream_t s = as_stream(stream);
+	auto *h = new alpb_batched_cg_s();
+	h->n = n;
+	h->nnz = nnz;
+	h->nseg = nseg;
+	h->offsets = row_ptr;
+	h->indices = col_idx;
+	h->values = values;
+	h->plan.m = n;
+	h->plan.nnz = nnz;
+	h->plan.offsets = row_ptr;
+	h->plan.sched = ALPB_SCHED_MERGE_PATH;
+	int rc = merge_plan_segmented(&h->plan, row_ptr, nseg, seg_rows, &h->st, s);
+	if (rc != ALPB_SUCCESS) {
+		alpb_batched_cg_destroy(h);
+		return rc;
+	}
+	const int64_t nt = h->plan.ntiles;
+	h->grid = cooperative_grid(k_batched_cg, MP_BLOCK, 0, 0);
+	if (h->grid > 2 * sm_count()) h->grid = 2 * sm_count();
+	if (h->grid <= 0) {
+		alpb_batched_cg_destroy(h);
+		set_error("alpb_batched_cg_create: no cooperative occupancy");
+		return ALPB_PANIC;
+	}
+	if (cudaMalloc(&h->work, size_t(4 * n) * 8) != cudaSuccess ||
+		cudaMalloc(&h->scratch, size_t(4 * nt) * 8) != cudaSuccess ||
+		cudaMalloc(&h->inst, size_t(nseg) * sizeof(BcgInst)) != cudaSuccess ||
+		cudaMalloc(&h->active, 8) != cudaSuccess || cudaMalloc(&h->gs, sizeof(GridSync)) != cudaSuccess) {
+		cudaGetLastError();
+		alpb_batched_cg_destroy(h);
+		set_error("alpb_batched_cg_create: out of device memory");
+		return ALPB_OUTOFMEM;
+	}
+	ALPB_CUDA(cudaMemsetAsync(h->inst, 0, size_t(nseg) * sizeof(BcgInst), s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	*out = h;
+	return ALPB_SUCCESS;
+}
+
+int alpb_batched_cg_destroy(alpb_batched_cg h) {
+	if (!h) return ALPB_SUCCESS;
+	if (h->graph) cudaGraphExecDestroy(h->graph);
+	segmented_free(&h->st);
+	cudaFree(h->plan.tile_row);
+	cudaFree(h->plan.head_first);
+	cudaFree(h->plan.tail_first);
+	cudaFree(h->plan.span_len);
+	cudaFree(h->plan.counter);
+	cudaFree(h->plan.head_val);
+	cudaFree(h->plan.tail_val);
+	cudaFree(h->plan.head_has);
+	cudaFree(h->plan.tail_has);
+	cudaFree(h->work);
+	cudaFree(h->scratch);
+	cudaFree(h->inst);
+	cudaFree(h->active);
+	cudaFree(h->gs);
+	delete h;
+	return ALPB_SUCCESS;
+}
+
+int alpb_batched_cg_solve(alpb_batched_cg h, const double *b, double *x, int64_t max_iter,
+	double tol, void *stream) {
+	ALPB_CHECK(h != nullptr, ALPB_ILLEGAL, "alpb_batched_cg_solve: null handle");
+	ALPB_CHECK(tol > 0 && max_iter > 0, ALPB_ILLEGAL, "alpb_batched_cg_solve: bad tol/max_iter");
+	return bcg_launch(h, b, x, max_iter, tol, as_stream(stream));
+}
+
+int alpb_batched_cg_capture(alpb_batched_cg h, const double *b, double *x, int64_t max_iter,
+	double tol, void *stream) {
+	ALPB_CHECK(h != nullptr, ALPB_ILLEGAL, "alpb_batched_cg_capture: null handle");
+	ALPB_CHECK(tol > 0 && max_iter > 0, ALPB_ILLEGAL, "alpb_batched_cg_capture: bad tol/max_iter");
+	cudaStream_t s = as_stream(stream);
+	cudaStream_t cs;
+	ALPB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+	cudaGraph_t g;
+	ALPB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+	int rc = bcg_launch(h, b, x, max_iter, tol, cs);
+	cudaError_t e = cudaStreamEndCapture(cs, &g);
+	cudaStreamDestroy(cs);
+	if (rc != ALPB_SUCCESS) return rc;
+	ALPB_CUDA(e);
+	if (h->graph) cudaGraphExecDestroy(h->graph);
+	h->graph = nullptr;
+	cudaError_t ie = cudaGraphInstantiate(&h->graph, g, 0);
+	cudaGraphDestroy(g);
+	ALPB_CUDA(ie);
+	(void) s;
+	return ALPB_SUCCESS;
+}
+
+int alpb_batched_cg_replay(alpb_batched_cg h, void *stream) {
+	ALPB_CHECK(h != nullptr && h->graph != nullptr, ALPB_ILLEGAL,
+		"alpb_batched_cg_replay: no captured solve");
+	ALPB_CUDA(cudaGraphLaunch(h->graph, as_stream(stream)));
+	g_launches.fetch_add(1);
+	return ALPB_SUCCESS;
+}
+
+int alpb_batched_cg_results(alpb_batched_cg h, int64_t *iterations, double *residuals,
+	int32_t *converged, void *stream) {
+	ALPB_CHECK(h != nullptr, ALPB_ILLEGAL, "alpb_batched_cg_results: null handle");
+	cudaStream_t s = as_stream(stream);
+	std::vector<BcgInst> v(size_t(h->nseg));
+	GridSync gs;
+	ALPB_CUDA(cudaMemcpyAsync(v.data(), h->inst, v.size() * sizeof(BcgInst),
+		cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaMemcpyAsync(&gs, h->gs, sizeof(GridSync), cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	ALPB_CHECK(gs.err == 0, ALPB_PANIC, "alpb_batched_cg: grid barrier timed out");
+	int all = 1;
+	for (size_t i = 0; i < v.size(); ++i) {
+		if (iterations) iterations[i] = v[i].iterations;
+		if (residuals) residuals[i] = v[i].rr;
+		if (converged) converged[i] = v[i].converged;
+		all &= v[i].converged;
+	}
+	return all ? ALPB_SUCCESS : ALPB_FAILED;
+}
+
+} // extern "C"

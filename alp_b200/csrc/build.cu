@@ -236,6 +236,68 @@ __global__ void k_poisson2d(int64_t L, double shift, int64_t *row_ptr, uint32_t 
 	}
 }
 
+// block-diagonal batch of 5-point Poisson systems
+__global__ void k_poisson2d_batch(int64_t nseg, const int64_t *Ls, const double *shifts,
+	const int64_t *seg_rows, const int64_t *seg_nnz, int64_t total, int64_t *row_ptr,
+	uint32_t *col, double *val) {
+	for (int64_t g = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < total;
+		 g += int64_t(gridDim.x) * blockDim.x) {
+		int64_t lo = 0, hi = nseg - 1;  // instance: last s with seg_rows[s] <= g
+		while (lo < hi) {
+			const int64_t mid = (lo + hi + 1) >> 1;
+			if (seg_rows[mid] <= g) lo = mid; else hi = mid - 1;
+		}
+		const int64_t s = lo, L = Ls[s], r0 = seg_rows[s], i = g - r0;
+		const int64_t x = i % L, y = i / L;
+		const int64_t py = (y > 0) + (y < L - 1);
+		int64_t start = y == 0 ? 0 : (4 * L - 2) + (y - 1) * (5 * L - 2);
+		start += x * (3 + py) - (x > 0 ? 1 : 0);
+		start += seg_nnz[s];
+		row_ptr[g] = start;
+		if (g == total - 1) row_ptr[total] = start + 1 + (x > 0) + (x < L - 1) + py;
+		int64_t p = start;
+		if (y > 0) { col[p] = uint32_t(g - L); val[p++] = -1.0; }
+		if (x > 0) { col[p] = uint32_t(g - 1); val[p++] = -1.0; }
+		col[p] = uint32_t(g); val[p++] = 4.0 + shifts[s];
+		if (x < L - 1) { col[p] = uint32_t(g + 1); val[p++] = -1.0; }
+		if (y < L - 1) { col[p] = uint32_t(g + L); val[p++] = -1.0; }
+	}
+}
+
+// Symmetric, strictly diagonally dominant values on a CRS pattern: the
+// off-diagonal (i, j) takes -(lo + (hi - lo) u) with u hashed from the
+// unordered pair, so A = A^T; the diagonal takes factor * sum_j |a_ij|.
+__global__ void k_sym_dd_values(const int64_t *row_ptr, const uint32_t *col, int64_t m,
+	uint64_t seed, double lo, double hi, double factor, double *val) {
+	const int lane = threadIdx.x & 31;
+	for (int64_t i = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; i < m;
+		 i += (int64_t(gridDim.x) * blockDim.x) >> 5) {
+		double sum = 0.0;
+		for (int64_t k = row_ptr[i] + lane; k < row_ptr[i + 1]; k += 32) {
+			const uint64_t j = col[k];
+			if (int64_t(j) == i) continue;
+			const uint64_t a = uint64_t(i) < j ? uint64_t(i) : j, b = uint64_t(i) < j ? j : uint64_t(i);
+			const double v = -(lo + (hi - lo) * u01(hash3(seed, (a << 32) | b, 0x5e11ull)));
+			val[k] = v;
+			sum += -v;
+		}
+		for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+		sum = __shfl_sync(0xffffffffu, sum, 0);
+		for (int64_t k = row_ptr[i] + lane; k < row_ptr[i + 1]; k += 32)
+			if (int64_t(col[k]) == i) val[k] = factor * sum;
+	}
+}
+
+// Box-Muller (Box & Muller, Ann. Math. Statist. 29, 1958) on two hash draws
+__global__ void k_gen_normal(double *out, int64_t n, uint64_t seed, uint64_t sid) {
+	for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n;
+		 k += int64_t(gridDim.x) * blockDim.x) {
+		const double u1 = 1.0 - u01(hash3(seed, sid, uint64_t(2 * k)));  // (0, 1]
+		const double u2 = u01(hash3(seed, sid, uint64_t(2 * k + 1)));
+		out[k] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+	}
+}
+
 } // namespace alpb
 
 using namespace alpb;
@@ -456,6 +518,35 @@ int alpb_gen_stencil_crs(int dims, const int64_t *sizes, double diag, double off
 	}
 	k_stencil_fill<<<grid_for(m, 256), 256, 0, s>>>(g, m, row_ptr, diag, off, ref_order, col_idx,
 		values);
+	ALPB_LAUNCHED();
+	return ALPB_SUCCESS;
+}
+
+int alpb_gen_poisson2d_batch(int64_t nseg, const int64_t *L, const double *shift,
+	const int64_t *seg_rows, const int64_t *seg_nnz, int64_t total_rows, int64_t *row_ptr,
+	uint32_t *col_idx, double *values, void *stream) {
+	ALPB_CHECK(nseg > 0 && total_rows > 0, ALPB_ILLEGAL, "alpb_gen_poisson2d_batch: empty batch");
+	ALPB_CHECK(total_rows <= int64_t(UINT32_MAX), ALPB_OVERFLW,
+		"alpb_gen_poisson2d_batch: too many rows for uint32 indices");
+	k_poisson2d_batch<<<grid_for(total_rows, 256), 256, 0, as_stream(stream)>>>(nseg, L, shift,
+		seg_rows, seg_nnz, total_rows, row_ptr, col_idx, values);
+	ALPB_LAUNCHED();
+	return ALPB_SUCCESS;
+}
+
+int alpb_gen_sym_dd_values(const int64_t *row_ptr, const uint32_t *col_idx, int64_t m,
+	uint64_t seed, double lo, double hi, double diag_factor, double *values, void *stream) {
+	ALPB_CHECK(m >= 0 && hi >= lo, ALPB_ILLEGAL, "alpb_gen_sym_dd_values: bad arguments");
+	if (m == 0) return ALPB_SUCCESS;
+	k_sym_dd_values<<<grid_for(m * 32, 256), 256, 0, as_stream(stream)>>>(row_ptr, col_idx, m, seed,
+		lo, hi, diag_factor, values);
+	ALPB_LAUNCHED();
+	return ALPB_SUCCESS;
+}
+
+int alpb_gen_normal(double *out, int64_t count, uint64_t seed, uint64_t sid, void *stream) {
+	if (count <= 0) return ALPB_SUCCESS;
+	k_gen_normal<<<grid_for(count, 256), 256, 0, as_stream(stream)>>>(out, count, seed, sid);
 	ALPB_LAUNCHED();
 	return ALPB_SUCCESS;
 }

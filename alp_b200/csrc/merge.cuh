@@ -31,6 +31,9 @@ struct MergeTables {
 	uint64_t *tail_val;        // [ntiles] partial of the tail row
 	uint8_t *head_has;
 	uint8_t *tail_has;
+	// [ntiles+1] first diagonal of each tile when tiles are cut per segment
+	// (batched solves: no tile straddles two instances); null: t * MP_TILE
+	const int64_t *tile_d = nullptr;
 };
 
 template <class T>
@@ -94,8 +97,15 @@ __device__ __forceinline__ void merge_tile(int64_t t, const MergeTables &mt,
 	const int tid = threadIdx.x;
 	const int64_t m = mt.m, nnz = mt.nnz;
 	const int64_t i0 = mt.tile_row[t], i1 = mt.tile_row[t + 1];
-	int64_t d0 = t * MP_TILE, d1 = d0 + MP_TILE;
-	if (d1 > m + nnz) d1 = m + nnz;
+	int64_t d0, d1;
+	if (mt.tile_d) {
+		d0 = mt.tile_d[t];
+		d1 = mt.tile_d[t + 1];
+	} else {
+		d0 = t * MP_TILE;
+		d1 = d0 + MP_TILE;
+		if (d1 > m + nnz) d1 = m + nnz;
+	}
 	const int64_t j0 = d0 - i0, j1 = d1 - i1;
 	const int nrows = int(i1 - i0);
 	const int nnzt = int(j1 - j0);
@@ -220,8 +230,27 @@ struct PlainX {
 	__device__ __forceinline__ T operator()(uint32_t j) const { return __ldg(x + j); }
 };
 
-// Host side: build the spanning-row tables of a plan (alpb_spmv_plan_s).
-int merge_tables_build(alpb_spmv_plan_s *p, cudaStream_t s);
+// Table kernels (spmv.cu): tile starts by merge-path search, then the
+// spanning-row tables.
+__global__ void k_merge_tiles(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
+	int64_t *tile_row);
+__global__ void k_merge_tables(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
+	const int64_t *tile_row, int64_t *head_first, int64_t *tail_first, int32_t *span_len);
+
+// Segmented tables (batched solves): tiles are cut at segment boundaries.
+struct SegmentedTiles {
+	int64_t nseg = 0;
+	int64_t *seg_rows = nullptr;  // [nseg+1] first row of each segment (device)
+	int64_t *seg_tile = nullptr;  // [nseg+1] first tile of each segment (device)
+	int64_t *tile_d = nullptr;    // [ntiles+1]
+	int32_t *tile_seg = nullptr;  // [ntiles] segment of each tile
+};
+// Build a plan whose tiles never straddle segments (seg_rows on the device,
+// nseg+1 entries, ascending from 0 to m).  Fills p's merge tables and `st`.
+int merge_plan_segmented(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t nseg,
+	const int64_t *seg_rows, SegmentedTiles *st, cudaStream_t s);
+void segmented_free(SegmentedTiles *st);
+
 MergeTables merge_tables(const alpb_spmv_plan_s &p);
 
 } // namespace alpb

@@ -84,6 +84,36 @@ int alpb_malloc(void **ptr, size_t bytes) {
 	return ALPB_SUCCESS;
 }
 
+int alpb_malloc_managed(void **ptr, size_t bytes) {
+	ALPB_CHECK(ptr != nullptr, ALPB_ILLEGAL, "alpb_malloc_managed: null out pointer");
+	*ptr = nullptr;
+	if (bytes == 0) return ALPB_SUCCESS;
+	bytes = (bytes + 255) & ~size_t(255);
+	cudaError_t e = cudaMallocManaged(ptr, bytes, cudaMemAttachGlobal);
+	if (e == cudaErrorMemoryAllocation) {
+		cudaGetLastError();
+		set_error("alpb_malloc_managed: out of memory for %zu bytes", bytes);
+		return ALPB_OUTOFMEM;
+	}
+	ALPB_CUDA(e);
+	return ALPB_SUCCESS;
+}
+
+int alpb_prefetch(const void *ptr, size_t bytes, int to_device, void *stream) {
+	if (!ptr || bytes == 0) return ALPB_SUCCESS;
+	int dev = 0;
+	ALPB_CUDA(cudaGetDevice(&dev));
+	cudaMemLocation loc;
+	loc.type = to_device ? cudaMemLocationTypeDevice : cudaMemLocationTypeHost;
+	loc.id = to_device ? dev : 0;
+	cudaError_t e = cudaMemPrefetchAsync(ptr, bytes, loc, 0, as_stream(stream));
+	if (e != cudaSuccess) {
+		// prefetching is a hint: ignore devices without managed-memory support
+		cudaGetLastError();
+	}
+	return ALPB_SUCCESS;
+}
+
 int alpb_free(void *ptr) {
 	if (ptr) ALPB_CUDA(cudaFree(ptr));
 	return ALPB_SUCCESS;

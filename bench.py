@@ -1,0 +1,452 @@
+#!/usr/bin/env python
+"""Benchmark of the ALP/GraphBLAS hot path on B200.
+
+Headline workload: FP64 plus-times grb::mxv on an R-MAT graph of scale 22
+(4,194,304 vertices, edge factor 16, a/b/c/d = .57/.19/.19/.05, seeded,
+duplicates merged, edge weights U(0,1)), dense x ~ U(0,1), y accumulated.
+One step = one product u += A x over the whole matrix.
+
+value   algorithmic GB/s = (12 nnz + 8 (m+1) + 8 n + 16 m) / step time, inputs
+        resident in HBM (the matrix, 0.8 GB, exceeds the 126 MB L2, so no
+        flush is needed between steps; x stays L2-resident by design).
+e2e     the same metric through the C-ABI with host buffers: each step copies
+        x from pinned host memory, runs alpb_mxv, copies u back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference runs the unmodified ALP reference_omp backend (compiled
+from the reference sources into oracle/_ref) on the host cores, on the same
+workload, metric and unit.  Under torchrun every rank runs an independent
+replica (scaling "weak"); times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = ("mxv GB/s vs HBM peak; batched CG solves/s & adjoint grads/s vs plain, 1 B200")
+SCALE = 22
+EDGE_FACTOR = 16
+SEED = 42
+
+
+def algorithmic_bytes(m: int, n: int, nnz: int, val_bytes: int = 8, vec_bytes: int = 8) -> int:
+    """Bytes one mxv must move at least: values + indices once, offsets,
+    x once, u read + written."""
+    return nnz * (val_bytes + 4) + (m + 1) * 8 + n * vec_bytes + 2 * m * vec_bytes
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(kernel_tag: str):
+    """DRAM bytes per launch recorded by the ncu summary of the kernel
+    (profiles/<tag>.md, line `traffic_bytes_per_launch: N`), else None."""
+    f = ROOT / "profiles" / f"{kernel_tag}.md"
+    if not f.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> list[dict]:
+        if self.proc is None:
+            return []
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = []
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append({"sm": float(parts[1]), "sm_max": float(parts[2]),
+                             "power": float(parts[3]) if parts[3] not in ("[N/A]", "") else None,
+                             "hw_slowdown": parts[5], "hw_thermal": parts[6],
+                             "sw_thermal": parts[7], "sw_power_cap": parts[8]})
+            except ValueError:
+                continue
+        return rows
+
+    @staticmethod
+    def summary(rows: list[dict]) -> dict:
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        load = [r for r in rows if r["power"] is None or r["power"] > 300] or rows
+        reasons = set()
+        for r in load:
+            if r["hw_slowdown"] == "Active":
+                reasons.add("hw_slowdown")
+            if r["hw_thermal"] == "Active":
+                reasons.add("hw_thermal_slowdown")
+            if r["sw_thermal"] == "Active":
+                reasons.add("sw_thermal_slowdown")
+            if r["sw_power_cap"] == "Active":
+                reasons.add("sw_power_cap")
+        return {"sm_mhz": statistics.median(r["sm"] for r in load),
+                "sm_max_mhz": max(r["sm_max"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(load)}
+
+
+# ------------------------------------------------------------------ GPU arm --
+def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+
+    torch.cuda.set_device(local_rank)
+    abi.call("alpb_init", local_rank)
+    stream = torch.cuda.current_stream()
+    sp = dev.stream_ptr(stream)
+
+    A = dev.rmat(args.scale, EDGE_FACTOR, seed=SEED, vtype=abi.FP64)
+    x = dev.gen_values(A.n, abi.FP64, seed=SEED + 7)
+    u = torch.zeros(A.m, dtype=torch.float64, device="cuda")
+    plan = dev.Plan(A, sched=abi.SCHED_AUTO)
+    plan.autotune(abi.RING_PLUS_TIMES_F64, x, u)
+    sched, vw, tiles = plan.info()
+    nbytes = algorithmic_bytes(A.m, A.n, A.nnz)
+
+    def step():
+        dev.mxv(abi.RING_PLUS_TIMES_F64, A, u, x, plan=plan, stream=stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    l0 = abi.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    barrier()
+    launches = abi.launches() - l0
+    ms = e0.elapsed_time(e1) / args.steps
+    # keep the GPU under the same load long enough for the clock sampler
+    t_hold = time.time()
+    while time.time() - t_hold < 1.0:
+        for _ in range(50):
+            step()
+        torch.cuda.synchronize()
+    clock_rows = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nbytes / (ms * 1e-3) / 1e9
+
+    # end to end through the C-ABI with host buffers
+    hx = torch.empty(A.n, dtype=torch.float64, pin_memory=True)
+    hx.copy_(x.cpu())
+    hu = torch.zeros(A.m, dtype=torch.float64, pin_memory=True)
+    dx = torch.empty_like(x)
+
+    def e2e_step():
+        abi.call("alpb_memcpy_h2d", dev.ptr(dx), C.c_void_p(hx.data_ptr()), A.n * 8, sp)
+        dev.mxv(abi.RING_PLUS_TIMES_F64, A, u, dx, plan=plan, stream=stream)
+        abi.call("alpb_memcpy_d2h", C.c_void_p(hu.data_ptr()), dev.ptr(u), A.m * 8, sp)
+
+    for _ in range(max(3, args.warmup)):
+        e2e_step()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * nbytes / (e2e_ms * 1e-3) / 1e9
+
+    peaks = measured_peaks()
+    kernel_tag = (f"spmv_merge_rmat{args.scale}" if sched == abi.SCHED_MERGE_PATH
+                  else f"spmv_vector_rmat{args.scale}")
+    traffic = profiled_traffic(kernel_tag)
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    extra = {}
+    if rank == 0 and not args.no_extra:
+        extra = extra_workloads(args, A, plan)
+    result = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded R-MAT, counter-based hash)",
+        "config": {"workload": f"mxv FP64 plus-times, R-MAT scale {args.scale}", "m": A.m, "n": A.n,
+                   "nnz": A.nnz, "edge_factor": EDGE_FACTOR, "rmat_abcd": [0.57, 0.19, 0.19, 0.05],
+                   "seed": SEED, "schedule": {1: "merge_path", 2: "vector"}[sched],
+                   "vector_width": vw, "tiles": tiles, "bytes_per_step": nbytes,
+                   "l2": "inputs larger than L2 (matrix 0.8 GB); no flush",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4),
+                     "peak_source": peaks["source"],
+                     "traffic": traffic,
+                     "kernel": "k_spmv_merge<RingPlusTimesF64>" if sched == 1
+                     else f"k_spmv_vector_dense<RingPlusTimesF64,{vw}>"},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": A.n * 8,
+                "d2h_bytes_per_step": A.m * 8, "ms_per_step": round(e2e_ms, 5)},
+        "gpu_launches": int(launches),
+        "clocks": ClockSampler.summary(clock_rows),
+    }
+    if extra:
+        result["extra"] = extra
+    return result
+
+
+def timed(fn, reps: int, stream):
+    import torch
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def extra_workloads(args, A, plan) -> dict:
+    """Secondary workloads of the same sweep, timed the same way (not part of
+    `value`): boolean lor/land with a 50% dense output mask, int32 min-plus,
+    simple_pagerank on the scale-22 pattern, CG on the 27-point 32^3 grid."""
+    import ctypes as C
+    import torch
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+    stream = torch.cuda.current_stream()
+    out = {}
+    # boolean lor/land, value mask with 50% true, dense: the reference reads a
+    # non-inverted mask on its CRS gather by structure, so every row runs
+    Ab = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices, None, abi.VOID)
+    xb = dev.gen_values(A.n, abi.BOOL, seed=11, p=0.5)
+    mk = dev.gen_values(A.m, abi.BOOL, seed=12, p=0.5)
+    ub = torch.zeros(A.m, dtype=torch.uint8, device="cuda")
+    pb = dev.Plan(Ab, sched=abi.SCHED_MERGE_PATH)
+    ms = timed(lambda: dev.mxv(abi.RING_LOR_LAND_BOOL, Ab, ub, xb, u_mask=mk,
+                               u_mask_count=A.m, plan=pb), 20, stream)
+    nb = A.nnz * 4 + (A.m + 1) * 8 + A.m + A.n + 2 * A.m
+    out["mxv_lor_land_masked50"] = {"ms": round(ms, 4), "GB/s": round(nb / ms / 1e6, 1),
+                                    "bytes": nb, "matrix": "pattern (void)"}
+    # int32 min-plus, weights U{1..100}
+    Ai = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices,
+                 torch.empty(A.nnz, dtype=torch.int32, device="cuda"), abi.INT32)
+    abi.call("alpb_gen_edge_values", dev.ptr(Ai.values), abi.INT32, dev.ptr(A.offsets),
+             dev.ptr(A.indices), A.m, A.nnz, SEED + 1, 1, 100, dev.stream_ptr())
+    xi = dev.gen_values(A.n, abi.INT32, seed=13, lo=0, hi=1000)
+    ui = torch.full((A.m,), 2**31 - 1, dtype=torch.int32, device="cuda")
+    ms = timed(lambda: dev.mxv(abi.RING_MIN_PLUS_I32, Ai, ui, xi, plan=pb), 20, stream)
+    nb = algorithmic_bytes(A.m, A.n, A.nnz, 4, 4)
+    out["mxv_min_plus_i32"] = {"ms": round(ms, 4), "GB/s": round(nb / ms / 1e6, 1), "bytes": nb}
+    del Ai, xi, ui
+    # simple_pagerank, unit weights (column-stochastic after the out-degree scaling)
+    L = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices,
+                torch.ones(A.nnz, dtype=torch.float64, device="cuda"), abi.FP64)
+    LT = dev.transpose(L)
+    pr = torch.zeros(A.m, dtype=torch.float64, device="cuda")
+    it, res = C.c_int64(), C.c_double()
+    torch.cuda.synchronize()
+    t0 = time.time()
+    rc = abi.lib().alpb_pagerank(L.m, dev.ptr(L.offsets), dev.ptr(L.indices), dev.ptr(L.values),
+                                 dev.ptr(LT.offsets), dev.ptr(LT.indices), dev.ptr(LT.values),
+                                 dev.ptr(pr), 0, 0.85, 1e-9, 1000, C.byref(it), C.byref(res),
+                                 dev.stream_ptr())
+    torch.cuda.synchronize()
+    t = time.time() - t0
+    per_iter = (A.nnz * 12 + (A.n + 1) * 8 + 6 * A.n * 8)
+    out["pagerank_rmat22"] = {"rc": rc, "iterations": it.value, "residual": res.value,
+                              "ms_total": round(t * 1e3, 2),
+                              "ms_per_iter": round(t * 1e3 / max(it.value, 1), 4),
+                              "GB/s": round(per_iter * it.value / t / 1e9, 1)}
+    del L, LT, pr
+    # plain CG, 27-point 32^3
+    S = dev.stencil((32, 32, 32), 26.0, -1.0)
+    ones = torch.ones(S.n, dtype=torch.float64, device="cuda")
+    b = torch.zeros_like(ones)
+    dev.mxv(abi.RING_PLUS_TIMES_F64, S, b, ones)
+    ps = dev.Plan(S, sched=abi.SCHED_MERGE_PATH)
+    x = torch.zeros_like(b)
+
+    def cg():
+        x.zero_()
+        abi.lib().alpb_cg_solve(S.m, dev.ptr(S.offsets), dev.ptr(S.indices), dev.ptr(S.values),
+                                dev.ptr(b), dev.ptr(x), 500, 1e-10, C.byref(it), C.byref(res),
+                                None, ps.h, dev.stream_ptr())
+    cg()
+    t0 = time.time()
+    for _ in range(5):
+        cg()
+    torch.cuda.synchronize()
+    t = (time.time() - t0) / 5
+    out["cg_27pt_32"] = {"iterations": it.value, "residual": res.value,
+                         "ms_per_solve": round(t * 1e3, 3),
+                         "err_vs_ones_inf": float((x - 1).abs().max().item())}
+    return out
+
+
+# ------------------------------------------------------------ reference arm --
+def reference_arm(args) -> dict:
+    """The unmodified reference_omp backend on the host cores: grb::mxv on the
+    same R-MAT scale-22 matrix (generated by the seeded C generator that the
+    device generator mirrors bit for bit)."""
+    from oracle.oracle import FP64, REF_OMP_SO, Reference, Restatement, crs_to_coo
+    if not REF_OMP_SO.exists():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libalp_ref_omp.so not built"}
+    os.environ.setdefault("OMP_PROC_BIND", "true")
+    R = Restatement()
+    rp, col, vals = R.rmat(SCALE, EDGE_FACTOR, seed=SEED, vtype=FP64)
+    n = len(rp) - 1
+    I, J = crs_to_coo(rp, col)
+    x = R.values(n, FP64, SEED + 7)
+    u = np.zeros(n)
+    ref = Reference(omp=True)
+    nbytes = algorithmic_bytes(n, n, len(col))
+    # one call builds the reference matrix and runs warmup + timed steps
+    reps = args.warmup + args.steps
+    ms_list = []
+    rc, ms = ref.mxv(0, 0, 0, n, n, I, J, vals, u, None, x, reps=reps)
+    if rc != 0:
+        return {"impl": "reference", "unavailable": f"reference mxv returned rc={rc}"}
+    value = nbytes / (ms * 1e-3) / 1e9
+    cores = ref.threads()
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "GB/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded R-MAT, counter-based hash)",
+        "config": {"workload": f"mxv FP64 plus-times, R-MAT scale {SCALE}", "m": n, "n": n,
+                   "nnz": int(len(col)), "bytes_per_step": nbytes},
+        "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"grb::mxv (reference_omp, {cores} threads) on the full "
+                                   f"R-MAT scale-{SCALE} matrix, mean of {reps} calls"},
+        "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def cpu_baseline_sample() -> dict | None:
+    """reference_omp on a bounded sample of the workload: the same generator
+    at scale 20 (1/4 of the rows), all host threads."""
+    try:
+        from oracle.oracle import FP64, REF_OMP_SO, Reference, Restatement, crs_to_coo
+        if not REF_OMP_SO.exists():
+            return None
+        os.environ.setdefault("OMP_PROC_BIND", "true")
+        R = Restatement()
+        rp, col, vals = R.rmat(20, EDGE_FACTOR, seed=SEED, vtype=FP64)
+        n = len(rp) - 1
+        I, J = crs_to_coo(rp, col)
+        x = R.values(n, FP64, SEED + 7)
+        u = np.zeros(n)
+        ref = Reference(omp=True)
+        rc, ms = ref.mxv(0, 0, 0, n, n, I, J, vals, u, None, x, reps=20)
+        if rc != 0:
+            return None
+        nb = algorithmic_bytes(n, n, len(col))
+        return {"value": round(nb / (ms * 1e-3) / 1e9, 2), "unit": "GB/s", "cores": ref.threads(),
+                "kind": "reference",
+                "sample": f"grb::mxv (reference_omp) on R-MAT scale 20 ({len(col)} nnz), "
+                          "same generator and seed, mean of 20 calls"}
+    except Exception as e:  # a missing checker must not break the GPU line
+        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"failed: {e}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--scale", type=int, default=SCALE,
+                    help="R-MAT scale (22 is the benchmark; smaller for profiling captures)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = gpu_arm(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        res["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

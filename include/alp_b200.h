@@ -127,6 +127,11 @@ ALPB_API int64_t alpb_launch_count(void);
  * reference/alloc.hpp allocation modes); bytes are rounded up to 256 B. */
 ALPB_API int alpb_malloc(void **ptr, size_t bytes);
 ALPB_API int alpb_free(void *ptr);
+/* managed (unified) memory for containers whose values the host also reads
+ * (grb::Vector of the C++ backend: raw(), operator[], iterators); prefetch
+ * moves the pages to the device (to_device != 0) or the host. */
+ALPB_API int alpb_malloc_managed(void **ptr, size_t bytes);
+ALPB_API int alpb_prefetch(const void *ptr, size_t bytes, int to_device, void *stream);
 ALPB_API int alpb_memcpy_h2d(void *dst, const void *src, size_t bytes, void *stream);
 ALPB_API int alpb_memcpy_d2h(void *dst, const void *src, size_t bytes, void *stream);
 ALPB_API int alpb_memcpy_d2d(void *dst, const void *src, size_t bytes, void *stream);
@@ -184,9 +189,24 @@ ALPB_API int alpb_crs_transpose(int64_t m, int64_t n, int64_t nnz,
 ALPB_API int alpb_gen_stencil_crs(int dims, const int64_t *sizes, double diag,
 	double off, int ref_order, int64_t *row_ptr, uint32_t *col_idx, double *values,
 	int64_t *nnz, void *stream);
-/* 2-D 5-point Poisson on an L x L grid (Dirichlet), diag 4+shift, off -1. */
+/* 2-D 5-point Poisson on an L x L grid (Dirichlet), diag 4+shift, off -1;
+ * columns ascending in each row. */
 ALPB_API int alpb_gen_poisson2d_crs(int64_t L, double shift, int64_t *row_ptr,
 	uint32_t *col_idx, double *values, void *stream);
+/* nseg such systems as one block-diagonal CRS: instance i has side L[i] and
+ * shift shift[i] (device arrays), rows [seg_rows[i], seg_rows[i+1]) and
+ * nonzeroes from seg_nnz[i] (device arrays the caller fills: prefix sums of
+ * L^2 and 5L^2-4L).  row_ptr has seg_rows[nseg]+1 entries. */
+ALPB_API int alpb_gen_poisson2d_batch(int64_t nseg, const int64_t *L, const double *shift,
+	const int64_t *seg_rows, const int64_t *seg_nnz, int64_t total_rows, int64_t *row_ptr,
+	uint32_t *col_idx, double *values, void *stream);
+/* Symmetric strictly diagonally dominant values on a symmetric CRS pattern:
+ * a_ij = a_ji = -U(lo, hi) keyed by the pair {i, j}, a_ii = factor * sum |a_ij|. */
+ALPB_API int alpb_gen_sym_dd_values(const int64_t *row_ptr, const uint32_t *col_idx, int64_t m,
+	uint64_t seed, double lo, double hi, double diag_factor, double *values, void *stream);
+/* standard normal samples (Box-Muller on two hash draws per sample) */
+ALPB_API int alpb_gen_normal(double *out, int64_t count, uint64_t seed, uint64_t stream_id,
+	void *stream);
 
 /* ======================================================================
  * SpMV (replaces internal::vxm_generic + vxm_inner_kernel_gather,
@@ -284,6 +304,42 @@ ALPB_API int alpb_ewise_muladd_f64(double *out, int add_op, int mul_op, int64_t 
 /* foldl: x[i] = x[i] op y[i] (y NULL -> scalar sy); foldr: y[i] = x op y[i]. */
 ALPB_API int alpb_foldl_f64(double *x, int op, int64_t n, const double *y, double sy,
 	void *stream);
+/* Generic element-wise primitive with ALP's sparse semantics (the device side
+ * of grb::set, the vector forms of grb::foldl / grb::foldr, grb::eWiseApply
+ * and grb::eWiseMul / eWiseMulAdd; reference/blas1.hpp, reference/io.hpp).
+ * Operands: z (in/out), x, y as (values, type, assigned flags or NULL when
+ * dense); x == NULL or y == NULL means the scalar alpha or beta.  An optional
+ * mask (masked != 0) restricts the indices, as utils::interpretMask reads it
+ * under descr.  Kinds:
+ *   SET    z_i = x_i wherever x_i exists
+ *   FOLDL  z_i = z_i op x_i where both exist; a monoid also folds into absent
+ *          z_i from its identity
+ *   FOLDR  z_i = x_i op z_i, likewise
+ *   APPLY  z = x op y: an operator on the intersection, a monoid on the union
+ *          (absent operand = identity); z's old entries are dropped
+ *   MULADD z_i = z_i (op) (x_i (mul_op) y_i) where x_i and y_i exist
+ * Values are computed in double and cast to the output type. */
+#define ALPB_VEC_SET 0
+#define ALPB_VEC_FOLDL 1
+#define ALPB_VEC_FOLDR 2
+#define ALPB_VEC_APPLY 3
+#define ALPB_VEC_MULADD 4
+ALPB_API int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_op,
+	uint32_t descr, int64_t n, void *z, int z_type, uint8_t *z_assigned, int64_t *z_nnz,
+	const void *mask, const uint8_t *mask_assigned, int mask_type, int masked,
+	const void *x, int x_type, const uint8_t *x_assigned, double alpha,
+	const void *y, int y_type, const uint8_t *y_assigned, double beta, void *stream);
+/* *result = *result (+) [(+)_i x_i (*) y_i] over the indices where x, y (y may
+ * be NULL: a plain fold of x) and the mask are present; values of any type
+ * code, computed in double; identity is the additive monoid's.  Covers
+ * grb::dot and the vector-to-scalar grb::foldl / foldr (masked or not). */
+ALPB_API int alpb_vec_reduce(double *result, int add_op, double identity, int mul_op,
+	uint32_t descr, int64_t n, const void *x, int x_type, const uint8_t *x_assigned,
+	const void *y, int y_type, const uint8_t *y_assigned, const void *mask,
+	const uint8_t *mask_assigned, int mask_type, int masked, void *stream);
+/* number of assigned entries (synchronises). */
+ALPB_API int alpb_count_assigned(const uint8_t *assigned, int64_t n, int64_t *count,
+	void *stream);
 /* reduce a dense vector to a host scalar: *result = *result op fold(x). */
 ALPB_API int alpb_reduce_f64(double *result, int op, int64_t n, const double *x,
 	const uint8_t *assigned, void *stream);
@@ -315,6 +371,61 @@ ALPB_API int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr,
 	const int64_t *ccs_col_ptr, const uint32_t *ccs_row_idx, const double *ccs_values,
 	double *pr, int init_given, double alpha, double conv, int64_t max_iter,
 	int64_t *iterations, double *residual, void *stream);
+
+/* ======================================================================
+ * Adjoint gradients of a CG solve (implicit function theorem; no iterate is
+ * stored).  No counterpart exists in the reference: the reference checks
+ * them by assembling -lambda_i x_j on the host after a reference CG on A^T.
+ * ====================================================================== */
+/* out[k] = alpha * lam[row(k)] * x[col(k)] over the stored pattern (CRS
+ * order): the pattern-masked SDDMM.  plan may be NULL. */
+ALPB_API int alpb_sddmm(alpb_spmv_plan plan, int64_t m, int64_t nnz, const int64_t *offsets,
+	const uint32_t *indices, const double *lam, const double *x, double alpha, double *out,
+	void *stream);
+/* lambda = A^{-T} g by CG on A's CCS, then grad_values[k] = -lambda_i x_j on A's
+ * CRS pattern (grad_values may be NULL).  dL/db = lambda. */
+ALPB_API int alpb_cg_adjoint(int64_t n, const int64_t *row_ptr, const uint32_t *col_idx,
+	const double *values, const int64_t *ccs_col_ptr, const uint32_t *ccs_row_idx,
+	const double *ccs_values, const double *x, const double *g, double *lambda,
+	double *grad_values, int64_t max_iter, double tol, int64_t *iterations, double *residual,
+	alpb_spmv_plan plan_crs, alpb_spmv_plan plan_ccs, void *stream);
+/* Loss L = 0.5 ||x - x_target||^2 of x = A^{-1} b: forward CG from x = 0, then
+ * the adjoint; returns L, x, lambda = dL/db and dL/dA on the pattern.  work:
+ * n + 1 doubles. */
+ALPB_API int alpb_cg_grad(int64_t n, const int64_t *row_ptr, const uint32_t *col_idx,
+	const double *values, const int64_t *ccs_col_ptr, const uint32_t *ccs_row_idx,
+	const double *ccs_values, const double *b, const double *x_target, double *x,
+	double *lambda, double *grad_values, double *work, int64_t max_iter, double tol,
+	double *loss, int64_t *iterations_fwd, int64_t *iterations_adj,
+	alpb_spmv_plan plan_crs, alpb_spmv_plan plan_ccs, void *stream);
+
+/* ======================================================================
+ * Batched CG: many independent SPD systems of uneven size, stored as one
+ * block-diagonal CRS (instance i owns rows [seg_rows[i], seg_rows[i+1])),
+ * solved in ONE persistent cooperative launch with per-instance convergence
+ * masks.  Each instance follows algorithms::conjugate_gradient
+ * (conjugate_gradient.hpp:191-483) with its own relative tolerance
+ * tol * ||b_i||.  No counterpart exists in the reference, which solves one
+ * system per call; this replaces calling grb::algorithms::conjugate_gradient
+ * once per instance.
+ * ====================================================================== */
+typedef struct alpb_batched_cg_s *alpb_batched_cg;
+/* Plan the batch (tiles cut per instance) and reserve its work vectors. */
+ALPB_API int alpb_batched_cg_create(alpb_batched_cg *h, int64_t n, int64_t nnz,
+	const int64_t *row_ptr, const uint32_t *col_idx, const double *values, int64_t nseg,
+	const int64_t *seg_rows, void *stream);
+ALPB_API int alpb_batched_cg_destroy(alpb_batched_cg h);
+/* One solve: x holds the initial guesses on entry (all instances). */
+ALPB_API int alpb_batched_cg_solve(alpb_batched_cg h, const double *b, double *x,
+	int64_t max_iter, double tol, void *stream);
+/* Capture one solve on (b, x) into a CUDA graph, then replay it. */
+ALPB_API int alpb_batched_cg_capture(alpb_batched_cg h, const double *b, double *x,
+	int64_t max_iter, double tol, void *stream);
+ALPB_API int alpb_batched_cg_replay(alpb_batched_cg h, void *stream);
+/* Per-instance iterations, r.r and converged flags of the last solve
+ * (synchronises); ALPB_FAILED if any instance did not converge. */
+ALPB_API int alpb_batched_cg_results(alpb_batched_cg h, int64_t *iterations,
+	double *residuals, int32_t *converged, void *stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,870 @@
+/*
+ * Level-1 primitives of the b200 backend (reference: graphblas/reference/
+ * blas1.hpp).  Every primitive runs on the device through alpb_vec_op /
+ * alpb_vec_reduce with ALP's sparse semantics and returns once the result is
+ * in place (blocking execution).  Operators and monoids are those of
+ * graphblas/ops.hpp that have a device code (internal::b200rt::op_code); any
+ * other operator, or a domain without a device type, gives UNSUPPORTED.
+ *
+ * eWiseLambda is the exception: its lambda is host code, so it runs on the
+ * host over the vectors' managed memory (no device copy of user code exists).
+ */
+#ifndef _H_GRB_B200_BLAS1
+#define _H_GRB_B200_BLAS1
+
+#include <type_traits>
+
+#include <graphblas/base/blas1.hpp>
+#include <graphblas/b200/io.hpp>
+#include <graphblas/b200/runtime.hpp>
+#include <graphblas/b200/vector.hpp>
+
+namespace grb {
+
+	namespace internal {
+		namespace b200rt {
+
+			/** Keeps a template argument out of deduction (for nullable operands). */
+			template< typename T >
+			struct nd { typedef T type; };
+
+			template< class Monoid >
+			struct monoid_code {
+				static constexpr int value = op_code< typename Monoid::Operator >::value;
+				static double identity() {
+					return static_cast< double >( Monoid().template getIdentity< double >() );
+				}
+			};
+
+			/** z <- kind(z, x, y) through alpb_vec_op; x / y may be scalars. */
+			template< Descriptor descr, typename Z, typename X, typename Y, typename M,
+				typename Coords >
+			RC vec_op( const int kind, const int op, const bool monoid, const double identity,
+				const int mul_op, Vector< Z, grb::b200, Coords > &z,
+				const Vector< M, grb::b200, typename nd< Coords >::type > * const mask,
+				const Vector< X, grb::b200, typename nd< Coords >::type > * const x, const double alpha,
+				const Vector< Y, grb::b200, typename nd< Coords >::type > * const y, const double beta
+			) {
+				const size_t n = z.b200_size();
+				if( mask && size( *mask ) > 0 && size( *mask ) != n ) { return MISMATCH; }
+				if( ( x && size( *x ) != n ) || ( y && size( *y ) != n ) ) { return MISMATCH; }
+				if( op < 0 ) { return UNSUPPORTED; }
+				if( descr & descriptors::dense ) {
+					if( nnz( z ) < n && kind != ALPB_VEC_SET && kind != ALPB_VEC_APPLY ) { return ILLEGAL; }
+					if( ( x && nnz( *x ) < n ) || ( y && nnz( *y ) < n ) ) { return ILLEGAL; }
+				}
+				const int zt = type_code< Z >::value;
+				const int xt = x ? type_code< X >::value : zt;
+				const int yt = y ? type_code< Y >::value : zt;
+				const bool masked = mask && size( *mask ) > 0;
+				const int mt = masked ? type_code< M >::value : ALPB_VOID;
+				if( zt < 0 || xt < 0 || yt < 0 || mt < 0 ) { return UNSUPPORTED; }
+				if( n == 0 ) { return SUCCESS; }
+				z.b200_device_ready();
+				if( x ) { x->b200_device_ready(); }
+				if( y ) { y->b200_device_ready(); }
+				if( masked ) { mask->b200_device_ready(); }
+				// a dense output stays dense unless eWiseApply may drop entries
+				const bool out_sparse = !z.b200_dense() || kind == ALPB_VEC_APPLY;
+				const RC rc = check( alpb_vec_op( kind, op, monoid ? 1 : 0, identity, mul_op, descr, n,
+					z.b200_values(), zt, out_sparse ? z.b200_flags() : nullptr,
+					out_sparse ? z.b200_counter() : nullptr,
+					masked ? mask->b200_values() : nullptr,
+					masked ? mask->b200_flags_or_dense() : nullptr, mt, masked ? 1 : 0,
+					x ? x->b200_values() : nullptr, xt, x ? x->b200_flags_or_dense() : nullptr, alpha,
+					y ? y->b200_values() : nullptr, yt, y ? y->b200_flags_or_dense() : nullptr, beta,
+					stream() ), "blas1" );
+				(void) alpb_stream_sync( stream() );
+				if( kind == ALPB_VEC_APPLY ) { z.b200_mark_sparse(); }
+				z.b200_refresh();
+				return rc;
+			}
+
+			/** *out (+)= reduce( x (*) y ) through alpb_vec_reduce. */
+			template< Descriptor descr, typename OutT, typename X, typename Y, typename M,
+				typename Coords >
+			RC vec_reduce( OutT &out, const int add_op, const double identity, const int mul_op,
+				const Vector< X, grb::b200, Coords > &x,
+				const Vector< Y, grb::b200, typename nd< Coords >::type > * const y,
+				const Vector< M, grb::b200, typename nd< Coords >::type > * const mask
+			) {
+				const size_t n = x.b200_size();
+				if( y && size( *y ) != n ) { return MISMATCH; }
+				const bool masked = mask && size( *mask ) > 0;
+				if( masked && size( *mask ) != n ) { return MISMATCH; }
+				if( add_op < 0 || mul_op < 0 ) { return UNSUPPORTED; }
+				if( descr & descriptors::dense ) {
+					if( nnz( x ) < n || ( y && nnz( *y ) < n ) ) { return ILLEGAL; }
+				}
+				const int xt = type_code< X >::value, yt = y ? type_code< Y >::value : xt;
+				const int mt = masked ? type_code< M >::value : ALPB_VOID;
+				if( xt < 0 || yt < 0 || mt < 0 ) { return UNSUPPORTED; }
+				if( n == 0 ) { return SUCCESS; }
+				x.b200_device_ready();
+				if( y ) { y->b200_device_ready(); }
+				if( masked ) { mask->b200_device_ready(); }
+				double r = static_cast< double >( out );
+				const RC rc = check( alpb_vec_reduce( &r, add_op, identity, mul_op, descr, n,
+					x.b200_values(), xt, x.b200_flags_or_dense(),
+					y ? y->b200_values() : nullptr, yt, y ? y->b200_flags_or_dense() : nullptr,
+					masked ? mask->b200_values() : nullptr, masked ? mask->b200_flags_or_dense() : nullptr,
+					mt, masked ? 1 : 0, stream() ), "reduce" );
+				if( rc == SUCCESS ) { out = static_cast< OutT >( r ); }
+				return rc;
+			}
+
+		}
+	}
+
+	// ------------------------------------------------------------------ dot --
+	template< Descriptor descr = descriptors::no_operation, class AddMonoid, class AnyOp,
+		typename OutputType, typename InputType1, typename InputType2, typename Coords >
+	RC dot( OutputType &z, const Vector< InputType1, b200, Coords > &x,
+		const Vector< InputType2, b200, Coords > &y, const AddMonoid &addMonoid = AddMonoid(),
+		const AnyOp &anyOp = AnyOp(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_monoid< AddMonoid >::value && grb::is_operator< AnyOp >::value,
+			void >::type * const = nullptr
+	) {
+		(void) addMonoid;
+		(void) anyOp;
+		if( phase == RESIZE ) { return size( x ) == size( y ) ? SUCCESS : MISMATCH; }
+		using namespace internal::b200rt;
+		return vec_reduce< descr, OutputType, InputType1, InputType2, bool >( z,
+			monoid_code< AddMonoid >::value, monoid_code< AddMonoid >::identity(),
+			op_code< AnyOp >::value, x, &y, nullptr );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename IOType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC dot( IOType &x, const Vector< InputType1, b200, Coords > &left,
+		const Vector< InputType2, b200, Coords > &right, const Ring &ring = Ring(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && !grb::is_object< IOType >::value &&
+			grb::is_semiring< Ring >::value, void >::type * const = nullptr
+	) {
+		return dot< descr >( x, left, right, ring.getAdditiveMonoid(),
+			ring.getMultiplicativeOperator(), phase );
+	}
+
+	// ------------------------------------------------- vector -> scalar fold --
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
+		typename InputType, typename MaskType, typename Coords >
+	RC foldl( IOType &x, const Vector< InputType, b200, Coords > &y,
+		const Vector< MaskType, b200, Coords > &mask, const Monoid &monoid = Monoid(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< IOType >::value &&
+			!grb::is_object< InputType >::value && !grb::is_object< MaskType >::value &&
+			grb::is_monoid< Monoid >::value, void >::type * const = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_reduce< descr, IOType, InputType, InputType, MaskType >( x,
+			monoid_code< Monoid >::value, monoid_code< Monoid >::identity(), ALPB_OP_LEFT_ASSIGN, y,
+			nullptr, &mask );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
+		typename InputType, typename Coords >
+	RC foldl( IOType &x, const Vector< InputType, b200, Coords > &y,
+		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< IOType >::value &&
+			!grb::is_object< InputType >::value && grb::is_monoid< Monoid >::value,
+			void >::type * const = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_reduce< descr, IOType, InputType, InputType, bool >( x,
+			monoid_code< Monoid >::value, monoid_code< Monoid >::identity(), ALPB_OP_LEFT_ASSIGN, y,
+			nullptr, nullptr );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename InputType,
+		typename IOType, typename Coords >
+	RC foldr( const Vector< InputType, b200, Coords > &x, IOType &beta,
+		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< InputType >::value &&
+			!grb::is_object< IOType >::value && grb::is_monoid< Monoid >::value,
+			void >::type * const = nullptr
+	) {
+		return foldl< descr >( beta, x, monoid, phase );
+	}
+
+	// ------------------------------------------------- scalar -> vector fold --
+	template< Descriptor descr = descriptors::no_operation, class Op, typename IOType,
+		typename InputType, typename Coords >
+	RC foldl( Vector< IOType, b200, Coords > &x, const InputType beta, const Op &op = Op(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< IOType >::value &&
+			!grb::is_object< InputType >::value && grb::is_operator< Op >::value,
+			void >::type * = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDL,
+			internal::b200rt::op_code< Op >::value, false, 0.0, 0, x, nullptr, nullptr,
+			static_cast< double >( beta ), nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
+		typename InputType, typename Coords >
+	RC foldl( Vector< IOType, b200, Coords > &x, const InputType beta,
+		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< IOType >::value &&
+			!grb::is_object< InputType >::value && grb::is_monoid< Monoid >::value,
+			void >::type * = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDL,
+			monoid_code< Monoid >::value, false, 0.0, 0, x, nullptr, nullptr,
+			static_cast< double >( beta ), nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Op, typename IOType,
+		typename MaskType, typename InputType, typename Coords >
+	RC foldl( Vector< IOType, b200, Coords > &x, const Vector< MaskType, b200, Coords > &m,
+		const InputType beta, const Op &op = Op(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< IOType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType >::value &&
+			grb::is_operator< Op >::value, void >::type * = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, IOType, IOType, IOType, MaskType >( ALPB_VEC_FOLDL,
+			internal::b200rt::op_code< Op >::value, false, 0.0, 0, x, &m, nullptr,
+			static_cast< double >( beta ), nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
+		typename InputType, typename Coords >
+	RC foldr( const InputType &alpha, Vector< IOType, b200, Coords > &y,
+		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< InputType >::value &&
+			!grb::is_object< IOType >::value && grb::is_monoid< Monoid >::value,
+			void >::type * const = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDR,
+			monoid_code< Monoid >::value, false, 0.0, 0, y, nullptr, nullptr,
+			static_cast< double >( alpha ), nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class OP, typename IOType,
+		typename InputType, typename Coords >
+	RC foldr( const InputType &alpha, Vector< IOType, b200, Coords > &y, const OP &op = OP(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< InputType >::value &&
+			!grb::is_object< IOType >::value && grb::is_operator< OP >::value,
+			void >::type * const = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDR,
+			internal::b200rt::op_code< OP >::value, false, 0.0, 0, y, nullptr, nullptr,
+			static_cast< double >( alpha ), nullptr, 0.0 );
+	}
+
+	// ------------------------------------------------- vector -> vector fold --
+	template< Descriptor descr = descriptors::no_operation, class OP, typename IOType,
+		typename InputType, typename Coords >
+	RC foldl( Vector< IOType, b200, Coords > &x, const Vector< InputType, b200, Coords > &y,
+		const OP &op = OP(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< grb::is_operator< OP >::value &&
+			!grb::is_object< IOType >::value && !grb::is_object< InputType >::value,
+			void >::type * = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, IOType, InputType, InputType, bool >( ALPB_VEC_FOLDL,
+			internal::b200rt::op_code< OP >::value, false, 0.0, 0, x, nullptr, &y, 0.0, nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
+		typename InputType, typename Coords >
+	RC foldl( Vector< IOType, b200, Coords > &x, const Vector< InputType, b200, Coords > &y,
+		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< grb::is_monoid< Monoid >::value &&
+			!grb::is_object< IOType >::value && !grb::is_object< InputType >::value,
+			void >::type * = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, IOType, InputType, InputType, bool >( ALPB_VEC_FOLDL,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, x, nullptr, &y,
+			0.0, nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class OP, typename IOType,
+		typename MaskType, typename InputType, typename Coords >
+	RC foldl( Vector< IOType, b200, Coords > &x, const Vector< MaskType, b200, Coords > &m,
+		const Vector< InputType, b200, Coords > &y, const OP &op = OP(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< grb::is_operator< OP >::value &&
+			!grb::is_object< IOType >::value && !grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType >::value, void >::type * = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, IOType, InputType, InputType, MaskType >(
+			ALPB_VEC_FOLDL, internal::b200rt::op_code< OP >::value, false, 0.0, 0, x, &m, &y, 0.0,
+			nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
+		typename MaskType, typename InputType, typename Coords >
+	RC foldl( Vector< IOType, b200, Coords > &x, const Vector< MaskType, b200, Coords > &m,
+		const Vector< InputType, b200, Coords > &y, const Monoid &monoid = Monoid(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< grb::is_monoid< Monoid >::value &&
+			!grb::is_object< IOType >::value && !grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType >::value, void >::type * = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, IOType, InputType, InputType, MaskType >( ALPB_VEC_FOLDL,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, x, &m, &y, 0.0,
+			nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class OP, typename IOType,
+		typename InputType, typename Coords >
+	RC foldr( const Vector< InputType, b200, Coords > &x, Vector< IOType, b200, Coords > &y,
+		const OP &op = OP(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< grb::is_operator< OP >::value &&
+			!grb::is_object< InputType >::value && !grb::is_object< IOType >::value,
+			void >::type * = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, IOType, InputType, InputType, bool >( ALPB_VEC_FOLDR,
+			internal::b200rt::op_code< OP >::value, false, 0.0, 0, y, nullptr, &x, 0.0, nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
+		typename InputType, typename Coords >
+	RC foldr( const Vector< InputType, b200, Coords > &x, Vector< IOType, b200, Coords > &y,
+		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< grb::is_monoid< Monoid >::value &&
+			!grb::is_object< InputType >::value && !grb::is_object< IOType >::value,
+			void >::type * = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, IOType, InputType, InputType, bool >( ALPB_VEC_FOLDR,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, y, nullptr, &x,
+			0.0, nullptr, 0.0 );
+	}
+
+	// ----------------------------------------------------------- eWiseApply --
+	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &x, const Vector< InputType2, b200, Coords > &y,
+		const OP &op = OP(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_operator< OP >::value, void >::type * const = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, OutputType, InputType1, InputType2, bool >(
+			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, nullptr, &x, 0.0,
+			&y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &x, const Vector< InputType2, b200, Coords > &y,
+		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_monoid< Monoid >::value, void >::type * const = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType1, InputType2, bool >( ALPB_VEC_APPLY,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, nullptr, &x,
+			0.0, &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &x, const InputType2 beta, const OP &op = OP(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_operator< OP >::value, void >::type * const = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, OutputType, InputType1, InputType1, bool >(
+			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, nullptr, &x, 0.0,
+			nullptr, static_cast< double >( beta ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z, const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &y, const OP &op = OP(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_operator< OP >::value, void >::type * const = nullptr
+	) {
+		(void) op;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, OutputType, InputType2, InputType2, bool >(
+			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, nullptr, nullptr,
+			static_cast< double >( alpha ), &y, 0.0 );
+	}
+
+	// ------------------------------------------------------------- eWiseMul --
+	/** z = z (+) ( alpha (*) y ) over the ring (reference/blas1.hpp:8610-9172). */
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
+		typename InputType2, typename OutputType, typename Coords >
+	RC eWiseMul( Vector< OutputType, b200, Coords > &z, const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &y, const Ring &ring = Ring(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_semiring< Ring >::value, void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType2, InputType2, bool >( ALPB_VEC_MULADD,
+			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
+			op_code< typename Ring::MultiplicativeOperator >::value, z, nullptr, nullptr,
+			static_cast< double >( alpha ), &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
+		typename InputType2, typename OutputType, typename Coords >
+	RC eWiseMul( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &x, const Vector< InputType2, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_semiring< Ring >::value, void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType1, InputType2, bool >( ALPB_VEC_MULADD,
+			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
+			op_code< typename Ring::MultiplicativeOperator >::value, z, nullptr, &x, 0.0, &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
+		typename InputType2, typename OutputType, typename Coords >
+	RC eWiseMul( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &x, const InputType2 beta,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_semiring< Ring >::value, void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType1, InputType1, bool >( ALPB_VEC_MULADD,
+			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
+			op_code< typename Ring::MultiplicativeOperator >::value, z, nullptr, &x, 0.0, nullptr,
+			static_cast< double >( beta ) );
+	}
+
+	// ---------------------------------------------------------- eWiseMulAdd --
+	namespace internal {
+		namespace b200rt {
+			/** z = z (+) (a (*) x) (+) y over the ring (reference/blas1.hpp:6347-6770):
+			 *  the product folds into z where a and x are present, then y folds in as
+			 *  a monoid (absent z entries start from the identity); a scalar y reaches
+			 *  every entry. */
+			template< Descriptor descr, class Ring, typename Z, typename A, typename X, typename Y,
+				typename M, typename Coords >
+			RC muladd( Vector< Z, grb::b200, Coords > &z,
+				const Vector< M, grb::b200, typename nd< Coords >::type > * const mask,
+				const Vector< A, grb::b200, typename nd< Coords >::type > * const a, const double alpha,
+				const Vector< X, grb::b200, typename nd< Coords >::type > * const x, const double chi,
+				const Vector< Y, grb::b200, typename nd< Coords >::type > * const y, const double gamma
+			) {
+				const int add = op_code< typename Ring::AdditiveOperator >::value;
+				const int mul = op_code< typename Ring::MultiplicativeOperator >::value;
+				const double zero = static_cast< double >( Ring().template getZero< Z >() );
+				RC rc;
+				if( !a && !x ) {
+					// both scalars: fold the constant product into every entry
+					rc = vec_op< descr, Z, Z, Z, M >( ALPB_VEC_FOLDL, add, false, zero, 0, z, mask,
+						nullptr, 0.0, nullptr, 0.0 );
+					const double p = 0.0;
+					(void) p;
+					if( rc == SUCCESS ) {
+						Vector< Z, grb::b200, Coords > c( z.b200_size() );
+						rc = set< descriptors::no_operation >( c, static_cast< Z >( alpha * chi ) );
+						if( rc == SUCCESS ) {
+							rc = vec_op< descr, Z, Z, Z, M >( ALPB_VEC_FOLDL, add, true, zero, 0, z, mask,
+								&c, 0.0, nullptr, 0.0 );
+						}
+					}
+				} else {
+					rc = vec_op< descr, Z, A, X, M >( ALPB_VEC_MULADD, add, false, zero, mul, z, mask,
+						a, alpha, x, chi );
+				}
+				if( rc != SUCCESS ) { return rc; }
+				if( y ) {
+					return vec_op< descr, Z, Y, Y, M >( ALPB_VEC_FOLDL, add, true, zero, 0, z, mask, y,
+						0.0, nullptr, 0.0 );
+				}
+				Vector< Z, grb::b200, Coords > g( z.b200_size() );
+				rc = set< descriptors::no_operation >( g, static_cast< Z >( gamma ) );
+				if( rc != SUCCESS ) { return rc; }
+				return vec_op< descr, Z, Z, Z, M >( ALPB_VEC_FOLDL, add, true, zero, 0, z, mask, &g,
+					0.0, nullptr, 0.0 );
+			}
+		}
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const InputType1 alpha,
+		const InputType2 chi,
+		const InputType3 gamma,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value &&
+			!grb::is_object< InputType3 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, OutputType, OutputType, bool >( z, nullptr,
+			nullptr, static_cast< double >( alpha ), nullptr, static_cast< double >( chi ), nullptr, static_cast< double >( gamma ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const InputType1 alpha,
+		const InputType2 chi,
+		const Vector< InputType3, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, OutputType, InputType3, bool >( z, nullptr,
+			nullptr, static_cast< double >( alpha ), nullptr, static_cast< double >( chi ), &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &x,
+		const InputType3 gamma,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType3 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, InputType2, OutputType, bool >( z, nullptr,
+			nullptr, static_cast< double >( alpha ), &x, 0.0, nullptr, static_cast< double >( gamma ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &x,
+		const Vector< InputType3, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< InputType1 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, InputType2, InputType3, bool >( z, nullptr,
+			nullptr, static_cast< double >( alpha ), &x, 0.0, &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &a,
+		const InputType2 chi,
+		const InputType3 gamma,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< InputType2 >::value &&
+			!grb::is_object< InputType3 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, OutputType, OutputType, bool >( z, nullptr,
+			&a, 0.0, nullptr, static_cast< double >( chi ), nullptr, static_cast< double >( gamma ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &a,
+		const InputType2 chi,
+		const Vector< InputType3, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< InputType2 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, OutputType, InputType3, bool >( z, nullptr,
+			&a, 0.0, nullptr, static_cast< double >( chi ), &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &a,
+		const Vector< InputType2, b200, Coords > &x,
+		const InputType3 gamma,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< InputType3 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, InputType2, OutputType, bool >( z, nullptr,
+			&a, 0.0, &x, 0.0, nullptr, static_cast< double >( gamma ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &a,
+		const Vector< InputType2, b200, Coords > &x,
+		const Vector< InputType3, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, InputType2, InputType3, bool >( z, nullptr,
+			&a, 0.0, &x, 0.0, &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &m,
+		const InputType1 alpha,
+		const InputType2 chi,
+		const InputType3 gamma,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value &&
+			!grb::is_object< InputType3 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, OutputType, OutputType, MaskType >( z, &m,
+			nullptr, static_cast< double >( alpha ), nullptr, static_cast< double >( chi ), nullptr, static_cast< double >( gamma ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &m,
+		const InputType1 alpha,
+		const InputType2 chi,
+		const Vector< InputType3, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, OutputType, InputType3, MaskType >( z, &m,
+			nullptr, static_cast< double >( alpha ), nullptr, static_cast< double >( chi ), &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &m,
+		const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &x,
+		const InputType3 gamma,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType3 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, InputType2, OutputType, MaskType >( z, &m,
+			nullptr, static_cast< double >( alpha ), &x, 0.0, nullptr, static_cast< double >( gamma ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &m,
+		const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &x,
+		const Vector< InputType3, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType1 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, InputType2, InputType3, MaskType >( z, &m,
+			nullptr, static_cast< double >( alpha ), &x, 0.0, &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &m,
+		const Vector< InputType1, b200, Coords > &a,
+		const InputType2 chi,
+		const InputType3 gamma,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType2 >::value &&
+			!grb::is_object< InputType3 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, OutputType, OutputType, MaskType >( z, &m,
+			&a, 0.0, nullptr, static_cast< double >( chi ), nullptr, static_cast< double >( gamma ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &m,
+		const Vector< InputType1, b200, Coords > &a,
+		const InputType2 chi,
+		const Vector< InputType3, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType2 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, OutputType, InputType3, MaskType >( z, &m,
+			&a, 0.0, nullptr, static_cast< double >( chi ), &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &m,
+		const Vector< InputType1, b200, Coords > &a,
+		const Vector< InputType2, b200, Coords > &x,
+		const InputType3 gamma,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< MaskType >::value &&
+			!grb::is_object< InputType3 >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, InputType2, OutputType, MaskType >( z, &m,
+			&a, 0.0, &x, 0.0, nullptr, static_cast< double >( gamma ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
+	RC eWiseMulAdd( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &m,
+		const Vector< InputType1, b200, Coords > &a,
+		const Vector< InputType2, b200, Coords > &x,
+		const Vector< InputType3, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			grb::is_semiring< Ring >::value &&
+			!grb::is_object< MaskType >::value,
+			void >::type * const = nullptr
+	) {
+		(void) ring;
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, InputType2, InputType3, MaskType >( z, &m,
+			&a, 0.0, &x, 0.0, &y, 0.0 );
+	}
+
+	// ---------------------------------------------------------- eWiseLambda --
+	namespace internal {
+		namespace b200rt {
+			inline void touch() {}
+			template< typename T, typename C, typename... Args >
+			void touch( const Vector< T, grb::b200, C > &v, const Args &... args ) {
+				(void) v.raw();  // synchronised host access; pages return on next device use
+				touch( args... );
+			}
+			template< typename First, typename... Args >
+			void touch( const First &, const Args &... args ) { touch( args... ); }
+		}
+	}
+
+	/** Runs f(i) on the host for every assigned index of x (all when dense). */
+	template< Descriptor descr = descriptors::no_operation, class Func, typename DataType1,
+		typename Coords, typename... Args >
+	RC eWiseLambda( const Func f, const Vector< DataType1, b200, Coords > &x,
+		const Args &... args
+	) {
+		x.b200_host_ready();
+		internal::b200rt::touch( x, args... );
+		const size_t n = size( x );
+		const uint8_t * const fl = x.b200_flags();
+		const bool dense = x.b200_dense() || ( descr & descriptors::dense );
+		for( size_t i = 0; i < n; ++i ) {
+			if( dense || fl[ i ] ) { f( i ); }
+		}
+		return SUCCESS;
+	}
+
+}
+
+#endif

@@ -1,0 +1,264 @@
+/*
+ * grb::Matrix for the b200 backend (reference: graphblas/reference/matrix.hpp,
+ * Matrix<D, reference, RIT, CIT, NIT> at :1018-2300).
+ *
+ * Like the reference, the matrix keeps BOTH orientations: a CRS for the
+ * row gather (mxv) and a CCS for the column gather (vxm, transposed products,
+ * adjoint solves), each in the reference's compressed-storage layout
+ * (int64 offsets, uint32 indices, values of D, none for a pattern matrix) and
+ * in device memory.  SpMV plans (schedule + merge-path tables) are made the
+ * first time an orientation is multiplied and kept with the matrix.
+ */
+#ifndef _H_GRB_B200_MATRIX
+#define _H_GRB_B200_MATRIX
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <utility>
+#include <vector>
+
+#include <graphblas/base/matrix.hpp>
+#include <graphblas/b200/runtime.hpp>
+
+namespace grb {
+
+	namespace internal {
+
+		namespace b200rt {
+
+			/** One compressed orientation on the device. */
+			template< typename S >
+			struct Storage {
+				int64_t * offsets = nullptr;
+				uint32_t * indices = nullptr;
+				S * values = nullptr;
+				mutable alpb_spmv_plan plan = nullptr;
+
+				void release_all() noexcept {
+					if( plan ) { (void) alpb_spmv_plan_destroy( plan ); }
+					release( offsets );
+					release( indices );
+					release( values );
+					plan = nullptr;
+					offsets = nullptr;
+					indices = nullptr;
+					values = nullptr;
+				}
+			};
+
+			template< typename D >
+			struct value_storage { typedef typename storage< D >::type type; };
+			template<>
+			struct value_storage< void > { typedef char type; };
+
+		}
+
+	}
+
+	template< typename D, typename RIT, typename CIT, typename NIT >
+	class Matrix< D, b200, RIT, CIT, NIT > {
+
+		static_assert( sizeof( RIT ) <= 4 && sizeof( CIT ) <= 4,
+			"the b200 backend stores 32-bit row and column indices" );
+
+		public:
+
+			typedef D value_type;
+			typedef typename internal::b200rt::value_storage< D >::type storage_type;
+			typedef internal::b200rt::Storage< storage_type > storage_t;
+
+		private:
+
+			size_t _m = 0, _n = 0, _cap = 0, _nz = 0;
+			storage_t _crs, _ccs;
+
+			void init( const size_t m, const size_t n, const size_t cap ) {
+				_m = m;
+				_n = n;
+				_cap = cap;
+				_nz = 0;
+				_crs.offsets = internal::b200rt::alloc< int64_t >( m + 1 );
+				_ccs.offsets = internal::b200rt::alloc< int64_t >( n + 1 );
+				(void) alpb_memset( _crs.offsets, 0, ( m + 1 ) * 8, internal::b200rt::stream() );
+				(void) alpb_memset( _ccs.offsets, 0, ( n + 1 ) * 8, internal::b200rt::stream() );
+				(void) alpb_stream_sync( internal::b200rt::stream() );
+			}
+
+			void move_from( Matrix &o ) noexcept {
+				_m = o._m; _n = o._n; _cap = o._cap; _nz = o._nz;
+				_crs = o._crs;
+				_ccs = o._ccs;
+				o._crs = storage_t();
+				o._ccs = storage_t();
+				o._m = o._n = o._cap = o._nz = 0;
+			}
+
+			static void copy_storage( storage_t &dst, const storage_t &src, const size_t outer,
+				const size_t nz
+			) {
+				dst.offsets = internal::b200rt::alloc< int64_t >( outer + 1 );
+				(void) alpb_memcpy_d2d( dst.offsets, src.offsets, ( outer + 1 ) * 8,
+					internal::b200rt::stream() );
+				if( nz > 0 ) {
+					dst.indices = internal::b200rt::alloc< uint32_t >( nz );
+					(void) alpb_memcpy_d2d( dst.indices, src.indices, nz * 4, internal::b200rt::stream() );
+					if( internal::b200rt::type_code< D >::value != ALPB_VOID ) {
+						dst.values = internal::b200rt::alloc< storage_type >( nz );
+						(void) alpb_memcpy_d2d( dst.values, src.values, nz * sizeof( storage_type ),
+							internal::b200rt::stream() );
+					}
+				}
+			}
+
+		public:
+
+			Matrix( const size_t rows, const size_t columns, const size_t nz ) {
+				init( rows, columns, nz );
+			}
+
+			Matrix( const size_t rows, const size_t columns ) : Matrix( rows, columns, 0 ) {}
+
+			Matrix( const Matrix &o ) {
+				_m = o._m; _n = o._n; _cap = o._cap; _nz = o._nz;
+				copy_storage( _crs, o._crs, _m, _nz );
+				copy_storage( _ccs, o._ccs, _n, _nz );
+				(void) alpb_stream_sync( internal::b200rt::stream() );
+			}
+
+			Matrix( Matrix &&o ) noexcept { move_from( o ); }
+
+			Matrix & operator=( Matrix &&o ) noexcept {
+				if( this != &o ) {
+					_crs.release_all();
+					_ccs.release_all();
+					move_from( o );
+				}
+				return *this;
+			}
+
+			~Matrix() {
+				_crs.release_all();
+				_ccs.release_all();
+			}
+
+			/** Const iterator over ((row, column), value) -- host copy of the CRS. */
+			class const_iterator {
+				private:
+					std::vector< int64_t > _off;
+					std::vector< uint32_t > _idx;
+					std::vector< storage_type > _val;
+					size_t _row = 0, _k = 0;
+				public:
+					typedef std::pair< std::pair< size_t, size_t >, D > value_type;
+					const_iterator() = default;
+					const_iterator( const Matrix &A, const bool at_end ) {
+						if( at_end ) { _k = A._nz; _row = A._m; return; }
+						_off.resize( A._m + 1 );
+						_idx.resize( A._nz );
+						(void) alpb_memcpy_d2h( _off.data(), A._crs.offsets, ( A._m + 1 ) * 8,
+							internal::b200rt::stream() );
+						if( A._nz ) {
+							(void) alpb_memcpy_d2h( _idx.data(), A._crs.indices, A._nz * 4,
+								internal::b200rt::stream() );
+							if( A._crs.values ) {
+								_val.resize( A._nz );
+								(void) alpb_memcpy_d2h( _val.data(), A._crs.values,
+									A._nz * sizeof( storage_type ), internal::b200rt::stream() );
+							}
+						}
+						(void) alpb_stream_sync( internal::b200rt::stream() );
+						while( _row < A._m && _off[ _row + 1 ] <= static_cast< int64_t >( _k ) ) { ++_row; }
+					}
+					bool operator!=( const const_iterator &o ) const { return _k != o._k; }
+					bool operator==( const const_iterator &o ) const { return _k == o._k; }
+					const_iterator & operator++() {
+						++_k;
+						while( _row + 1 < _off.size() && _off[ _row + 1 ] <= static_cast< int64_t >( _k ) ) {
+							++_row;
+						}
+						return *this;
+					}
+					value_type operator*() const {
+						return value_type( std::make_pair( _row, static_cast< size_t >( _idx[ _k ] ) ),
+							_val.empty() ? D() : static_cast< D >( _val[ _k ] ) );
+					}
+			};
+
+			const_iterator cbegin() const { return const_iterator( *this, false ); }
+			const_iterator cend() const { return const_iterator( *this, true ); }
+			const_iterator begin() const { return cbegin(); }
+			const_iterator end() const { return cend(); }
+
+			// ---- backend-internal access ----
+			size_t b200_rows() const noexcept { return _m; }
+			size_t b200_cols() const noexcept { return _n; }
+			size_t b200_nnz() const noexcept { return _nz; }
+			size_t b200_capacity() const noexcept { return _cap; }
+			const storage_t & b200_crs() const noexcept { return _crs; }
+			const storage_t & b200_ccs() const noexcept { return _ccs; }
+
+			/** Plan of one orientation, made on first use. */
+			alpb_spmv_plan b200_plan( const bool rows ) const {
+				const storage_t &s = rows ? _crs : _ccs;
+				if( !s.plan && _nz > 0 ) {
+					(void) alpb_spmv_plan_create( &s.plan, static_cast< int64_t >( rows ? _m : _n ),
+						static_cast< int64_t >( _nz ), s.offsets, ALPB_SCHED_AUTO, 0,
+						internal::b200rt::stream() );
+				}
+				return s.plan;
+			}
+
+			void b200_clear() {
+				_crs.release_all();
+				_ccs.release_all();
+				const size_t m = _m, n = _n, cap = _cap;
+				init( m, n, cap );
+			}
+
+			void b200_reserve( const size_t cap ) { if( cap > _cap ) { _cap = cap; } }
+
+			/** Replace the contents by the (I, J, V) triples, in input order: both
+			 *  orientations are built on the device with the reference's in-row
+			 *  order (alpb_coo_to_crs). */
+			RC b200_build( const std::vector< uint32_t > &I, const std::vector< uint32_t > &J,
+				const std::vector< storage_type > &V
+			) {
+				using namespace internal::b200rt;
+				const size_t nz = I.size();
+				const int vt = type_code< D >::value;
+				if( vt < 0 ) { return UNSUPPORTED; }
+				_crs.release_all();
+				_ccs.release_all();
+				init( _m, _n, nz > _cap ? nz : _cap );
+				if( nz == 0 ) { return SUCCESS; }
+				uint32_t * dI = alloc< uint32_t >( nz );
+				uint32_t * dJ = alloc< uint32_t >( nz );
+				storage_type * dV = vt == ALPB_VOID ? nullptr : alloc< storage_type >( nz );
+				(void) alpb_memcpy_h2d( dI, I.data(), nz * 4, stream() );
+				(void) alpb_memcpy_h2d( dJ, J.data(), nz * 4, stream() );
+				if( dV ) { (void) alpb_memcpy_h2d( dV, V.data(), nz * sizeof( storage_type ), stream() ); }
+				_crs.indices = alloc< uint32_t >( nz );
+				_ccs.indices = alloc< uint32_t >( nz );
+				if( dV ) {
+					_crs.values = alloc< storage_type >( nz );
+					_ccs.values = alloc< storage_type >( nz );
+				}
+				RC rc = check( alpb_coo_to_crs( _m, _n, nz, dI, dJ, dV, vt, _crs.offsets, _crs.indices,
+					_crs.values, stream() ), "buildMatrixUnique (CRS)" );
+				if( rc == SUCCESS ) {
+					rc = check( alpb_coo_to_crs( _n, _m, nz, dJ, dI, dV, vt, _ccs.offsets, _ccs.indices,
+						_ccs.values, stream() ), "buildMatrixUnique (CCS)" );
+				}
+				(void) alpb_stream_sync( stream() );
+				release( dI );
+				release( dJ );
+				release( dV );
+				if( rc == SUCCESS ) { _nz = nz; }
+				return rc;
+			}
+	};
+
+}
+
+#endif

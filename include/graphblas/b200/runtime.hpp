@@ -1,0 +1,152 @@
+/*
+ * Glue between ALP's C++ types and the C-ABI of libalp_b200.so
+ * (include/alp_b200.h): element type codes, operator codes of ALP's
+ * operator classes (graphblas/ops.hpp), semiring codes, device buffers and
+ * the stream every b200 primitive is ordered on.
+ *
+ * Host code of the b200 backend is compiled by the host compiler only (no
+ * CUDA headers needed): it calls the C-ABI, which launches the kernels.
+ */
+#ifndef _H_GRB_B200_RUNTIME
+#define _H_GRB_B200_RUNTIME
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <iostream>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+
+#include <alp_b200.h>
+
+#include <graphblas/backends.hpp>
+#include <graphblas/ops.hpp>
+#include <graphblas/rc.hpp>
+
+namespace grb {
+
+	namespace internal {
+
+		namespace b200rt {
+
+			/** Stream all primitives are ordered on (NULL: the legacy default stream). */
+			inline void * stream() noexcept { return nullptr; }
+
+			/** The C-ABI returns grb::RC numbering; map it and keep the message. */
+			inline RC check( const int rc, const char * const where ) {
+				if( rc != ALPB_SUCCESS ) {
+#ifndef _GRB_NO_STDIO
+					std::cerr << "grb::b200: " << where << ": " << alpb_last_error() << "\n";
+#endif
+				}
+				return static_cast< RC >( rc );
+			}
+
+			/** Element type code of a C++ domain; -1 when the device cannot hold it. */
+			template< typename T, typename Enable = void >
+			struct type_code { static constexpr int value = -1; };
+			template<> struct type_code< double > { static constexpr int value = ALPB_FP64; };
+			template<> struct type_code< bool > { static constexpr int value = ALPB_BOOL; };
+			template<> struct type_code< int > { static constexpr int value = ALPB_INT32; };
+			template<> struct type_code< unsigned int > { static constexpr int value = ALPB_UINT32; };
+			template<> struct type_code< long > { static constexpr int value = ALPB_INT64; };
+			template<> struct type_code< long long > { static constexpr int value = ALPB_INT64; };
+			template<> struct type_code< unsigned long > { static constexpr int value = ALPB_INT64; };
+			template<> struct type_code< void > { static constexpr int value = ALPB_VOID; };
+
+			/** Device storage type of a domain (bool is held as one byte). */
+			template< typename T >
+			struct storage { typedef T type; };
+			template<>
+			struct storage< bool > { typedef uint8_t type; };
+
+			/** Operator code of an ALP operator class; -1 when not on the device. */
+			template< class OP >
+			struct op_code { static constexpr int value = -1; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::add< A, B, C, X > > { static constexpr int value = ALPB_OP_ADD; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::subtract< A, B, C, X > > { static constexpr int value = ALPB_OP_SUB; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::mul< A, B, C, X > > { static constexpr int value = ALPB_OP_MUL; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::divide< A, B, C, X > > { static constexpr int value = ALPB_OP_DIV; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::min< A, B, C, X > > { static constexpr int value = ALPB_OP_MIN; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::max< A, B, C, X > > { static constexpr int value = ALPB_OP_MAX; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::abs_diff< A, B, C, X > > { static constexpr int value = ALPB_OP_ABS_DIFF; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::left_assign< A, B, C, X > > { static constexpr int value = ALPB_OP_LEFT_ASSIGN; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::right_assign< A, B, C, X > > { static constexpr int value = ALPB_OP_RIGHT_ASSIGN; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::logical_or< A, B, C, X > > { static constexpr int value = ALPB_OP_LOR; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::logical_and< A, B, C, X > > { static constexpr int value = ALPB_OP_LAND; };
+			// on real domains the conjugating multiplications are plain products
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::conjugate_right_mul< A, B, C, X > > {
+				static constexpr int value = std::is_floating_point< A >::value ? ALPB_OP_MUL : -1;
+			};
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::conjugate_left_mul< A, B, C, X > > {
+				static constexpr int value = std::is_floating_point< A >::value ? ALPB_OP_MUL : -1;
+			};
+
+			/** Semiring code of a (additive, multiplicative) operator pair; -1 otherwise. */
+			template< class ADD, class MUL >
+			struct ring_code { static constexpr int value = -1; };
+			template< Backend X, Backend Y >
+			struct ring_code< operators::add< double, double, double, X >,
+				operators::mul< double, double, double, Y > > {
+				static constexpr int value = ALPB_RING_PLUS_TIMES_F64;
+			};
+			template< Backend X, Backend Y >
+			struct ring_code< operators::logical_or< bool, bool, bool, X >,
+				operators::logical_and< bool, bool, bool, Y > > {
+				static constexpr int value = ALPB_RING_LOR_LAND_BOOL;
+			};
+			template< Backend X, Backend Y >
+			struct ring_code< operators::min< int, int, int, X >,
+				operators::add< int, int, int, Y > > {
+				static constexpr int value = ALPB_RING_MIN_PLUS_I32;
+			};
+			template< Backend X, Backend Y >
+			struct ring_code< operators::add< double, double, double, X >,
+				operators::left_assign_if< double, bool, double, Y > > {
+				static constexpr int value = ALPB_RING_PLUS_PATTERN_F64;
+			};
+			template< Backend X, Backend Y >
+			struct ring_code< operators::add< int, int, int, X >,
+				operators::mul< int, int, int, Y > > {
+				static constexpr int value = ALPB_RING_PLUS_TIMES_I32;
+			};
+
+			/** Device allocation that reports OUTOFMEM through the C-ABI. */
+			template< typename T >
+			T * alloc( const size_t n ) {
+				void * p = nullptr;
+				if( n == 0 ) { return nullptr; }
+				const int rc = alpb_malloc( &p, n * sizeof( T ) );
+				if( rc != ALPB_SUCCESS ) {
+					throw std::runtime_error( std::string( "grb::b200: device allocation of " ) +
+						std::to_string( n * sizeof( T ) ) + " bytes failed: " + alpb_last_error() );
+				}
+				return static_cast< T * >( p );
+			}
+
+			inline void release( void * p ) noexcept {
+				if( p ) { (void) alpb_free( p ); }
+			}
+
+		} // namespace b200rt
+
+	} // namespace internal
+
+} // namespace grb
+
+#endif

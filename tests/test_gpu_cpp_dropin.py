@@ -1,0 +1,167 @@
+"""The C++ drop-in: ALP programs compiled unchanged against the b200 backend.
+
+* ALP's own self-contained unit tests (tests/unit/*.cpp of the ALP tree),
+  compiled against b200 by tests/cpp/Makefile, must print "Test OK".
+* tests/cpp/alp_driver.cpp is compiled twice -- against ALP's reference
+  backend (the checker, oracle/_ref/cpp) and against b200 (_build/cpp) -- and
+  both run the same case files: mxv / vxm over three semirings with masks and
+  descriptors, the BLAS1 primitives, conjugate_gradient and simple_pagerank.
+  Their printed results must agree: bool and int exactly, FP64 within
+  relative 1e-12 for single primitives and 1e-9 for the solvers, with equal
+  iteration counts.
+
+The binaries are built by __graft_entry__.build() (they need the ALP sources
+and are not rebuilt on the GPU host); a missing binary fails the test.
+"""
+import os
+import struct
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parent.parent
+B200_BIN = ROOT / "_build" / "cpp"
+REF_BIN = ROOT / "oracle" / "_ref" / "cpp"
+UNIT = ["masked_mxv", "sparse_mxv", "masked_vxm", "dot", "set", "eWiseMul", "muladd",
+        "masked_muladd", "eWiseLambda"]
+
+
+def _run(exe: Path, *args, timeout=300):
+    if not exe.exists():
+        pytest.fail(f"{exe} is not built (build() compiles it where the ALP sources exist)")
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    return subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True,
+                          timeout=timeout, env=env)
+
+
+@pytest.mark.parametrize("name", UNIT)
+def test_alp_unit_test_passes_on_b200(cuda, name):
+    r = _run(B200_BIN / f"unit_{name}_b200")
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "Test OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+
+
+# ------------------------------------------------------------ differential --
+def write_case(path, op, ring, descr, m, n, I, J, V, u=None, v=None, um=None, vm=None):
+    with open(path, "wb") as f:
+        f.write(struct.pack("<6q", op, ring, descr, m, n, len(I)))
+        f.write(np.asarray(I, np.uint32).tobytes())
+        f.write(np.asarray(J, np.uint32).tobytes())
+        f.write(np.asarray(V, np.float64).tobytes())
+        for arr in (u, v, um, vm):
+            if arr is None:
+                f.write(struct.pack("<q", 0))
+                continue
+            vals, flags = arr
+            f.write(struct.pack("<q", len(vals)))
+            f.write(np.asarray(vals, np.float64).tobytes())
+            f.write(np.asarray(flags, np.uint8).tobytes())
+
+
+def parse(out: str) -> dict:
+    res = {}
+    for line in out.splitlines():
+        parts = line.split()
+        if len(parts) == 3 and parts[1] != "nnz":
+            res[(parts[0], int(parts[1]))] = float(parts[2])
+        elif len(parts) >= 2:
+            res[(parts[0], parts[1] if len(parts) == 3 else None)] = parts[-1]
+    return res
+
+
+def compare(case_file, rtol):
+    a = _run(REF_BIN / "alp_driver_ref", case_file)
+    b = _run(B200_BIN / "alp_driver_b200", case_file)
+    assert a.returncode == 0, a.stdout[-1000:] + a.stderr[-1000:]
+    assert b.returncode == 0, b.stdout[-1000:] + b.stderr[-1000:]
+    ra, rb = parse(a.stdout), parse(b.stdout)
+    assert set(ra) == set(rb), (sorted(set(ra) ^ set(rb))[:10], a.stdout[:500], b.stdout[:500])
+    for k, va in ra.items():
+        vb = rb[k]
+        if isinstance(va, float):
+            assert abs(va - vb) <= rtol * max(abs(va), abs(vb), 1e-300) or va == vb, (k, va, vb)
+        else:
+            assert va == vb, (k, va, vb)
+
+
+def _vec(R, n, seed, p_assigned, lo=0, hi=100, vtype=3):
+    vals = R.values(n, vtype, seed, 1, lo, hi).astype(np.float64)
+    flags = R.values(n, 1, seed + 1, 2, p=p_assigned) if p_assigned < 1 else np.ones(n, np.uint8)
+    return vals, flags
+
+
+@pytest.mark.parametrize("ring", [0, 1, 2])
+@pytest.mark.parametrize("op", [0, 1], ids=["mxv", "vxm"])
+@pytest.mark.parametrize("descr", range(8),
+                         ids=["plain", "invert", "structural", "structinv", "addidentity",
+                              "explicitzero", "transpose", "dense"])
+@pytest.mark.parametrize("sparse", [False, True], ids=["dense", "sparse"])
+def test_driver_spmv_matches_reference(cuda, oracle, ring, op, descr, sparse):
+    from oracle.oracle import crs_to_coo
+    if descr == 7 and sparse:
+        pytest.skip("dense descriptor on sparse inputs is ILLEGAL on both (covered in the ABI tests)")
+    t = {0: 3, 1: 1, 2: 2}[ring]
+    rp, col, vals = oracle.rmat(8, edge_factor=6, seed=40 + ring, vtype=t, lo=1, hi=100)
+    n = len(rp) - 1
+    I, J = crs_to_coo(rp, col)
+    perm = np.random.default_rng(ring).permutation(len(I))
+    I, J, V = I[perm], J[perm], vals[perm].astype(np.float64)
+    if ring == 1:
+        u = (oracle.values(n, 1, 3, 1, p=0.3).astype(float), np.ones(n, np.uint8))
+        v = (oracle.values(n, 1, 4, 1, p=0.5).astype(float), np.ones(n, np.uint8))
+    else:
+        u = _vec(oracle, n, 3, 1.0, 0, 5000, t)
+        v = _vec(oracle, n, 5, 1.0, 0, 1000, t)
+    um = (oracle.values(n, 1, 7, 1, p=0.5).astype(float), np.ones(n, np.uint8))
+    vm = None
+    if sparse:
+        u = (u[0], oracle.values(n, 1, 9, 3, p=0.3))
+        v = (v[0], oracle.values(n, 1, 10, 3, p=0.6))
+        um = (um[0], oracle.values(n, 1, 11, 3, p=0.8))
+        vm = (oracle.values(n, 1, 12, 1, p=0.5).astype(float), oracle.values(n, 1, 13, 3, p=0.8))
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "case.bin"
+        write_case(f, op, ring, descr, n, n, I, J, V, u, v, um, vm)
+        compare(f, 1e-12)
+
+
+@pytest.mark.parametrize("sparse", [False, True])
+def test_driver_blas1_matches_reference(cuda, oracle, sparse):
+    n = 5000
+    u = _vec(oracle, n, 21, 0.6 if sparse else 1.0)
+    v = _vec(oracle, n, 23, 0.5 if sparse else 1.0)
+    m = (oracle.values(n, 1, 25, 1, p=0.5).astype(float),
+         oracle.values(n, 1, 26, 2, p=0.7) if sparse else np.ones(n, np.uint8))
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "case.bin"
+        write_case(f, 4, 0, 0, 0, 0, [], [], [], u, v, m, None)
+        compare(f, 1e-12)
+
+
+def test_driver_cg_matches_reference(cuda, oracle):
+    I, J, V = oracle.stencil_coo((12, 12, 12), 26.0, -1.0)
+    m = 12 ** 3
+    rp, col, vals = oracle.coo_to_crs(m, I, J, V, 3)
+    b = np.zeros(m)
+    oracle.mxv(0, 0, 2, m, m, rp, col, vals, 3, b, v=np.ones(m))
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "case.bin"
+        write_case(f, 2, 0, 0, m, m, I, J, V, (np.zeros(m), np.ones(m, np.uint8)),
+                   (b, np.ones(m, np.uint8)))
+        compare(f, 1e-9)
+
+
+def test_driver_pagerank_matches_reference(cuda, oracle):
+    from oracle.oracle import crs_to_coo
+    rp, col, _ = oracle.rmat(11, edge_factor=8, seed=77, vtype=3)
+    I, J = crs_to_coo(rp, col)
+    n = len(rp) - 1
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "case.bin"
+        write_case(f, 3, 0, 0, n, n, I, J, np.ones(len(I)))
+        compare(f, 1e-9)
