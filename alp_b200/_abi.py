@@ -84,6 +84,7 @@ PROTOS: dict[str, list] = {
                  P, P, I64,
                  P, P, I32, I64,
                  P, P],
+    "alpb_mxv_dense_noalloc": [I32, I32, I64, I64, I64, P, P, P, I32, P, P, P],
     "alpb_dot_f64": [PD, I32, I32, I64, P, P, P, P, P],
     "alpb_dot_f64_device": [P, I32, I32, I64, P, P, P],
     "alpb_set_scalar": [P, I32, I64, D, P, P, P],

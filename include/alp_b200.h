@@ -269,6 +269,27 @@ ALPB_API int alpb_mxv(int ring, uint32_t descr, int form,
 	int64_t v_mask_count,
 	alpb_spmv_plan plan, void *stream);
 
+/*
+ * Allocation-free dense SpMV.  No counterpart exists in the reference.  It is
+ * for callers that cannot allocate device memory at call time: a memory pool
+ * that already owns the whole device, code running inside an allocator or a
+ * stream callback, or a thread that must not meet cudaMalloc's implicit
+ * device synchronisation.  It computes u = u (+) A (x) v for dense u and v,
+ * without masks, under descriptor `none` -- the result alpb_mxv gives on the
+ * merge-path schedule, with the same `ring`, `form` and storage conventions.
+ * Its merge-path tables live in one fixed 7 MiB device array inside the
+ * library (held by every GPU that loads it, until the process exits), so the
+ * caller passes no plan and no scratch.  Limit: m_out + nnz <= 268,435,456
+ * (131,072 tiles of 2048 merge items); larger inputs return ALPB_ILLEGAL with
+ * an error message.  The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * Every call, from any thread or stream, shares the one array: calls that
+ * overlap in time on one device race and give wrong results; serialise them.
+ */
+ALPB_API int alpb_mxv_dense_noalloc(int ring, int form, int64_t m_out, int64_t n_in,
+	int64_t nnz, const int64_t *offsets, const uint32_t *indices, const void *values,
+	int value_type, void *u, const void *v, void *stream);
+
 /* ======================================================================
  * BLAS1 (replaces reference/blas1.hpp: dot 9262-9681, eWiseMul 8610-9172,
  * eWiseMulAdd 6347-6770, foldl/foldr 1069-2897, eWiseApply 2966-5343, set in
