@@ -79,14 +79,16 @@ int alpb_sddmm(alpb_spmv_plan plan, int64_t m, int64_t nnz, const int64_t *offse
 	ALPB_CHECK(m >= 0 && nnz >= 0, ALPB_ILLEGAL, "alpb_sddmm: negative size");
 	if (m == 0 || nnz == 0) return ALPB_SUCCESS;
 	cudaStream_t s = as_stream(stream);
+	if (plan)
+		ALPB_CHECK(plan->m == m && plan->nnz == nnz, ALPB_MISMATCH,
+			"alpb_sddmm: plan was made for another storage");
 	alpb_spmv_plan own = nullptr;
-	if (!plan) {
-		int rc = alpb_spmv_plan_create(&own, m, nnz, offsets, ALPB_SCHED_MERGE_PATH, 0, stream);
+	if (!plan || plan->tile != MP_TILE) {
+		// k_sddmm runs block tiles: it needs tables cut at MP_TILE
+		int rc = plan_create_tiles(&own, m, nnz, offsets, ALPB_SCHED_MERGE_PATH, 0, MP_TILE, s);
 		if (rc != ALPB_SUCCESS) return rc;
 		plan = own;
 	}
-	ALPB_CHECK(plan->m == m && plan->nnz == nnz, ALPB_MISMATCH,
-		"alpb_sddmm: plan was made for another storage");
 	const unsigned grid = unsigned(plan->ntiles < int64_t(sm_count()) * 8 ? plan->ntiles
 		: int64_t(sm_count()) * 8);
 	k_sddmm<<<grid, MP_BLOCK, 0, s>>>(merge_tables(*plan), offsets, indices, lam, x, alpha, out);

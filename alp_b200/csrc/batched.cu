@@ -122,6 +122,7 @@ int merge_plan_segmented(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t ns
 	ALPB_CUDA(cudaStreamSynchronize(s));
 	ALPB_CHECK(nt > 0, ALPB_ILLEGAL, "segmented plan: no work");
 	p->ntiles = nt;
+	p->tile = MP_TILE;
 	const size_t n = size_t(nt);
 	ALPB_CUDA(cudaMalloc(&st->tile_d, (n + 1) * 8));
 	ALPB_CUDA(cudaMalloc(&st->tile_seg, n * 4));

@@ -202,17 +202,19 @@ extern "C" int alpb_cg_solve(int64_t n, const int64_t *row_ptr, const uint32_t *
 	*residual = INFINITY;
 	if (n == 0) return ALPB_SUCCESS;
 	cudaStream_t s = as_stream(stream);
+	if (plan)
+		ALPB_CHECK(plan->m == n && plan->offsets == row_ptr, ALPB_MISMATCH,
+			"alpb_cg_solve: plan was made for another storage");
 	alpb_spmv_plan own_plan = nullptr;
-	if (!plan) {
+	if (!plan || plan->tile != MP_TILE) {
+		// the fused kernel runs block tiles: it needs tables cut at MP_TILE
 		int64_t nnz = 0;
 		ALPB_CUDA(cudaMemcpyAsync(&nnz, row_ptr + n, 8, cudaMemcpyDeviceToHost, s));
 		ALPB_CUDA(cudaStreamSynchronize(s));
-		int rc = alpb_spmv_plan_create(&own_plan, n, nnz, row_ptr, ALPB_SCHED_MERGE_PATH, 0, stream);
+		int rc = plan_create_tiles(&own_plan, n, nnz, row_ptr, ALPB_SCHED_MERGE_PATH, 0, MP_TILE, s);
 		if (rc != ALPB_SUCCESS) return rc;
 		plan = own_plan;
 	}
-	ALPB_CHECK(plan->m == n && plan->offsets == row_ptr, ALPB_MISMATCH,
-		"alpb_cg_solve: plan was made for another storage");
 	const int64_t nt = plan->ntiles;
 	int grid = cooperative_grid(k_cg, MP_BLOCK, 0, 0);
 	ALPB_CHECK(grid > 0, ALPB_PANIC, "alpb_cg_solve: no cooperative occupancy");

@@ -86,8 +86,12 @@ __global__ void k_vec(VecArgs a) {
 		bool write = false, assign = false;
 		double out = 0.0;
 		switch (a.kind) {
-		case ALPB_VEC_SET:  // z_i = x_i where x is present
-			if (xh) { out = xv; write = true; assign = true; }
+		case ALPB_VEC_SET:  // z_i = x_i (or i under use_index) where x is present
+			if (xh) {
+				out = (a.descr & ALPB_DESC_USE_INDEX) ? double(i) : xv;
+				write = true;
+				assign = true;
+			}
 			break;
 		case ALPB_VEC_FOLDL:  // z_i = z_i op x_i
 		case ALPB_VEC_FOLDR:  // z_i = x_i op z_i

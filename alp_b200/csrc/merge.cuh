@@ -232,10 +232,12 @@ struct PlainX {
 
 // Table kernels (spmv.cu): tile starts by merge-path search, then the
 // spanning-row tables.
+// `tile` = merge items per tile.
 __global__ void k_merge_tiles(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
-	int64_t *tile_row);
+	int64_t *tile_row, int64_t tile = MP_TILE);
 __global__ void k_merge_tables(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
-	const int64_t *tile_row, int64_t *head_first, int64_t *tail_first, int32_t *span_len);
+	const int64_t *tile_row, int64_t *head_first, int64_t *tail_first, int32_t *span_len,
+	int64_t tile = MP_TILE);
 
 // Segmented tables (batched solves): tiles are cut at segment boundaries.
 struct SegmentedTiles {

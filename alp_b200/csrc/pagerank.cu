@@ -173,7 +173,7 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 	ALPB_CUDA(cudaMemcpyAsync(&nnz, ccs_col_ptr + n, 8, cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
 	alpb_spmv_plan plan = nullptr;
-	int rc = alpb_spmv_plan_create(&plan, n, nnz, ccs_col_ptr, ALPB_SCHED_MERGE_PATH, 0, stream);
+	int rc = plan_create_tiles(&plan, n, nnz, ccs_col_ptr, ALPB_SCHED_MERGE_PATH, 0, MP_TILE, s);
 	if (rc != ALPB_SUCCESS) return rc;
 	const int64_t nt = plan->ntiles;
 	int grid = cooperative_grid(k_pagerank, MP_BLOCK, 0, 0);

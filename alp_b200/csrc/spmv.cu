@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "spmv.cuh"
 #include "merge.cuh"
+#include "wmerge.cuh"
 
 #include <algorithm>
 
@@ -37,10 +38,10 @@ __device__ __forceinline__ int64_t merge_search_global(const int64_t *offsets, i
 }
 
 __global__ void k_merge_tiles(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
-	int64_t *tile_row) {
+	int64_t *tile_row, int64_t tile) {
 	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t <= ntiles;
 		 t += int64_t(gridDim.x) * blockDim.x) {
-		int64_t d = t * MP_TILE;
+		int64_t d = t * tile;
 		if (d > m + nnz) d = m + nnz;
 		tile_row[t] = merge_search_global(offsets, m, nnz, d);
 	}
@@ -71,22 +72,23 @@ __global__ void k_row_stats(const int64_t *offsets, int64_t m, unsigned long lon
 // first tile of its head / tail row when that row crosses tiles, and for the
 // first tile of a spanning row the number of tiles it covers.
 __global__ void k_merge_tables(const int64_t *offsets, int64_t m, int64_t nnz, int64_t ntiles,
-	const int64_t *tile_row, int64_t *head_first, int64_t *tail_first, int32_t *span_len) {
+	const int64_t *tile_row, int64_t *head_first, int64_t *tail_first, int32_t *span_len,
+	int64_t tile) {
 	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < ntiles;
 		 t += int64_t(gridDim.x) * blockDim.x) {
 		const int64_t i0 = tile_row[t], i1 = tile_row[t + 1];
-		const int64_t d0 = t * MP_TILE;
-		int64_t d1 = d0 + MP_TILE;
+		const int64_t d0 = t * tile;
+		int64_t d1 = d0 + tile;
 		if (d1 > m + nnz) d1 = m + nnz;
 		const int64_t j0 = d0 - i0, j1 = d1 - i1;
-		head_first[t] = (i1 > i0 && offsets[i0] < j0) ? (i0 + offsets[i0]) / MP_TILE : -1;
+		head_first[t] = (i1 > i0 && offsets[i0] < j0) ? (i0 + offsets[i0]) / tile : -1;
 		int64_t tf = -1;
 		if (i1 < m) {
 			const int64_t start = offsets[i1] > j0 ? offsets[i1] : j0;
-			if (j1 > start) tf = (i1 + offsets[i1]) / MP_TILE;
+			if (j1 > start) tf = (i1 + offsets[i1]) / tile;
 		}
 		tail_first[t] = tf;
-		span_len[t] = (tf == t) ? int32_t((i1 + offsets[i1 + 1]) / MP_TILE - t + 1) : 0;
+		span_len[t] = (tf == t) ? int32_t((i1 + offsets[i1 + 1]) / tile - t + 1) : 0;
 	}
 }
 
@@ -129,6 +131,49 @@ k_spmv_merge(MergeTables mt, const int64_t *__restrict__ offsets,
 	AccumulateY<R> epi{y};
 	for (int64_t t = blockIdx.x; t < mt.ntiles; t += gridDim.x)
 		merge_tile<R>(t, mt, offsets, indices, values, xl, epi, left, sm);
+}
+
+// Warp-tile merge path (wmerge.cuh): persistent warps, one warp tile at a
+// time, no block-wide barrier.
+#ifndef ALPB_WM_WARPS
+#define ALPB_WM_WARPS 8
+#endif
+constexpr int WM_WARPS = ALPB_WM_WARPS;  // warps per block
+#ifndef ALPB_WM_MIN_BLOCKS
+#define ALPB_WM_MIN_BLOCKS 1
+#endif
+
+// y_r = y_r (+) row sum for the rows that end in a warp tile; their old
+// values are fetched into the warp's shared memory with the tile, so that
+// finishing a row is one store instead of a dependent load and store.
+template <class R>
+struct WarpAccumulateY {
+	using T = typename R::T;
+	T *__restrict__ y;
+	T *ybuf;            // WM_TILE entries of the warp's shared memory
+	int64_t base = 0;
+	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
+		base = i0;
+		for (int k = lane; k < nrows; k += 32) ybuf[k] = y[i0 + k];
+	}
+	__device__ __forceinline__ void row(int64_t r, T v, bool has) {
+		if (has) y[r] = R::add(ybuf[r - base], v);  // foldl( y_r, row sum ), blas2.hpp:534-549
+	}
+};
+
+template <class R>
+__global__ void __launch_bounds__(32 * WM_WARPS, ALPB_WM_MIN_BLOCKS)
+k_spmv_wmerge(MergeTables mt, const int64_t *__restrict__ offsets,
+	const uint32_t *__restrict__ indices, const typename R::T *__restrict__ values,
+	const typename R::T *__restrict__ x, typename R::T *__restrict__ y, int left) {
+	__shared__ WarpSmem<R> sm[WM_WARPS];
+	__shared__ typename R::T ybuf[WM_WARPS][WM_TILE];
+	PlainX<typename R::T> xl{x};
+	WarpAccumulateY<R> epi{y, ybuf[threadIdx.x >> 5]};
+	const int w = threadIdx.x >> 5;
+	const int64_t nw = int64_t(gridDim.x) * WM_WARPS;
+	for (int64_t t = int64_t(blockIdx.x) * WM_WARPS + w; t < mt.ntiles; t += nw)
+		warp_tile<R>(t, mt, offsets, indices, values, xl, epi, left, sm[w]);
 }
 
 // ------------------------------------------------------ vector schedules --
@@ -274,9 +319,29 @@ template <class R>
 int launch_merge(const SpmvArgs &a, const alpb_spmv_plan_s &p, cudaStream_t s) {
 	using T = typename R::T;
 	if (p.ntiles == 0) return ALPB_SUCCESS;
-	k_spmv_merge<R><<<unsigned(p.ntiles), MP_BLOCK, 0, s>>>(merge_tables(p), a.offsets, a.indices,
-		reinterpret_cast<const T *>(a.values), reinterpret_cast<const T *>(a.v),
-		reinterpret_cast<T *>(a.u), a.left);
+	if (p.tile == WM_TILE) {
+		static int blocks_per_sm = 0;
+		if (!blocks_per_sm) {
+			ALPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
+				k_spmv_wmerge<R>, 32 * WM_WARPS, 0));
+			if (blocks_per_sm < 1) blocks_per_sm = 1;
+		}
+		int64_t grid = (p.ntiles + WM_WARPS - 1) / WM_WARPS;
+		const int64_t cap = int64_t(sm_count()) * blocks_per_sm;
+		if (grid > cap) grid = cap;
+		const MergeTables mt = merge_tables(p);
+		k_spmv_wmerge<R><<<unsigned(grid), 32 * WM_WARPS, 0, s>>>(mt, a.offsets, a.indices,
+			reinterpret_cast<const T *>(a.values), reinterpret_cast<const T *>(a.v),
+			reinterpret_cast<T *>(a.u), a.left);
+		ALPB_LAUNCHED();
+		// rows crossing tiles: one lane per 32 tiles' worth of first tiles
+		k_wm_fixup<R><<<grid_for((p.ntiles + 31) / 32 * 32, 256), 256, 0, s>>>(mt,
+			AccumulateY<R>{reinterpret_cast<T *>(a.u)});
+	} else {
+		k_spmv_merge<R><<<unsigned(p.ntiles), MP_BLOCK, 0, s>>>(merge_tables(p), a.offsets,
+			a.indices, reinterpret_cast<const T *>(a.values), reinterpret_cast<const T *>(a.v),
+			reinterpret_cast<T *>(a.u), a.left);
+	}
 	ALPB_LAUNCHED();
 	return ALPB_SUCCESS;
 }
@@ -370,7 +435,7 @@ int ring_value_type(int ring) {
 	return -1;
 }
 
-int plan_build(alpb_spmv_plan_s *p, const int64_t *offsets, cudaStream_t s) {
+int plan_build(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t tile, cudaStream_t s) {
 	// row-length profile
 	unsigned long long *d_max = nullptr;
 	double *d_sq = nullptr;
@@ -394,10 +459,11 @@ int plan_build(alpb_spmv_plan_s *p, const int64_t *offsets, cudaStream_t s) {
 	const double var = p->m ? hsq / double(p->m) - p->mean * p->mean : 0.0;
 	p->cv = p->mean > 0 ? sqrt(var > 0 ? var : 0.0) / p->mean : 0.0;
 	// merge-path tile table
-	p->ntiles = (p->m + p->nnz + MP_TILE - 1) / MP_TILE;
+	p->tile = tile;
+	p->ntiles = (p->m + p->nnz + tile - 1) / tile;
 	if (p->ntiles > 0) {
-		ALPB_CHECK(p->nnz + MP_TILE < (int64_t(1) << 31), ALPB_OVERFLW,
-			"alpb_spmv_plan_create: merge path tiles use 32-bit offsets (nnz %lld)",
+		ALPB_CHECK(tile != MP_TILE || p->nnz + MP_TILE < (int64_t(1) << 31), ALPB_OVERFLW,
+			"alpb_spmv_plan_create: block merge tiles use 32-bit offsets (nnz %lld)",
 			(long long) p->nnz);
 		const size_t nt = size_t(p->ntiles);
 		ALPB_CUDA(cudaMalloc(&p->tile_row, (nt + 1) * 8));
@@ -411,10 +477,10 @@ int plan_build(alpb_spmv_plan_s *p, const int64_t *offsets, cudaStream_t s) {
 		ALPB_CUDA(cudaMalloc(&p->tail_has, nt));
 		ALPB_CUDA(cudaMemsetAsync(p->counter, 0, nt * 4, s));
 		k_merge_tiles<<<grid_for(p->ntiles + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz,
-			p->ntiles, p->tile_row);
+			p->ntiles, p->tile_row, tile);
 		ALPB_LAUNCHED();
 		k_merge_tables<<<grid_for(p->ntiles, 256), 256, 0, s>>>(offsets, p->m, p->nnz, p->ntiles,
-			p->tile_row, p->head_first, p->tail_first, p->span_len);
+			p->tile_row, p->head_first, p->tail_first, p->span_len, tile);
 		ALPB_LAUNCHED();
 	}
 	return ALPB_SUCCESS;
@@ -430,6 +496,15 @@ int alpb_spmv_plan_create(alpb_spmv_plan *plan, int64_t m, int64_t nnz, const in
 	int sched, int vector_width, void *stream) {
 	ALPB_CHECK(plan != nullptr, ALPB_ILLEGAL, "alpb_spmv_plan_create: null plan");
 	*plan = nullptr;
+	return plan_create_tiles(plan, m, nnz, offsets, sched, vector_width, WM_TILE,
+		as_stream(stream));
+}
+
+} // extern "C"
+
+int alpb::plan_create_tiles(alpb_spmv_plan_s **plan, int64_t m, int64_t nnz,
+	const int64_t *offsets, int sched, int vector_width, int64_t tile, cudaStream_t s) {
+	*plan = nullptr;
 	ALPB_CHECK(m >= 0 && nnz >= 0, ALPB_ILLEGAL, "alpb_spmv_plan_create: negative size");
 	ALPB_CHECK(sched >= ALPB_SCHED_AUTO && sched <= ALPB_SCHED_VECTOR, ALPB_ILLEGAL,
 		"alpb_spmv_plan_create: schedule %d", sched);
@@ -438,7 +513,7 @@ int alpb_spmv_plan_create(alpb_spmv_plan *plan, int64_t m, int64_t nnz, const in
 	p->nnz = nnz;
 	p->offsets = offsets;
 	cudaGetDevice(&p->device);
-	int rc = plan_build(p, offsets, as_stream(stream));
+	int rc = plan_build(p, offsets, tile, s);
 	if (rc != ALPB_SUCCESS) {
 		alpb_spmv_plan_destroy(p);
 		return rc;
@@ -459,6 +534,8 @@ int alpb_spmv_plan_create(alpb_spmv_plan *plan, int64_t m, int64_t nnz, const in
 	*plan = p;
 	return ALPB_SUCCESS;
 }
+
+extern "C" {
 
 int alpb_spmv_plan_destroy(alpb_spmv_plan p) {
 	if (!p) return ALPB_SUCCESS;

@@ -11,6 +11,7 @@ struct alpb_spmv_plan_s {
 	int vw = 8;
 	int device = 0;
 	int64_t ntiles = 0;
+	int64_t tile = 0;               // merge items per tile of the tables below
 	// merge-path tables (the scratch memory of the merge-path schedule)
 	int64_t *tile_row = nullptr;    // ntiles + 1 merge-path row splits
 	int64_t *head_first = nullptr;  // ntiles
@@ -58,9 +59,15 @@ int dispatch_spmv(int ring, const SpmvArgs &a, const alpb_spmv_plan_s *p, int fo
 	cudaStream_t s);
 int ring_value_type(int ring);
 
-// merge-path geometry, shared with the fused solvers
+// merge-path geometry of the block-tile engine (merge.cuh), shared with the
+// fused solvers
 constexpr int MP_BLOCK = 256;
 constexpr int MP_IPT = 8;
 constexpr int MP_TILE = MP_BLOCK * MP_IPT;
+
+// Plan with merge tables of `tile` items per tile (MP_TILE for the block
+// engine, WM_TILE for the warp engine).
+int plan_create_tiles(alpb_spmv_plan_s **plan, int64_t m, int64_t nnz, const int64_t *offsets,
+	int sched, int vector_width, int64_t tile, cudaStream_t s);
 
 } // namespace alpb

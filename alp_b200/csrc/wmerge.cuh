@@ -1,0 +1,266 @@
+// Warp-granular merge-path tiles.
+//
+// Same merge list as merge.cuh (a tile owns a fixed number of consecutive
+// merge items, whatever the row lengths), but one warp owns one tile of
+// 32 x WM_IPT items and synchronises only with __syncwarp:
+//   1. the tile's row ends and products a_ij (*) x_j are staged in the warp's
+//      shared memory with coalesced, lane-strided loads (the epilogue may
+//      prefetch what its rows need at the same time: Epi::begin_tile);
+//   2. every lane walks WM_IPT consecutive merge items and finishes the rows
+//      whose row end it meets;
+//   3. the lanes' carries (the partial of the row each lane stops in) are
+//      combined with a segmented inclusive scan over shuffles, keyed by row:
+//      a lane's first finished row gets the carries of the lanes before it;
+//   4. a row that crosses tiles leaves one partial per tile in the tile's
+//      head or tail slot, and a second, tiny pass (k_wm_fixup) sums each
+//      such row's slots in tile order.  No atomics and no fences.
+// Every sum has a fixed order (in-lane order, scan tree, slot order): results
+// are deterministic from run to run.
+#pragma once
+#include "merge.cuh"
+
+#include <type_traits>
+
+namespace alpb {
+
+#ifndef ALPB_WM_IPT
+#define ALPB_WM_IPT 8
+#endif
+constexpr int WM_IPT = ALPB_WM_IPT;    // merge items per lane
+constexpr int WM_TILE = 32 * WM_IPT;   // merge items per warp tile
+constexpr unsigned WM_FULL = 0xffffffffu;
+
+template <class R>
+struct WarpSmem {
+	typename R::T prod[WM_TILE];
+	int32_t row_end[WM_TILE + 2];  // [k] = end of tile row k-1, relative to j0, clamped
+};
+
+template <class T>
+__device__ __forceinline__ T wm_shfl_up(T v, int off) {
+	if constexpr (std::is_same<T, bool>::value) return __shfl_up_sync(WM_FULL, int(v), off) != 0;
+	else return __shfl_up_sync(WM_FULL, v, off);
+}
+template <class T>
+__device__ __forceinline__ T wm_shfl(T v, int src) {
+	if constexpr (std::is_same<T, bool>::value) return __shfl_sync(WM_FULL, int(v), src) != 0;
+	else return __shfl_sync(WM_FULL, v, src);
+}
+template <class T>
+__device__ __forceinline__ T wm_shfl_xor(T v, int m) {
+	if constexpr (std::is_same<T, bool>::value) return __shfl_xor_sync(WM_FULL, int(v), m) != 0;
+	else return __shfl_xor_sync(WM_FULL, v, m);
+}
+
+// Value bits of a slot, read through L2 (slots are written by other SMs).
+template <class T>
+__device__ __forceinline__ T wm_load_slot(const uint64_t *p) {
+	const unsigned long long b = __ldcg(reinterpret_cast<const unsigned long long *>(p));
+	T v;
+	memcpy(&v, &b, sizeof(T));
+	return v;
+}
+
+// Shared body of a warp tile: stages the tile, walks it, scans the carries
+// and calls epi.row for every row that ends in the tile -- except the head
+// row when it started in an earlier tile (hf >= 0).  epi.begin_tile(i0,
+// nrows, lane) runs first, on every lane, for the rows [i0, i0 + nrows) that
+// end in the tile (its shared-memory writes are visible to epi.row).  Leaves in every lane:
+// head_v/head_h (the partial of row i0 up to its end, in the lane whose first
+// finished row is row 0) and sv/sh (lane 31: the partial of the tail row).
+template <class R, class XL, class Epi>
+__device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
+	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
+	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
+	WarpSmem<R> &sm, int64_t i0, int64_t i1, int64_t hf, int &first_row,
+	typename R::T &head_v, bool &head_h, typename R::T &sv, bool &sh) {
+	using T = typename R::T;
+	const int lane = threadIdx.x & 31;
+	const int64_t m = mt.m, nnz = mt.nnz;
+	int64_t d0, d1;
+	if (mt.tile_d) {
+		d0 = mt.tile_d[t];
+		d1 = mt.tile_d[t + 1];
+	} else {
+		d0 = t * WM_TILE;
+		d1 = d0 + WM_TILE;
+		if (d1 > m + nnz) d1 = m + nnz;
+	}
+	const int64_t j0 = d0 - i0, j1 = d1 - i1;
+	const int nrows = int(i1 - i0);
+	const int nnzt = int(j1 - j0);
+	epi.begin_tile(i0, nrows, lane);
+
+	// row ends, relative to j0; clamped to the tile (the walk compares them
+	// with positions <= nnzt only)
+	for (int k = lane; k <= nrows + 1; k += 32) {
+		int64_t v;
+		if (k == 0) v = offsets[i0] - j0;
+		else {
+			const int64_t r = i0 + k;
+			v = (r <= m ? offsets[r] : j1 + 1) - j0;
+		}
+		if (v > WM_TILE + 1) v = WM_TILE + 1;
+		if (v < -1) v = -1;
+		sm.row_end[k] = int32_t(v);
+	}
+	{
+		uint32_t col[WM_IPT];
+		T a[WM_IPT];
+#pragma unroll
+		for (int u = 0; u < WM_IPT; ++u) {
+			const int k = lane + 32 * u;
+			if (k < nnzt) {
+				col[u] = __ldcs(indices + j0 + k);
+				a[u] = values ? __ldcs(values + j0 + k) : R::one();
+			}
+		}
+#pragma unroll
+		for (int u = 0; u < WM_IPT; ++u) {
+			const int k = lane + 32 * u;
+			if (k < nnzt) {
+				const T xv = xl(col[u]);
+				sm.prod[k] = left ? R::mull(xv, a[u]) : R::mulr(a[u], xv);
+			}
+		}
+	}
+	__syncwarp();
+
+	// merge-path split of this lane's WM_IPT items
+	const int items = nrows + nnzt;
+	int dl = lane * WM_IPT;
+	if (dl > items) dl = items;
+	int ti, tj;
+	{
+		int lo = dl - nnzt > 0 ? dl - nnzt : 0, hi = dl < nrows ? dl : nrows;
+		while (lo < hi) {
+			const int pivot = (lo + hi) >> 1;
+			if (sm.row_end[pivot + 1] <= dl - pivot - 1) lo = pivot + 1; else hi = pivot;
+		}
+		ti = lo;
+		tj = dl - lo;
+	}
+	int dend = dl + WM_IPT;
+	if (dend > items) dend = items;
+
+	T acc = R::zero();
+	bool has = false;
+	first_row = -1;
+	T first_val = R::zero();
+	bool first_has = false;
+	for (int d = dl; d < dend; ++d) {
+		if (tj < sm.row_end[ti + 1]) {
+			acc = R::add(acc, sm.prod[tj]);
+			has = true;
+			++tj;
+		} else {
+			if (first_row < 0) {
+				first_row = ti;
+				first_val = acc;
+				first_has = has;
+			} else {
+				epi.row(i0 + ti, acc, has);
+			}
+			acc = R::zero();
+			has = false;
+			++ti;
+		}
+	}
+
+	// segmented inclusive scan of the carries, keyed by the row each lane
+	// stops in (rows are non-decreasing over lanes)
+	sv = acc;
+	sh = has;
+#pragma unroll
+	for (int off = 1; off < 32; off <<= 1) {
+		const T v = wm_shfl_up(sv, off);
+		const bool h = wm_shfl_up(sh, off);
+		const int r = __shfl_up_sync(WM_FULL, ti, off);
+		if (lane >= off && r == ti) {
+			sv = R::add(v, sv);
+			sh = sh || h;
+		}
+	}
+	// carry into this lane: the scan of lane-1, whose stop row is this lane's
+	// start row
+	T cin = wm_shfl_up(sv, 1);
+	bool cin_h = wm_shfl_up(sh, 1);
+	if (lane == 0) {
+		cin = R::zero();
+		cin_h = false;
+	}
+	head_v = R::zero();
+	head_h = false;
+	if (first_row >= 0) {
+		head_v = R::add(cin, first_val);
+		head_h = cin_h || first_has;
+		if (!(first_row == 0 && hf >= 0)) epi.row(i0 + first_row, head_v, head_h);
+	}
+	__syncwarp();  // the warp's shared memory is reused by its next tile
+}
+
+// One warp tile t for the two-pass SpMV: rows that end in the tile are
+// finished here (epi.row); a row crossing tiles leaves this tile's partial in
+// head_val[t] (the row ends here) or tail_val[t] (it continues), and
+// k_wm_fixup finishes it.  A spanning row always holds nonzeroes, so its
+// partials need no presence flag: an empty partial is the additive identity.
+template <class R, class XL, class Epi>
+__device__ __forceinline__ void warp_tile(int64_t t, const MergeTables &mt,
+	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
+	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
+	WarpSmem<R> &sm) {
+	using T = typename R::T;
+	const int lane = threadIdx.x & 31;
+	const int64_t i0 = mt.tile_row[t], i1 = mt.tile_row[t + 1];
+	const int64_t hf = mt.head_first[t], tf = mt.tail_first[t];
+	int first_row;
+	T head_v, sv;
+	bool head_h, sh;
+	wm_core<R>(t, mt, offsets, indices, values, xl, epi, left, sm, i0, i1, hf, first_row, head_v,
+		head_h, sv, sh);
+	if (hf >= 0 && first_row == 0) store_bits<T>(mt.head_val + t, head_v);
+	if (tf >= 0 && lane == 31) store_bits<T>(mt.tail_val + t, sv);
+}
+
+// Second pass: every row that crosses tiles, y_r = y_r (+) its slots summed
+// in tile order (tail slots of its first..last-1 tiles, head slot of its last
+// tile).  One lane per first tile for spans up to 32 tiles; the whole warp
+// for longer ones.
+template <class R, class Epi>
+__global__ void __launch_bounds__(256) k_wm_fixup(MergeTables mt, Epi epi) {
+	using T = typename R::T;
+	const int lane = threadIdx.x & 31;
+	const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+	const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	for (int64_t base = warp * 32; base < mt.ntiles; base += nwarps * 32) {
+		const int64_t t = base + lane;
+		const int32_t n = t < mt.ntiles ? mt.span_len[t] : 0;
+		if (n > 0 && n <= 32) {
+			T v = R::zero();
+			for (int64_t k = t; k < t + n - 1; ++k) v = R::add(v, wm_load_slot<T>(mt.tail_val + k));
+			v = R::add(v, wm_load_slot<T>(mt.head_val + t + n - 1));
+			epi.row(mt.tile_row[t + 1], v, true);
+		}
+		unsigned long_rows = __ballot_sync(WM_FULL, n > 32);
+		while (long_rows) {
+			const int src = __ffs(long_rows) - 1;
+			long_rows &= long_rows - 1;
+			const int64_t f = base + src;
+			const int32_t nn = __shfl_sync(WM_FULL, n, src);
+			T v = R::zero();
+			for (int64_t k = f + lane; k < f + nn - 1; k += 32)
+				v = R::add(v, wm_load_slot<T>(mt.tail_val + k));
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) {
+				const T vo = wm_shfl_xor(v, o);
+				v = R::add(v, vo);
+			}
+			if (lane == 0) {
+				v = R::add(v, wm_load_slot<T>(mt.head_val + f + nn - 1));
+				epi.row(mt.tile_row[f + 1], v, true);
+			}
+		}
+	}
+}
+
+} // namespace alpb

@@ -332,7 +332,8 @@ ALPB_API int alpb_foldl_f64(double *x, int op, int64_t n, const double *y, doubl
  * dense); x == NULL or y == NULL means the scalar alpha or beta.  An optional
  * mask (masked != 0) restricts the indices, as utils::interpretMask reads it
  * under descr.  Kinds:
- *   SET    z_i = x_i wherever x_i exists
+ *   SET    z_i = x_i wherever x_i exists (z_i = i under the use_index bit of
+ *          descr, as reference/io.hpp setIndexOrValue)
  *   FOLDL  z_i = z_i op x_i where both exist; a monoid also folds into absent
  *          z_i from its identity
  *   FOLDR  z_i = x_i op z_i, likewise

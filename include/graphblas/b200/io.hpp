@@ -105,7 +105,7 @@ namespace grb {
 				if( zt < 0 || mt < 0 ) { return UNSUPPORTED; }
 				x.b200_device_ready();
 				if( mask ) { mask->b200_device_ready(); }
-				if( !mask ) {
+				if( !mask && !( descr & descriptors::use_index ) ) {
 					const RC rc = check( alpb_set_scalar( x.b200_values(), zt, n, static_cast< double >( val ),
 						x.b200_flags(), x.b200_counter(), stream() ), "set" );
 					if( rc == SUCCESS ) { x.b200_mark_dense(); }
@@ -113,9 +113,10 @@ namespace grb {
 				}
 				const RC rc = check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0,
 					descr, n, x.b200_values(), zt, x.b200_flags(), x.b200_counter(),
-					mask->b200_values(), mask->b200_flags_or_dense(), mt, 1,
+					mask ? mask->b200_values() : nullptr,
+					mask ? mask->b200_flags_or_dense() : nullptr, mt, mask ? 1 : 0,
 					nullptr, zt, nullptr, static_cast< double >( val ),
-					nullptr, zt, nullptr, 0.0, stream() ), "set (masked)" );
+					nullptr, zt, nullptr, 0.0, stream() ), "set" );
 				x.b200_refresh();
 				return rc;
 			}

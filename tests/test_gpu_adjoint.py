@@ -3,7 +3,14 @@ over the C-ABI (test code only), against
   * gradients assembled from the reference algorithm: CG forward, CG on A^T,
     then -lambda_i x_j on the host (the C restatement of
     algorithms::conjugate_gradient), and
-  * central finite differences with h = 1e-6.
+  * central finite differences with h = 1e-6: [L(theta+h) - L(theta-h)] / 2h.
+    Subtracting two separately solved losses would lose every digit the
+    solver leaves (~1e-14 relative, divided by 2h), so the difference is
+    formed exactly instead: with x+ = x(theta+h), x- = x(theta-h),
+        A(theta+h) (x+ - x-) = (A(theta-h) - A(theta+h)) x-
+    whose right-hand side has two nonzeros of size 2h; solving it for
+    d = x+ - x- keeps d to ~1e-14 RELATIVE, and
+        L(theta+h) - L(theta-h) = 0.5 d . (2 (x- - x*) + d).
 
 Gradients are per stored entry: dL/dA_ij = -lambda_i x_j.  A is symmetric
 (a_ij = a_ji keyed by the pair), so a finite difference perturbs the pair
@@ -139,37 +146,47 @@ def test_adjoint_matches_central_differences(cuda):
     tkey = i.astype(np.int64) * A.m + rows
     partner = order[np.searchsorted(key[order], tkey)]
 
-    def loss(vals):
-        xx = cg_solve(A, vals, b, to_floor=True)
-        return 0.5 * float(((xx - xs) ** 2).sum())
-
     h = 1e-6
     rng = np.random.default_rng(0)
     picks = rng.choice(A.nnz, size=64, replace=False)
     base = A.values.clone()
+    x_base = cg_solve(A, base, b, to_floor=True)
+
+    def loss_diff(vp, vm, dvals):
+        """L(vp) - L(vm) where A(vp) - A(vm) has the entries dvals (stored
+        position, value)."""
+        xm = cg_solve(A, vm, b, to_floor=True)
+        rhs = torch.zeros_like(b)        # (A(vm) - A(vp)) xm
+        for pos, dv in dvals:
+            rhs[int(rows[pos])] -= dv * xm[int(i[pos])]
+        d = cg_solve(A, vp, rhs, to_floor=True)
+        return 0.5 * float((d * (2 * (xm - xs) + d)).sum())
+
     worst = 0.0
     for k in picks:
         p = int(partner[k])
         vp, vm = base.clone(), base.clone()
         vp[int(k)] += h
         vm[int(k)] -= h
+        dvals = [(int(k), 2 * h)]
         if p != k:
             vp[p] += h
             vm[p] -= h
-        fd = (loss(vp) - loss(vm)) / (2 * h)
+            dvals.append((p, 2 * h))
+        fd = loss_diff(vp, vm, dvals) / (2 * h)
         an = grad[k] + (grad[p] if p != k else 0.0)
         err = abs(fd - an) / max(abs(an), 1e-3 * np.abs(grad).max())
         worst = max(worst, err)
     assert worst < 1e-5, worst
-    # dL/db on a few entries
+    # dL/db on a few entries: x(b + h e_j) - x(b - h e_j) = A^{-1} (2h e_j)
     gb = bb.grad.cpu().numpy()
     for j in rng.choice(A.m, size=8, replace=False):
-        bp, bm = b.clone(), b.clone()
-        bp[int(j)] += h
-        bm[int(j)] -= h
-        xp, xm = cg_solve(A, base, bp, to_floor=True), cg_solve(A, base, bm, to_floor=True)
-        fd = (0.5 * float(((xp - xs) ** 2).sum()) - 0.5 * float(((xm - xs) ** 2).sum())) / (2 * h)
-        assert abs(fd - gb[j]) <= 1e-5 * max(abs(gb[j]), 1e-3 * np.abs(gb).max())
+        e = torch.zeros_like(b)
+        e[int(j)] = 2 * h
+        d = cg_solve(A, base, e, to_floor=True)
+        xm = x_base - 0.5 * d
+        fd = 0.5 * float((d * (2 * (xm - xs) + d)).sum()) / (2 * h)
+        assert abs(fd - gb[j]) <= 1e-5 * max(abs(gb[j]), 1e-3 * np.abs(gb).max()), (j, fd, gb[j])
 
 
 def test_cg_grad_entry_point(cuda):
