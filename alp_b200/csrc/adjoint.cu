@@ -9,40 +9,49 @@
 // transpose product needs neither atomics nor a second orientation build
 // beyond the CCS the reference also keeps (reference/matrix.hpp:1298-1301).
 // The gradient with respect to the stored values is a pattern-masked
-// SDDMM (sampled dense-dense product) over A's CRS, on merge-path tiles so
-// that every nonzero is written once, coalesced, whatever the row lengths.
+// SDDMM (sampled dense-dense product) over A's CRS, on warp merge-path tiles
+// so that every nonzero is written once, coalesced, whatever the row lengths.
 #include "common.cuh"
 #include "merge.cuh"
+#include "wmerge.cuh"
 #include "spmv.cuh"
 
 #include <cmath>
 
 namespace alpb {
 
-// out[k] = alpha * lam[row(k)] * x[col(k)] for every stored k (CRS order)
-__global__ void __launch_bounds__(MP_BLOCK)
+// out[k] = alpha * lam[row(k)] * x[col(k)] for every stored k (CRS order),
+// one warp merge tile (wmerge.cuh geometry) at a time
+constexpr int SDDMM_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * SDDMM_WARPS)
 k_sddmm(MergeTables mt, const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
 	const double *__restrict__ lam, const double *__restrict__ x, double alpha,
 	double *__restrict__ out) {
-	__shared__ int32_t row_end[MP_TILE + 2];
+	__shared__ int32_t row_end_s[SDDMM_WARPS][WM_TILE + 2];
+	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	int32_t *row_end = row_end_s[w];
 	const int64_t m = mt.m, nnz = mt.nnz;
-	for (int64_t t = blockIdx.x; t < mt.ntiles; t += gridDim.x) {
+	for (int64_t t = int64_t(blockIdx.x) * SDDMM_WARPS + w; t < mt.ntiles;
+		 t += int64_t(gridDim.x) * SDDMM_WARPS) {
 		const int64_t i0 = mt.tile_row[t], i1 = mt.tile_row[t + 1];
-		int64_t d0 = t * MP_TILE, d1 = d0 + MP_TILE;
+		int64_t d0 = t * WM_TILE, d1 = d0 + WM_TILE;
 		if (d1 > m + nnz) d1 = m + nnz;
 		const int64_t j0 = d0 - i0, j1 = d1 - i1;
 		const int nrows = int(i1 - i0), nnzt = int(j1 - j0);
-		for (int k = threadIdx.x; k <= nrows + 1; k += blockDim.x) {
+		for (int k = lane; k <= nrows + 1; k += 32) {
 			int64_t v;
-			if (k == 0) v = offsets[i0];
+			if (k == 0) v = offsets[i0] - j0;
 			else {
 				const int64_t r = i0 + k;
-				v = r <= m ? offsets[r] : j1 + 1;
+				v = (r <= m ? offsets[r] : j1 + 1) - j0;
 			}
-			row_end[k] = int32_t(v - j0);
+			if (v > WM_TILE + 1) v = WM_TILE + 1;
+			if (v < -1) v = -1;
+			row_end[k] = int32_t(v);
 		}
-		__syncthreads();
-		for (int k = threadIdx.x; k < nnzt; k += blockDim.x) {
+		__syncwarp();
+		for (int k = lane; k < nnzt; k += 32) {
 			// tile row of nonzero k: the first r with end(r) > k
 			int lo = 0, hi = nrows;
 			while (lo < hi) {
@@ -53,7 +62,7 @@ k_sddmm(MergeTables mt, const int64_t *__restrict__ offsets, const uint32_t *__r
 			const uint32_t j = __ldcs(indices + j0 + k);
 			__stcs(out + j0 + k, alpha * __ldg(lam + i) * __ldg(x + j));
 		}
-		__syncthreads();
+		__syncwarp();
 	}
 }
 
@@ -80,18 +89,18 @@ int alpb_sddmm(alpb_spmv_plan plan, int64_t m, int64_t nnz, const int64_t *offse
 	if (m == 0 || nnz == 0) return ALPB_SUCCESS;
 	cudaStream_t s = as_stream(stream);
 	if (plan)
-		ALPB_CHECK(plan->m == m && plan->nnz == nnz, ALPB_MISMATCH,
+		ALPB_CHECK(plan->m == m && plan->nnz == nnz && plan->tile == WM_TILE, ALPB_MISMATCH,
 			"alpb_sddmm: plan was made for another storage");
 	alpb_spmv_plan own = nullptr;
-	if (!plan || plan->tile != MP_TILE) {
-		// k_sddmm runs block tiles: it needs tables cut at MP_TILE
-		int rc = plan_create_tiles(&own, m, nnz, offsets, ALPB_SCHED_MERGE_PATH, 0, MP_TILE, s);
+	if (!plan) {
+		int rc = plan_create_tiles(&own, m, nnz, offsets, ALPB_SCHED_MERGE_PATH, 0, WM_TILE, s);
 		if (rc != ALPB_SUCCESS) return rc;
 		plan = own;
 	}
-	const unsigned grid = unsigned(plan->ntiles < int64_t(sm_count()) * 8 ? plan->ntiles
-		: int64_t(sm_count()) * 8);
-	k_sddmm<<<grid, MP_BLOCK, 0, s>>>(merge_tables(*plan), offsets, indices, lam, x, alpha, out);
+	int64_t grid = (plan->ntiles + SDDMM_WARPS - 1) / SDDMM_WARPS;
+	if (grid > int64_t(sm_count()) * 8) grid = int64_t(sm_count()) * 8;
+	k_sddmm<<<unsigned(grid), 32 * SDDMM_WARPS, 0, s>>>(merge_tables(*plan), offsets, indices, lam,
+		x, alpha, out);
 	ALPB_LAUNCHED();
 	if (own) {
 		ALPB_CUDA(cudaStreamSynchronize(s));

@@ -7,8 +7,8 @@
 // separated by a bounded grid barrier, with every scalar kept on the device:
 //
 //   A: temp = A u_new, gathering u_new_j = r_j + gamma u_old_j on the fly
-//      (merge-path tiles, merge.cuh); the row epilogue writes temp_i and
-//      u_new_i and forms the terms of beta = temp . u_new.
+//      (warp merge-path tiles, wmerge.cuh); the row epilogue writes temp_i
+//      and u_new_i and forms the terms of beta = temp . u_new.
 //   B: alpha = sigma / beta; x += alpha u_new; r -= alpha temp; r . r.
 //
 // The u update of the reference (u = r + (r.r / sigma) u, :455-468) is thus
@@ -18,6 +18,7 @@
 // the returned residual is r.r.
 #include "common.cuh"
 #include "merge.cuh"
+#include "wmerge.cuh"
 #include "persist.cuh"
 #include "spmv.cuh"
 
@@ -42,36 +43,39 @@ struct CgArgs {
 	const double *values;
 	const double *b;
 	double *x, *r, *u0, *u1, *temp;
-	double *own, *span, *own2, *span2;  // [ntiles] tile terms / spanning-row terms
-	double *blk;                        // [grid] block partials of r.r
+	double *blk;  // [4][grid] block partials: prelude r.r, prelude b.b, beta, r.r
 	int64_t n, max_iter;
 	double tol;
 	CgState *st;
 };
 
+constexpr int CG_WARPS = 4;
+
+// Shared memory of one warp: the tile engine's staging plus the epilogue's
+// prefetched vector entries for the rows that end in the tile.
+struct CgWarpSmem {
+	WarpSmem<RF> tile;
+	double p0[WM_TILE];
+	double p1[WM_TILE];
+};
+
 struct PreludeEpi {
 	const CgArgs *a;
+	CgWarpSmem *sm;
+	int64_t base = 0;
 	double acc_rr = 0.0, acc_bb = 0.0;
-	__device__ __forceinline__ void terms(int64_t i, double v, bool has, double &rr, double &bb) {
+	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
+		base = i0;
+		for (int k = lane; k < nrows; k += 32) sm->p0[k] = a->b[i0 + k];
+	}
+	__device__ __forceinline__ void row(int64_t i, double v, bool has) {
 		const double t = has ? 0.0 + v : 0.0;      // temp = 0; temp += A x
-		const double bi = a->b[i];
+		const double bi = sm->p0[i - base];
 		const double ri = (0.0 + bi) - t;           // r = 0; r += b; r -= temp
 		a->r[i] = ri;
 		a->u0[i] = 0.0;
-		rr = ri * ri;
-		bb = bi * bi;
-	}
-	__device__ __forceinline__ void row(int64_t i, double v, bool has) {
-		double rr, bb;
-		terms(i, v, has, rr, bb);
-		acc_rr += rr;
-		acc_bb += bb;
-	}
-	__device__ __forceinline__ void row_span(int64_t first, int64_t i, double v, bool has) {
-		double rr, bb;
-		terms(i, v, has, rr, bb);
-		a->span[first] = rr;
-		a->span2[first] = bb;
+		acc_rr += ri * ri;
+		acc_bb += bi * bi;
 	}
 };
 
@@ -87,53 +91,74 @@ struct GatherU {
 
 struct IterEpi {
 	const CgArgs *a;
+	CgWarpSmem *sm;
 	const double *u_old;
 	double *u_new;
 	double gamma;
+	int64_t base = 0;
 	double acc = 0.0;
-	__device__ __forceinline__ double term(int64_t i, double v, bool has) {
+	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
+		base = i0;
+		for (int k = lane; k < nrows; k += 32) {
+			sm->p0[k] = __ldcg(a->r + i0 + k);
+			sm->p1[k] = __ldcg(u_old + i0 + k);
+		}
+	}
+	__device__ __forceinline__ void row(int64_t i, double v, bool has) {
 		const double t = has ? 0.0 + v : 0.0;      // temp = 0; temp += A u
 		a->temp[i] = t;
-		const double un = __ldcg(a->r + i) + gamma * __ldcg(u_old + i);
+		const double un = sm->p0[i - base] + gamma * sm->p1[i - base];
 		u_new[i] = un;
-		return t * un;
-	}
-	__device__ __forceinline__ void row(int64_t i, double v, bool has) { acc += term(i, v, has); }
-	__device__ __forceinline__ void row_span(int64_t first, int64_t i, double v, bool has) {
-		a->span[first] = term(i, v, has);
+		acc += t * un;
 	}
 };
 
-__global__ void __launch_bounds__(MP_BLOCK) k_cg(CgArgs a) {
-	__shared__ MergeSmem<RF> sm;
+// Rows are finished by fixed tiles (warp_tile_ordered) and every partial is
+// reduced in a fixed order (lane terms in tile order, block_sum, then the
+// block partials in block order): the iterates are deterministic for a given
+// grid size.
+__global__ void __launch_bounds__(32 * CG_WARPS, 6) k_cg(CgArgs a) {
+	__shared__ CgWarpSmem sm[CG_WARPS];
 	__shared__ double red[33];
 	CgState *st = a.st;
+	int *err = &st->gs.err;
 	const int64_t G = gridDim.x;
 	const int64_t nt = a.mt.ntiles;
-	for (int64_t t = blockIdx.x; t < nt; t += G) {
-		a.span[t] = 0.0;
-		a.span2[t] = 0.0;
-	}
+	const int w = threadIdx.x >> 5;
+	const int64_t gw = int64_t(blockIdx.x) * CG_WARPS + w, nw = G * CG_WARPS;
+	double *blk_rr0 = a.blk, *blk_bb0 = a.blk + G, *blk_beta = a.blk + 2 * G,
+		   *blk_rr = a.blk + 3 * G;
+	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nt;
+		 t += G * blockDim.x)
+		a.mt.ready[t] = 0;
 	if (!grid_sync(&st->gs)) return;
+	int32_t epoch = 0;
 
 	// prelude: r = b - A x, u = r (by gamma = 0 below), sigma = r.r, |b|^2
 	{
-		PreludeEpi epi{&a};
+		PreludeEpi epi{&a, &sm[w]};
 		PlainX<double> xl{a.x};
-		for (int64_t t = blockIdx.x; t < nt; t += G) {
-			epi.acc_rr = epi.acc_bb = 0.0;
-			merge_tile<RF>(t, a.mt, a.offsets, a.indices, a.values, xl, epi, 0, sm);
-			const double s1 = block_sum(epi.acc_rr, red);
-			const double s2 = block_sum(epi.acc_bb, red);
-			if (threadIdx.x == 0) {
-				a.own[t] = s1;
-				a.own2[t] = s2;
-			}
+		++epoch;
+		int64_t t = gw;
+		WmMeta g = wm_meta(a.mt, t);
+		while (t < nt) {
+			const WmMeta next = wm_meta(a.mt, t + nw);
+			if (!warp_tile_ordered<RF>(t, g, a.mt, a.offsets, a.indices, a.values, xl, epi, 0,
+					sm[w].tile, epoch, err))
+				break;
+			t += nw;
+			g = next;
+		}
+		const double s1 = block_sum(epi.acc_rr, red);
+		const double s2 = block_sum(epi.acc_bb, red);
+		if (threadIdx.x == 0) {
+			blk_rr0[blockIdx.x] = s1;
+			blk_bb0[blockIdx.x] = s2;
 		}
 	}
 	if (!grid_sync(&st->gs)) return;
-	double sigma = block_sum_array(a.own, nt, red) + block_sum_array(a.span, nt, red);
-	const double bnorm = block_sum_array(a.own2, nt, red) + block_sum_array(a.span2, nt, red);
+	double sigma = block_sum_array(blk_rr0, G, red);
+	const double bnorm = block_sum_array(blk_bb0, G, red);
 	const double tol_abs = a.tol * sqrt(bnorm);
 
 	const int64_t chunk = (a.n + G - 1) / G;
@@ -147,18 +172,25 @@ __global__ void __launch_bounds__(MP_BLOCK) k_cg(CgArgs a) {
 		++iter;
 		// phase A: temp = A u_new, u_new = r + gamma u_old, beta terms
 		{
-			IterEpi epi{&a, u_old, u_new, gamma};
+			IterEpi epi{&a, &sm[w], u_old, u_new, gamma};
 			GatherU xl{a.r, u_old, gamma};
-			for (int64_t t = blockIdx.x; t < nt; t += G) {
-				epi.acc = 0.0;
-				merge_tile<RF>(t, a.mt, a.offsets, a.indices, a.values, xl, epi, 0, sm);
-				const double s = block_sum(epi.acc, red);
-				if (threadIdx.x == 0) a.own[t] = s;
+			++epoch;
+			int64_t t = gw;
+			WmMeta g = wm_meta(a.mt, t);
+			while (t < nt) {
+				const WmMeta next = wm_meta(a.mt, t + nw);
+				if (!warp_tile_ordered<RF>(t, g, a.mt, a.offsets, a.indices, a.values, xl, epi, 0,
+						sm[w].tile, epoch, err))
+					break;
+				t += nw;
+				g = next;
 			}
+			const double s = block_sum(epi.acc, red);
+			if (threadIdx.x == 0) blk_beta[blockIdx.x] = s;
 		}
 		if (!grid_sync(&st->gs)) return;
 		// phase B: alpha = sigma / beta, x += alpha u, r -= alpha temp, r.r
-		const double beta = block_sum_array(a.own, nt, red) + block_sum_array(a.span, nt, red);
+		const double beta = block_sum_array(blk_beta, G, red);
 		const double alpha = sigma / beta;
 		double part = 0.0;
 		for (int64_t i = rb + threadIdx.x; i < re; i += blockDim.x) {
@@ -169,9 +201,9 @@ __global__ void __launch_bounds__(MP_BLOCK) k_cg(CgArgs a) {
 			part += ri * ri;
 		}
 		part = block_sum(part, red);
-		if (threadIdx.x == 0) a.blk[blockIdx.x] = part;
+		if (threadIdx.x == 0) blk_rr[blockIdx.x] = part;
 		if (!grid_sync(&st->gs)) return;
-		rr = block_sum_array(a.blk, G, red);
+		rr = block_sum_array(blk_rr, G, red);
 		if (sqrt(rr) < tol_abs || iter >= a.max_iter) break;
 		gamma = rr / sigma;  // alpha = beta / sigma in the reference's naming
 		sigma = rr;
@@ -203,31 +235,26 @@ extern "C" int alpb_cg_solve(int64_t n, const int64_t *row_ptr, const uint32_t *
 	if (n == 0) return ALPB_SUCCESS;
 	cudaStream_t s = as_stream(stream);
 	if (plan)
-		ALPB_CHECK(plan->m == n && plan->offsets == row_ptr, ALPB_MISMATCH,
-			"alpb_cg_solve: plan was made for another storage");
+		ALPB_CHECK(plan->m == n && plan->offsets == row_ptr && plan->tile == WM_TILE,
+			ALPB_MISMATCH, "alpb_cg_solve: plan was made for another storage");
 	alpb_spmv_plan own_plan = nullptr;
-	if (!plan || plan->tile != MP_TILE) {
-		// the fused kernel runs block tiles: it needs tables cut at MP_TILE
+	if (!plan) {
 		int64_t nnz = 0;
 		ALPB_CUDA(cudaMemcpyAsync(&nnz, row_ptr + n, 8, cudaMemcpyDeviceToHost, s));
 		ALPB_CUDA(cudaStreamSynchronize(s));
-		int rc = plan_create_tiles(&own_plan, n, nnz, row_ptr, ALPB_SCHED_MERGE_PATH, 0, MP_TILE, s);
+		int rc = plan_create_tiles(&own_plan, n, nnz, row_ptr, ALPB_SCHED_MERGE_PATH, 0, WM_TILE, s);
 		if (rc != ALPB_SUCCESS) return rc;
 		plan = own_plan;
 	}
-	const int64_t nt = plan->ntiles;
-	int grid = cooperative_grid(k_cg, MP_BLOCK, 0, 0);
+	const int grid = solver_grid(k_cg, 32 * CG_WARPS, plan->ntiles, CG_WARPS);
 	ALPB_CHECK(grid > 0, ALPB_PANIC, "alpb_cg_solve: no cooperative occupancy");
-	// a few blocks per SM: the per-iteration scalar reductions read every
-	// tile's partial in every block
-	if (grid > 2 * sm_count()) grid = 2 * sm_count();
 	double *wk = work, *own_work = nullptr, *scratch = nullptr;
 	CgState *st = nullptr;
 	if (!wk) {
 		ALPB_CUDA(cudaMallocAsync(&own_work, size_t(4 * n) * 8, s));
 		wk = own_work;
 	}
-	ALPB_CUDA(cudaMallocAsync(&scratch, size_t(4 * nt + grid) * 8, s));
+	ALPB_CUDA(cudaMallocAsync(&scratch, size_t(4 * grid) * 8, s));
 	ALPB_CUDA(cudaMallocAsync(&st, sizeof(CgState), s));
 	ALPB_CUDA(cudaMemsetAsync(st, 0, sizeof(CgState), s));
 	CgArgs a;
@@ -241,17 +268,14 @@ extern "C" int alpb_cg_solve(int64_t n, const int64_t *row_ptr, const uint32_t *
 	a.u0 = wk + n;
 	a.u1 = wk + 2 * n;
 	a.temp = wk + 3 * n;
-	a.own = scratch;
-	a.span = scratch + nt;
-	a.own2 = scratch + 2 * nt;
-	a.span2 = scratch + 3 * nt;
-	a.blk = scratch + 4 * nt;
+	a.blk = scratch;
 	a.n = n;
 	a.max_iter = max_iter;
 	a.tol = tol;
 	a.st = st;
 	void *args[] = {&a};
-	ALPB_CUDA(cudaLaunchCooperativeKernel((void *) k_cg, dim3(grid), dim3(MP_BLOCK), args, 0, s));
+	ALPB_CUDA(cudaLaunchCooperativeKernel((void *) k_cg, dim3(grid), dim3(32 * CG_WARPS), args, 0,
+		s));
 	ALPB_LAUNCHED();
 	CgState h;
 	ALPB_CUDA(cudaMemcpyAsync(&h, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
@@ -260,7 +284,7 @@ extern "C" int alpb_cg_solve(int64_t n, const int64_t *row_ptr, const uint32_t *
 	if (own_work) ALPB_CUDA(cudaFreeAsync(own_work, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
 	if (own_plan) alpb_spmv_plan_destroy(own_plan);
-	ALPB_CHECK(h.gs.err == 0, ALPB_PANIC, "alpb_cg_solve: grid barrier timed out");
+	ALPB_CHECK(h.gs.err == 0, ALPB_PANIC, "alpb_cg_solve: a grid barrier or tile wait timed out");
 	*iterations = h.iterations;
 	*residual = h.residual;
 	if (!h.converged) {

@@ -34,6 +34,8 @@ struct MergeTables {
 	// [ntiles+1] first diagonal of each tile when tiles are cut per segment
 	// (batched solves: no tile straddles two instances); null: t * MP_TILE
 	const int64_t *tile_d = nullptr;
+	// [ntiles] publication epochs of the tail partials (warp_tile_ordered)
+	int32_t *ready = nullptr;
 };
 
 template <class T>

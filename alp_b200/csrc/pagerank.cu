@@ -11,6 +11,7 @@
 // mass, so the next gather can start right after the barrier.
 #include "common.cuh"
 #include "merge.cuh"
+#include "wmerge.cuh"
 #include "persist.cuh"
 #include "spmv.cuh"
 
@@ -34,45 +35,49 @@ struct PrArgs {
 	const int64_t *crs_ptr;
 	const double *crs_val;
 	double *pr, *rs, *next0, *next1;
-	double *own_res, *span_res, *own_dang, *span_dang;  // [ntiles]
-	double *blk;                                        // [grid]
+	double *blk;                   // [5][grid]: setup dangling mass; per iteration
+	                               // parity p, residual [1+2p] and dangling [2+2p]
 	int64_t n, max_iter;
 	double alpha, conv;
 	int init_given;
 	PrState *st;
 };
 
+constexpr int PR_WARPS = 4;
+
+struct PrWarpSmem {
+	WarpSmem<RF> tile;
+	double old_pr[WM_TILE];
+	double rs[WM_TILE];
+};
+
 struct PrEpi {
 	const PrArgs *a;
+	PrWarpSmem *sm;
 	double *next_out;
 	double d;
+	int64_t base = 0;
 	double acc_res = 0.0, acc_dang = 0.0;
-	__device__ __forceinline__ void terms(int64_t j, double v, bool has, double &res, double &dang) {
-		const double nn = has ? 0.0 + v : 0.0;       // pr_nextnext = 0; += pr_next L
-		const double old = __ldcg(a->pr + j);
-		const double nw = nn + d;                    // pr = pr_nextnext + dangling
-		a->pr[j] = nw;
-		res = old > nw ? old - nw : nw - old;
-		const double rsj = __ldg(a->rs + j);
-		if (rsj == 0.0) {                            // input of the next iteration
-			next_out[j] = 0.0;
-			dang = nw;
-		} else {
-			next_out[j] = nw * rsj;
-			dang = 0.0;
+	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
+		base = i0;
+		for (int k = lane; k < nrows; k += 32) {
+			sm->old_pr[k] = __ldcg(a->pr + i0 + k);
+			sm->rs[k] = __ldg(a->rs + i0 + k);
 		}
 	}
 	__device__ __forceinline__ void row(int64_t j, double v, bool has) {
-		double r, dg;
-		terms(j, v, has, r, dg);
-		acc_res += r;
-		acc_dang += dg;
-	}
-	__device__ __forceinline__ void row_span(int64_t first, int64_t j, double v, bool has) {
-		double r, dg;
-		terms(j, v, has, r, dg);
-		a->span_res[first] = r;
-		a->span_dang[first] = dg;
+		const double nn = has ? 0.0 + v : 0.0;       // pr_nextnext = 0; += pr_next L
+		const double old = sm->old_pr[j - base];
+		const double nw = nn + d;                    // pr = pr_nextnext + dangling
+		a->pr[j] = nw;
+		acc_res += old > nw ? old - nw : nw - old;
+		const double rsj = sm->rs[j - base];
+		if (rsj == 0.0) {                            // input of the next iteration
+			next_out[j] = 0.0;
+			acc_dang += nw;
+		} else {
+			next_out[j] = nw * rsj;
+		}
 	}
 };
 
@@ -81,39 +86,40 @@ struct GatherL2 {
 	__device__ __forceinline__ double operator()(uint32_t j) const { return __ldcg(x + j); }
 };
 
-__global__ void __launch_bounds__(MP_BLOCK) k_pagerank(PrArgs a) {
-	__shared__ MergeSmem<RF> sm;
+// One barrier per iteration; the block partials of iteration k live in the
+// parity-(k & 1) slots, so a block that already writes iteration k+1's never
+// overwrites what a slower block still reads of iteration k.
+__global__ void __launch_bounds__(32 * PR_WARPS, 6) k_pagerank(PrArgs a) {
+	__shared__ PrWarpSmem sm[PR_WARPS];
 	__shared__ double red[33];
 	PrState *st = a.st;
+	int *err = &st->gs.err;
 	const int64_t G = gridDim.x, n = a.n, nt = a.mt.ntiles;
 	const int lane = threadIdx.x & 31;
+	const int w = threadIdx.x >> 5;
+	const int64_t gw = int64_t(blockIdx.x) * PR_WARPS + w, nw = G * PR_WARPS;
 	// setup: out-degree counts of nonzero-valued entries (the pattern ring of
 	// :224-237), alpha / count (:281-289), initial guess, pre-scaled input
 	double dang = 0.0;
-	for (int64_t t = blockIdx.x; t < nt; t += G) {
-		a.span_res[t] = 0.0;
-		a.span_dang[t] = 0.0;
-	}
-	{
-		const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
-		const int64_t nw = (G * blockDim.x) >> 5;
-		for (int64_t i = warp; i < n; i += nw) {
-			const int64_t b = a.crs_ptr[i], e = a.crs_ptr[i + 1];
-			double cnt = 0.0;
-			for (int64_t k = b + lane; k < e; k += 32)
-				cnt += (a.crs_val == nullptr || a.crs_val[k] != 0.0) ? 1.0 : 0.0;
-			for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
-			if (lane == 0) {
-				const double rsi = cnt > 0.0 ? a.alpha / cnt : 0.0;
-				a.rs[i] = rsi;
-				const double p = a.init_given ? a.pr[i] : 1.0 / double(n);
-				a.pr[i] = p;
-				if (rsi == 0.0) {
-					a.next0[i] = 0.0;
-					dang += p;
-				} else {
-					a.next0[i] = p * rsi;
-				}
+	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nt;
+		 t += G * blockDim.x)
+		a.mt.ready[t] = 0;
+	for (int64_t i = gw; i < n; i += nw) {
+		const int64_t b = a.crs_ptr[i], e = a.crs_ptr[i + 1];
+		double cnt = 0.0;
+		for (int64_t k = b + lane; k < e; k += 32)
+			cnt += (a.crs_val == nullptr || a.crs_val[k] != 0.0) ? 1.0 : 0.0;
+		for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+		if (lane == 0) {
+			const double rsi = cnt > 0.0 ? a.alpha / cnt : 0.0;
+			a.rs[i] = rsi;
+			const double p = a.init_given ? a.pr[i] : 1.0 / double(n);
+			a.pr[i] = p;
+			if (rsi == 0.0) {
+				a.next0[i] = 0.0;
+				dang += p;
+			} else {
+				a.next0[i] = p * rsi;
 			}
 		}
 	}
@@ -127,21 +133,30 @@ __global__ void __launch_bounds__(MP_BLOCK) k_pagerank(PrArgs a) {
 	double *cur = a.next0, *nxt = a.next1;
 	for (;;) {
 		const double d = (a.alpha * dang + 1 - a.alpha) / double(n);  // (:390)
-		PrEpi epi{&a, nxt, d};
+		PrEpi epi{&a, &sm[w], nxt, d};
 		GatherL2 xl{cur};
-		for (int64_t t = blockIdx.x; t < nt; t += G) {
-			epi.acc_res = epi.acc_dang = 0.0;
-			merge_tile<RF>(t, a.mt, a.ccs_ptr, a.ccs_row, a.ccs_val, xl, epi, 1, sm);
-			const double s1 = block_sum(epi.acc_res, red);
-			const double s2 = block_sum(epi.acc_dang, red);
-			if (threadIdx.x == 0) {
-				a.own_res[t] = s1;
-				a.own_dang[t] = s2;
-			}
+		const int32_t epoch = int32_t(iter + 1);
+		int64_t t = gw;
+		WmMeta g = wm_meta(a.mt, t);
+		while (t < nt) {
+			const WmMeta next = wm_meta(a.mt, t + nw);
+			if (!warp_tile_ordered<RF>(t, g, a.mt, a.ccs_ptr, a.ccs_row, a.ccs_val, xl, epi, 1,
+					sm[w].tile, epoch, err))
+				break;
+			t += nw;
+			g = next;
+		}
+		double *blk_res = a.blk + (1 + 2 * (iter & 1)) * G;
+		double *blk_dang = a.blk + (2 + 2 * (iter & 1)) * G;
+		const double s1 = block_sum(epi.acc_res, red);
+		const double s2 = block_sum(epi.acc_dang, red);
+		if (threadIdx.x == 0) {
+			blk_res[blockIdx.x] = s1;
+			blk_dang[blockIdx.x] = s2;
 		}
 		if (!grid_sync(&st->gs)) return;
-		residual = block_sum_array(a.own_res, nt, red) + block_sum_array(a.span_res, nt, red);
-		dang = block_sum_array(a.own_dang, nt, red) + block_sum_array(a.span_dang, nt, red);
+		residual = block_sum_array(blk_res, G, red);
+		dang = block_sum_array(blk_dang, G, red);
 		++iter;
 		if (a.conv != 0.0 && residual <= a.conv) break;   // (:490)
 		if (iter >= a.max_iter) break;
@@ -173,11 +188,9 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 	ALPB_CUDA(cudaMemcpyAsync(&nnz, ccs_col_ptr + n, 8, cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
 	alpb_spmv_plan plan = nullptr;
-	int rc = plan_create_tiles(&plan, n, nnz, ccs_col_ptr, ALPB_SCHED_MERGE_PATH, 0, MP_TILE, s);
+	int rc = plan_create_tiles(&plan, n, nnz, ccs_col_ptr, ALPB_SCHED_MERGE_PATH, 0, WM_TILE, s);
 	if (rc != ALPB_SUCCESS) return rc;
-	const int64_t nt = plan->ntiles;
-	int grid = cooperative_grid(k_pagerank, MP_BLOCK, 0, 0);
-	if (grid > 2 * sm_count()) grid = 2 * sm_count();
+	const int grid = solver_grid(k_pagerank, 32 * PR_WARPS, plan->ntiles, PR_WARPS);
 	if (grid <= 0) {
 		alpb_spmv_plan_destroy(plan);
 		set_error("alpb_pagerank: no cooperative occupancy");
@@ -185,7 +198,7 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 	}
 	double *scratch = nullptr;
 	PrState *st = nullptr;
-	ALPB_CUDA(cudaMallocAsync(&scratch, size_t(3 * n + 4 * nt + grid) * 8, s));
+	ALPB_CUDA(cudaMallocAsync(&scratch, size_t(3 * n + 5 * int64_t(grid)) * 8, s));
 	ALPB_CUDA(cudaMallocAsync(&st, sizeof(PrState), s));
 	ALPB_CUDA(cudaMemsetAsync(st, 0, sizeof(PrState), s));
 	PrArgs a;
@@ -199,11 +212,7 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 	a.rs = scratch;
 	a.next0 = scratch + n;
 	a.next1 = scratch + 2 * n;
-	a.own_res = scratch + 3 * n;
-	a.span_res = a.own_res + nt;
-	a.own_dang = a.span_res + nt;
-	a.span_dang = a.own_dang + nt;
-	a.blk = a.span_dang + nt;
+	a.blk = scratch + 3 * n;
 	a.n = n;
 	a.max_iter = max_iter;
 	a.alpha = alpha;
@@ -211,7 +220,8 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 	a.init_given = init_given;
 	a.st = st;
 	void *args[] = {&a};
-	ALPB_CUDA(cudaLaunchCooperativeKernel((void *) k_pagerank, dim3(grid), dim3(MP_BLOCK), args, 0, s));
+	ALPB_CUDA(cudaLaunchCooperativeKernel((void *) k_pagerank, dim3(grid), dim3(32 * PR_WARPS), args,
+		0, s));
 	ALPB_LAUNCHED();
 	PrState h;
 	ALPB_CUDA(cudaMemcpyAsync(&h, st, sizeof(PrState), cudaMemcpyDeviceToHost, s));
@@ -219,7 +229,7 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 	ALPB_CUDA(cudaFreeAsync(st, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
 	alpb_spmv_plan_destroy(plan);
-	ALPB_CHECK(h.gs.err == 0, ALPB_PANIC, "alpb_pagerank: grid barrier timed out");
+	ALPB_CHECK(h.gs.err == 0, ALPB_PANIC, "alpb_pagerank: a grid barrier or tile wait timed out");
 	*iterations = h.iterations;
 	*residual = h.residual;
 	if (!(h.residual <= conv)) {

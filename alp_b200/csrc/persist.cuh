@@ -5,12 +5,15 @@
 
 namespace alpb {
 
-// Barrier state in device memory; zero-initialise before the launch.
-struct GridSync {
+// Barrier state in device memory; zero-initialise before the launch.  The
+// arrival counter and the polled words sit on separate 128-byte lines, so
+// that the pollers do not contend with the arrivals' atomics.
+struct alignas(128) GridSync {
 	unsigned int count;
+	unsigned int pad0[31];
 	unsigned int gen;
-	int err;    // 1: a barrier wait gave up (the kernel exits; host reports PANIC)
-	int pad;
+	int err;    // 1: a barrier or tile wait gave up (the kernel exits; host reports PANIC)
+	unsigned int pad1[30];
 };
 
 // ~1 s at the sleep granularity below: far beyond any legitimate wait of a
@@ -80,6 +83,19 @@ int cooperative_grid(K kernel, int block, size_t smem, int64_t want) {
 		return 0;
 	int64_t g = int64_t(per_sm) * sm_count();
 	if (want > 0 && want < g) g = want;
+	return int(g);
+}
+
+// Grid of a persistent solver kernel over `ntiles` warp tiles: about four
+// tiles per warp, at least two blocks per SM (latency hiding), at most the
+// co-resident maximum.  Every grid barrier and every scalar reduction costs
+// time in proportion to the block count, so small systems get small grids.
+template <class K>
+int solver_grid(K kernel, int block, int64_t ntiles, int warps_per_block) {
+	const int max_grid = cooperative_grid(kernel, block, 0, 0);
+	int64_t g = ntiles / (4 * int64_t(warps_per_block));
+	if (g < 2 * int64_t(sm_count())) g = 2 * int64_t(sm_count());
+	if (g > max_grid) g = max_grid;
 	return int(g);
 }
 

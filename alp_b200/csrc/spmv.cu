@@ -106,6 +106,7 @@ MergeTables merge_tables(const alpb_spmv_plan_s &p) {
 	t.tail_val = p.tail_val;
 	t.head_has = p.head_has;
 	t.tail_has = p.tail_has;
+	t.ready = p.ready;
 	return t;
 }
 
@@ -140,7 +141,7 @@ k_spmv_merge(MergeTables mt, const int64_t *__restrict__ offsets,
 #endif
 constexpr int WM_WARPS = ALPB_WM_WARPS;  // warps per block
 #ifndef ALPB_WM_MIN_BLOCKS
-#define ALPB_WM_MIN_BLOCKS 1
+#define ALPB_WM_MIN_BLOCKS 3  // caps registers at 84: three blocks of eight warps per SM
 #endif
 
 // y_r = y_r (+) row sum for the rows that end in a warp tile; their old
@@ -172,8 +173,14 @@ k_spmv_wmerge(MergeTables mt, const int64_t *__restrict__ offsets,
 	WarpAccumulateY<R> epi{y, ybuf[threadIdx.x >> 5]};
 	const int w = threadIdx.x >> 5;
 	const int64_t nw = int64_t(gridDim.x) * WM_WARPS;
-	for (int64_t t = int64_t(blockIdx.x) * WM_WARPS + w; t < mt.ntiles; t += nw)
-		warp_tile<R>(t, mt, offsets, indices, values, xl, epi, left, sm[w]);
+	int64_t t = int64_t(blockIdx.x) * WM_WARPS + w;
+	WmMeta g = wm_meta(mt, t);
+	while (t < mt.ntiles) {
+		const WmMeta next = wm_meta(mt, t + nw);
+		warp_tile<R>(t, g, mt, offsets, indices, values, xl, epi, left, sm[w]);
+		t += nw;
+		g = next;
+	}
 }
 
 // ------------------------------------------------------ vector schedules --
@@ -475,7 +482,9 @@ int plan_build(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t tile, cudaSt
 		ALPB_CUDA(cudaMalloc(&p->tail_val, nt * 8));
 		ALPB_CUDA(cudaMalloc(&p->head_has, nt));
 		ALPB_CUDA(cudaMalloc(&p->tail_has, nt));
+		ALPB_CUDA(cudaMalloc(&p->ready, nt * 4));
 		ALPB_CUDA(cudaMemsetAsync(p->counter, 0, nt * 4, s));
+		ALPB_CUDA(cudaMemsetAsync(p->ready, 0, nt * 4, s));
 		k_merge_tiles<<<grid_for(p->ntiles + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz,
 			p->ntiles, p->tile_row, tile);
 		ALPB_LAUNCHED();
@@ -548,6 +557,7 @@ int alpb_spmv_plan_destroy(alpb_spmv_plan p) {
 	cudaFree(p->tail_val);
 	cudaFree(p->head_has);
 	cudaFree(p->tail_has);
+	cudaFree(p->ready);
 	delete p;
 	return ALPB_SUCCESS;
 }

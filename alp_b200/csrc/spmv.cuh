@@ -22,6 +22,7 @@ struct alpb_spmv_plan_s {
 	uint64_t *tail_val = nullptr;   // ntiles
 	uint8_t *head_has = nullptr;    // ntiles
 	uint8_t *tail_has = nullptr;    // ntiles
+	int32_t *ready = nullptr;       // ntiles (publication epochs, fused solvers)
 	double mean = 0, maxlen = 0, cv = 0;
 	float tuned_ms = 0;
 };

@@ -30,9 +30,15 @@ constexpr int WM_IPT = ALPB_WM_IPT;    // merge items per lane
 constexpr int WM_TILE = 32 * WM_IPT;   // merge items per warp tile
 constexpr unsigned WM_FULL = 0xffffffffu;
 
+// Position of product k in shared memory.  The staging writes k = 32u + L
+// (lane L) and the walk reads k ~ 8L + c; XOR-ing the low four bits with bits
+// 3..6 makes both patterns hit sixteen distinct 8-byte bank pairs per
+// half-warp (a bijection of k within each aligned block of 128 entries).
+__device__ __forceinline__ int wm_pad(int k) { return k ^ ((k >> 3) & 15); }
+
 template <class R>
 struct WarpSmem {
-	typename R::T prod[WM_TILE];
+	typename R::T prod[WM_TILE < 128 ? 128 : WM_TILE];
 	int32_t row_end[WM_TILE + 2];  // [k] = end of tile row k-1, relative to j0, clamped
 };
 
@@ -120,7 +126,7 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 			const int k = lane + 32 * u;
 			if (k < nnzt) {
 				const T xv = xl(col[u]);
-				sm.prod[k] = left ? R::mull(xv, a[u]) : R::mulr(a[u], xv);
+				sm.prod[wm_pad(k)] = left ? R::mull(xv, a[u]) : R::mulr(a[u], xv);
 			}
 		}
 	}
@@ -148,9 +154,10 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 	first_row = -1;
 	T first_val = R::zero();
 	bool first_has = false;
+	int re = sm.row_end[ti + 1];  // end of the row being walked
 	for (int d = dl; d < dend; ++d) {
-		if (tj < sm.row_end[ti + 1]) {
-			acc = R::add(acc, sm.prod[tj]);
+		if (tj < re) {
+			acc = R::add(acc, sm.prod[wm_pad(tj)]);
 			has = true;
 			++tj;
 		} else {
@@ -164,6 +171,7 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 			acc = R::zero();
 			has = false;
 			++ti;
+			re = sm.row_end[ti + 1];
 		}
 	}
 
@@ -199,27 +207,110 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 	__syncwarp();  // the warp's shared memory is reused by its next tile
 }
 
+// Table entries of one warp tile (loaded one tile ahead by the persistent
+// loops, so that their latency hides behind the previous tile's work).
+struct WmMeta {
+	int64_t i0, i1, hf, tf;
+};
+__device__ __forceinline__ WmMeta wm_meta(const MergeTables &mt, int64_t t) {
+	WmMeta g{0, 0, -1, -1};
+	if (t < mt.ntiles) {
+		g.i0 = mt.tile_row[t];
+		g.i1 = mt.tile_row[t + 1];
+		g.hf = mt.head_first[t];
+		g.tf = mt.tail_first[t];
+	}
+	return g;
+}
+
 // One warp tile t for the two-pass SpMV: rows that end in the tile are
 // finished here (epi.row); a row crossing tiles leaves this tile's partial in
 // head_val[t] (the row ends here) or tail_val[t] (it continues), and
 // k_wm_fixup finishes it.  A spanning row always holds nonzeroes, so its
 // partials need no presence flag: an empty partial is the additive identity.
 template <class R, class XL, class Epi>
-__device__ __forceinline__ void warp_tile(int64_t t, const MergeTables &mt,
+__device__ __forceinline__ void warp_tile(int64_t t, const WmMeta &g, const MergeTables &mt,
 	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
 	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
 	WarpSmem<R> &sm) {
 	using T = typename R::T;
 	const int lane = threadIdx.x & 31;
-	const int64_t i0 = mt.tile_row[t], i1 = mt.tile_row[t + 1];
-	const int64_t hf = mt.head_first[t], tf = mt.tail_first[t];
 	int first_row;
 	T head_v, sv;
 	bool head_h, sh;
-	wm_core<R>(t, mt, offsets, indices, values, xl, epi, left, sm, i0, i1, hf, first_row, head_v,
-		head_h, sv, sh);
-	if (hf >= 0 && first_row == 0) store_bits<T>(mt.head_val + t, head_v);
-	if (tf >= 0 && lane == 31) store_bits<T>(mt.tail_val + t, sv);
+	wm_core<R>(t, mt, offsets, indices, values, xl, epi, left, sm, g.i0, g.i1, g.hf, first_row,
+		head_v, head_h, sv, sh);
+	if (g.hf >= 0 && first_row == 0) store_bits<T>(mt.head_val + t, head_v);
+	if (g.tf >= 0 && lane == 31) store_bits<T>(mt.tail_val + t, sv);
+}
+
+__device__ __forceinline__ int wm_ld_acquire(const int32_t *p) {
+	int32_t v;
+	asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ void wm_st_release(int32_t *p, int32_t v) {
+	asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Spin bound of a tile waiting for an earlier tile's tail partial (~0.5 s at
+// the sleep granularity below; far beyond any wait between co-resident warps).
+constexpr long long kWmSpinLimit = 1ll << 23;
+
+// One warp tile t of a fused solver, with every row finished by a FIXED tile:
+// a row crossing tiles is finished by the tile where it ends, which waits for
+// the tail partials that the row's earlier tiles publish in mt.ready under
+// `epoch` (larger than any value the array held before; it starts at zero).
+// Epilogue terms therefore accumulate in a fixed order wherever the tiles
+// run.  Requires every warp of the grid to be resident (a cooperative launch)
+// and each warp to take its tiles in increasing order: a tile publishes its
+// tail before it waits, and waits only on smaller tiles, so no wait can close
+// a cycle.  Epi: begin_tile and row(r, sum, has), from any lane.  Returns
+// false if a wait gave up or *err was set elsewhere (a timeout sets *err = 1;
+// the caller leaves at its next grid barrier, which checks the same flag).
+template <class R, class XL, class Epi>
+__device__ __forceinline__ bool warp_tile_ordered(int64_t t, const WmMeta &g,
+	const MergeTables &mt, const int64_t *__restrict__ offsets,
+	const uint32_t *__restrict__ indices, const typename R::T *__restrict__ values,
+	const XL &xl, Epi &epi, int left, WarpSmem<R> &sm, int32_t epoch, int *err) {
+	using T = typename R::T;
+	const int lane = threadIdx.x & 31;
+	int first_row;
+	T head_v, sv;
+	bool head_h, sh;
+	wm_core<R>(t, mt, offsets, indices, values, xl, epi, left, sm, g.i0, g.i1, g.hf, first_row,
+		head_v, head_h, sv, sh);
+	if (g.tf >= 0 && lane == 31) {
+		store_bits<T>(mt.tail_val + t, sv);
+		wm_st_release(mt.ready + t, epoch);  // orders the store above before the flag
+	}
+	if (g.hf < 0) return true;
+	T v = R::zero();
+	bool ok = true;
+	for (int64_t k = g.hf + lane; k < t && ok; k += 32) {
+		long long spins = 0;
+		while (wm_ld_acquire(mt.ready + k) < epoch) {
+			if (++spins > kWmSpinLimit) {
+				atomicExch(err, 1);
+				ok = false;
+				break;
+			}
+			if (*reinterpret_cast<volatile int *>(err)) {  // another wait gave up
+				ok = false;
+				break;
+			}
+			__nanosleep(64);
+		}
+		if (ok) v = R::add(v, wm_load_slot<T>(mt.tail_val + k));
+	}
+	if (!__all_sync(WM_FULL, ok)) return false;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		const T vo = wm_shfl_xor(v, o);
+		v = R::add(v, vo);
+	}
+	if (first_row == 0) epi.row(g.i0, R::add(v, head_v), true);
+	return true;
 }
 
 // Second pass: every row that crosses tiles, y_r = y_r (+) its slots summed
