@@ -214,7 +214,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
     e2e_value = world * nbytes / (e2e_ms * 1e-3) / 1e9
 
     peaks = measured_peaks()
-    kernel_tag = (f"spmv_merge_rmat{args.scale}" if sched == abi.SCHED_MERGE_PATH
+    kernel_tag = (f"spmv_wmerge_rmat{args.scale}" if sched == abi.SCHED_MERGE_PATH
                   else f"spmv_vector_rmat{args.scale}")
     traffic = profiled_traffic(kernel_tag)
     achieved = nbytes / (ms * 1e-3) / 1e9
@@ -237,7 +237,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
                      "frac": round(achieved / peaks["hbm_gbs"], 4),
                      "peak_source": peaks["source"],
                      "traffic": traffic,
-                     "kernel": "k_spmv_merge<RingPlusTimesF64>" if sched == 1
+                     "kernel": "k_spmv_wmerge<RingPlusTimesF64> + k_wm_fixup" if sched == 1
                      else f"k_spmv_vector_dense<RingPlusTimesF64,{vw}>"},
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": A.n * 8,
                 "d2h_bytes_per_step": A.m * 8, "ms_per_step": round(e2e_ms, 5)},
@@ -302,43 +302,172 @@ def extra_workloads(args, A, plan) -> dict:
     LT = dev.transpose(L)
     pr = torch.zeros(A.m, dtype=torch.float64, device="cuda")
     it, res = C.c_int64(), C.c_double()
-    torch.cuda.synchronize()
-    t0 = time.time()
-    rc = abi.lib().alpb_pagerank(L.m, dev.ptr(L.offsets), dev.ptr(L.indices), dev.ptr(L.values),
-                                 dev.ptr(LT.offsets), dev.ptr(LT.indices), dev.ptr(LT.values),
-                                 dev.ptr(pr), 0, 0.85, 1e-9, 1000, C.byref(it), C.byref(res),
-                                 dev.stream_ptr())
-    torch.cuda.synchronize()
-    t = time.time() - t0
+    prc = [0]
+
+    def pagerank():
+        prc[0] = abi.lib().alpb_pagerank(L.m, dev.ptr(L.offsets), dev.ptr(L.indices),
+                                         dev.ptr(L.values), dev.ptr(LT.offsets), dev.ptr(LT.indices),
+                                         dev.ptr(LT.values), dev.ptr(pr), 0, 0.85, 1e-9, 1000,
+                                         C.byref(it), C.byref(res), dev.stream_ptr())
+    ms = timed(pagerank, 2, stream)   # one call: plan, setup and every iteration
     per_iter = (A.nnz * 12 + (A.n + 1) * 8 + 6 * A.n * 8)
-    out["pagerank_rmat22"] = {"rc": rc, "iterations": it.value, "residual": res.value,
-                              "ms_total": round(t * 1e3, 2),
-                              "ms_per_iter": round(t * 1e3 / max(it.value, 1), 4),
-                              "GB/s": round(per_iter * it.value / t / 1e9, 1)}
+    out["pagerank_rmat22"] = {"rc": prc[0], "iterations": it.value, "residual": res.value,
+                              "ms_per_call": round(ms, 3),
+                              "ms_per_iter": round(ms / max(it.value, 1), 4),
+                              "GB/s": round(per_iter * it.value / ms / 1e6, 1)}
     del L, LT, pr
-    # plain CG, 27-point 32^3
+    # plain CG, 27-point 32^3 (the reference's CPU-runnable configuration)
     S = dev.stencil((32, 32, 32), 26.0, -1.0)
     ones = torch.ones(S.n, dtype=torch.float64, device="cuda")
     b = torch.zeros_like(ones)
     dev.mxv(abi.RING_PLUS_TIMES_F64, S, b, ones)
     ps = dev.Plan(S, sched=abi.SCHED_MERGE_PATH)
     x = torch.zeros_like(b)
+    work = torch.empty(4 * S.n, dtype=torch.float64, device="cuda")
 
     def cg():
         x.zero_()
-        abi.lib().alpb_cg_solve(S.m, dev.ptr(S.offsets), dev.ptr(S.indices), dev.ptr(S.values),
-                                dev.ptr(b), dev.ptr(x), 500, 1e-10, C.byref(it), C.byref(res),
-                                None, ps.h, dev.stream_ptr())
-    cg()
-    t0 = time.time()
-    for _ in range(5):
-        cg()
-    torch.cuda.synchronize()
-    t = (time.time() - t0) / 5
+        abi.call("alpb_cg_solve", S.m, dev.ptr(S.offsets), dev.ptr(S.indices), dev.ptr(S.values),
+                 dev.ptr(b), dev.ptr(x), 500, 1e-10, C.byref(it), C.byref(res), dev.ptr(work),
+                 ps.h, dev.stream_ptr())
+    ms = timed(cg, 5, stream)
     out["cg_27pt_32"] = {"iterations": it.value, "residual": res.value,
-                         "ms_per_solve": round(t * 1e3, 3),
+                         "ms_per_solve": round(ms, 4),
+                         "us_per_iteration": round(1e3 * ms / max(it.value, 1), 2),
                          "err_vs_ones_inf": float((x - 1).abs().max().item())}
+    del S, ps, work
+    out["batched_cg"] = batched_cg_workload(stream)
+    out["adjoint_cg"] = adjoint_workload(stream)
     return out
+
+
+def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024) -> dict:
+    """256 shifted 2-D 5-point Poisson systems, sides log-uniform in [32, 512],
+    shift U(0.01, 1), b ~ N(0, 1), relative tolerance 1e-8, FP64: one
+    graph-captured persistent launch against one alpb_cg_solve launch per
+    instance (plans and buffers prepared outside the timed regions)."""
+    import ctypes as C
+    import torch
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+    rng = np.random.default_rng(seed)
+    sides = np.round(np.exp(rng.uniform(np.log(32), np.log(512), nseg))).astype(np.int64)
+    shifts = rng.uniform(0.01, 1.0, nseg)
+    rows = sides * sides
+    nnzs = 5 * sides * sides - 4 * sides
+    seg_rows = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
+    seg_nnz = np.concatenate([[0], np.cumsum(nnzs)]).astype(np.int64)
+    n, nnz = int(seg_rows[-1]), int(seg_nnz[-1])
+    d = torch.device("cuda")
+    tL = torch.from_numpy(sides).to(d)
+    tS = torch.from_numpy(shifts).to(d)
+    tR = torch.from_numpy(seg_rows).to(d)
+    tN = torch.from_numpy(seg_nnz).to(d)
+    rp = torch.empty(n + 1, dtype=torch.int64, device=d)
+    ci = torch.empty(nnz, dtype=torch.int32, device=d)
+    va = torch.empty(nnz, dtype=torch.float64, device=d)
+    sp = dev.stream_ptr(stream)
+    abi.call("alpb_gen_poisson2d_batch", nseg, dev.ptr(tL), dev.ptr(tS), dev.ptr(tR), dev.ptr(tN),
+             n, dev.ptr(rp), dev.ptr(ci), dev.ptr(va), sp)
+    b = torch.empty(n, dtype=torch.float64, device=d)
+    abi.call("alpb_gen_normal", dev.ptr(b), n, seed, 1, sp)
+    x = torch.zeros_like(b)
+    tol, max_iter = 1e-8, 20000
+    h = C.c_void_p()
+    abi.call("alpb_batched_cg_create", C.byref(h), n, nnz, dev.ptr(rp), dev.ptr(ci), dev.ptr(va),
+             nseg, dev.ptr(tR), sp)
+    abi.call("alpb_batched_cg_capture", h, dev.ptr(b), dev.ptr(x), max_iter, tol, sp)
+
+    def batched():
+        x.zero_()
+        abi.call("alpb_batched_cg_replay", h, sp)
+    ms_b = timed(batched, 3, stream)
+    it = np.zeros(nseg, np.int64)
+    rr = np.zeros(nseg)
+    conv = np.zeros(nseg, np.int32)
+    rc = abi.lib().alpb_batched_cg_results(h, it.ctypes.data_as(C.c_void_p),
+                                           rr.ctypes.data_as(C.c_void_p),
+                                           conv.ctypes.data_as(C.c_void_p), sp)
+    xb = x.clone()
+    abi.lib().alpb_batched_cg_destroy(h)
+    # plain path: one alpb_cg_solve launch per instance, on its own CRS
+    systems = []
+    for L, sh in zip(sides, shifts):
+        A = dev.poisson2d(int(L), float(sh))
+        systems.append((A, dev.Plan(A, sched=abi.SCHED_MERGE_PATH),
+                        torch.empty(4 * A.n, dtype=torch.float64, device=d)))
+    xp = torch.zeros_like(b)
+    itp = np.zeros(nseg, np.int64)
+    i1, r1 = C.c_int64(), C.c_double()
+
+    def plain():
+        xp.zero_()
+        for k, (A, pl, wk) in enumerate(systems):
+            o = int(seg_rows[k])
+            rcs = abi.lib().alpb_cg_solve(A.m, dev.ptr(A.offsets), dev.ptr(A.indices),
+                                          dev.ptr(A.values), C.c_void_p(b.data_ptr() + 8 * o),
+                                          C.c_void_p(xp.data_ptr() + 8 * o), max_iter, tol,
+                                          C.byref(i1), C.byref(r1), dev.ptr(wk), pl.h, sp)
+            assert rcs == abi.SUCCESS, abi.last_error()
+            itp[k] = i1.value
+    ms_p = timed(plain, 1, stream)
+    diff = float(((xb - xp).abs().max() / xp.abs().max()).item())
+    return {"systems": nseg, "rows": n, "nnz": nnz, "tol": tol, "rc": rc,
+            "all_converged": bool(conv.all()), "iterations_max": int(it.max()),
+            "iterations_sum": int(it.sum()), "plain_iterations_sum": int(itp.sum()),
+            "batched_ms": round(ms_b, 3), "plain_ms": round(ms_p, 3),
+            "batched_solves_per_s": round(nseg / (ms_b * 1e-3), 1),
+            "plain_solves_per_s": round(nseg / (ms_p * 1e-3), 1),
+            "speedup": round(ms_p / ms_b, 2),
+            "max_rel_diff_batched_vs_plain": diff}
+
+
+def adjoint_workload(stream, side: int = 64) -> dict:
+    """Differentiated CG on the 27-point 64^3 pattern: off-diagonals -U(0.5, 1.5)
+    (symmetric), diagonal 1.05 |row sum|, b, x* ~ N(0, 1), L = 0.5 |x - x*|^2.
+    Forward solve (alpb_cg_solve) against the gradient (alpb_cg_adjoint: CG on
+    the CCS for lambda, then the SDDMM -lambda_i x_j), relative tolerance 1e-12."""
+    import ctypes as C
+    import torch
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+    sp = dev.stream_ptr(stream)
+    A = dev.stencil((side, side, side), 1.0, 1.0, ref_order=False)
+    abi.call("alpb_gen_sym_dd_values", dev.ptr(A.offsets), dev.ptr(A.indices), A.m, 11, 0.5, 1.5,
+             1.05, dev.ptr(A.values), sp)
+    At = dev.transpose(A)
+    pa, pt = dev.Plan(A, sched=abi.SCHED_MERGE_PATH), dev.Plan(At, sched=abi.SCHED_MERGE_PATH)
+    b = torch.empty(A.m, dtype=torch.float64, device="cuda")
+    xs = torch.empty_like(b)
+    abi.call("alpb_gen_normal", dev.ptr(b), A.m, 5, 1, sp)
+    abi.call("alpb_gen_normal", dev.ptr(xs), A.m, 6, 1, sp)
+    x = torch.zeros_like(b)
+    lam = torch.zeros_like(b)
+    g = torch.empty_like(b)
+    gv = torch.empty_like(A.values)
+    work = torch.empty(4 * A.m, dtype=torch.float64, device="cuda")
+    tol = 1e-12
+    itf, ita, res = C.c_int64(), C.c_int64(), C.c_double()
+
+    def forward():
+        x.zero_()
+        abi.call("alpb_cg_solve", A.m, dev.ptr(A.offsets), dev.ptr(A.indices), dev.ptr(A.values),
+                 dev.ptr(b), dev.ptr(x), 5000, tol, C.byref(itf), C.byref(res), dev.ptr(work),
+                 pa.h, sp)
+    ms_f = timed(forward, 3, stream)
+    torch.sub(x, xs, out=g)
+
+    def gradient():
+        lam.zero_()
+        abi.call("alpb_cg_adjoint", A.m, dev.ptr(A.offsets), dev.ptr(A.indices), dev.ptr(A.values),
+                 dev.ptr(At.offsets), dev.ptr(At.indices), dev.ptr(At.values), dev.ptr(x),
+                 dev.ptr(g), dev.ptr(lam), dev.ptr(gv), 5000, tol, C.byref(ita), C.byref(res),
+                 pa.h, pt.h, sp)
+    ms_g = timed(gradient, 3, stream)
+    return {"rows": A.m, "nnz": A.nnz, "tol": tol, "forward_iterations": itf.value,
+            "adjoint_iterations": ita.value, "forward_ms": round(ms_f, 3),
+            "gradient_ms": round(ms_g, 3), "gradient_over_forward": round(ms_g / ms_f, 3),
+            "forward_solves_per_s": round(1e3 / ms_f, 2), "grads_per_s": round(1e3 / ms_g, 2)}
 
 
 # ------------------------------------------------------------ reference arm --
