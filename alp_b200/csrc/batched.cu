@@ -15,6 +15,7 @@
 // masked out; the launch ends when no instance is active.
 #include "common.cuh"
 #include "merge.cuh"
+#include "wmerge.cuh"
 #include "persist.cuh"
 #include "spmv.cuh"
 
@@ -29,24 +30,24 @@ using RF = RingPlusTimesF64;
 
 // ------------------------------------------------------ segmented tables --
 __global__ void k_seg_tile_counts(const int64_t *offsets, const int64_t *seg_rows, int64_t nseg,
-	int64_t *counts) {
+	int64_t *counts, int64_t tile) {
 	for (int64_t s = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s <= nseg;
 		 s += int64_t(gridDim.x) * blockDim.x) {
 		if (s == nseg) { counts[s] = 0; continue; }
 		const int64_t r0 = seg_rows[s], r1 = seg_rows[s + 1];
 		const int64_t items = (r1 - r0) + (offsets[r1] - offsets[r0]);
-		counts[s] = (items + MP_TILE - 1) / MP_TILE;
+		counts[s] = (items + tile - 1) / tile;
 	}
 }
 
 __global__ void k_seg_tile_d(const int64_t *offsets, const int64_t *seg_rows, const int64_t *seg_tile,
-	int64_t nseg, int64_t m, int64_t nnz, int64_t *tile_d, int32_t *tile_seg) {
+	int64_t nseg, int64_t m, int64_t nnz, int64_t *tile_d, int32_t *tile_seg, int64_t tile) {
 	for (int64_t s = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < nseg;
 		 s += int64_t(gridDim.x) * blockDim.x) {
 		const int64_t r0 = seg_rows[s];
 		const int64_t base = r0 + offsets[r0];
 		for (int64_t t = seg_tile[s]; t < seg_tile[s + 1]; ++t) {
-			tile_d[t] = base + (t - seg_tile[s]) * MP_TILE;
+			tile_d[t] = base + (t - seg_tile[s]) * tile;
 			tile_seg[t] = int32_t(s);
 		}
 	}
@@ -109,7 +110,8 @@ int merge_plan_segmented(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t ns
 	void *tmp = nullptr;
 	size_t tb = 0;
 	ALPB_CUDA(cudaMallocAsync(&counts, size_t(nseg + 1) * 8, s));
-	k_seg_tile_counts<<<grid_for(nseg + 1, 256), 256, 0, s>>>(offsets, seg_rows, nseg, counts);
+	k_seg_tile_counts<<<grid_for(nseg + 1, 256), 256, 0, s>>>(offsets, seg_rows, nseg, counts,
+		WM_TILE);
 	ALPB_LAUNCHED();
 	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, counts, st->seg_tile, nseg + 1, s));
 	ALPB_CUDA(cudaMallocAsync(&tmp, tb, s));
@@ -122,7 +124,7 @@ int merge_plan_segmented(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t ns
 	ALPB_CUDA(cudaStreamSynchronize(s));
 	ALPB_CHECK(nt > 0, ALPB_ILLEGAL, "segmented plan: no work");
 	p->ntiles = nt;
-	p->tile = MP_TILE;
+	p->tile = WM_TILE;
 	const size_t n = size_t(nt);
 	ALPB_CUDA(cudaMalloc(&st->tile_d, (n + 1) * 8));
 	ALPB_CUDA(cudaMalloc(&st->tile_seg, n * 4));
@@ -135,9 +137,11 @@ int merge_plan_segmented(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t ns
 	ALPB_CUDA(cudaMalloc(&p->tail_val, n * 8));
 	ALPB_CUDA(cudaMalloc(&p->head_has, n));
 	ALPB_CUDA(cudaMalloc(&p->tail_has, n));
+	ALPB_CUDA(cudaMalloc(&p->ready, n * 4));
 	ALPB_CUDA(cudaMemsetAsync(p->counter, 0, n * 4, s));
+	ALPB_CUDA(cudaMemsetAsync(p->ready, 0, n * 4, s));
 	k_seg_tile_d<<<grid_for(nseg, 256), 256, 0, s>>>(offsets, seg_rows, st->seg_tile, nseg, p->m,
-		p->nnz, st->tile_d, st->tile_seg);
+		p->nnz, st->tile_d, st->tile_seg, WM_TILE);
 	ALPB_LAUNCHED();
 	k_seg_tile_rows<<<grid_for(nt + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz, nt, st->tile_d,
 		p->tile_row);
@@ -167,13 +171,13 @@ struct BcgInst {       // per-instance device state
 };
 
 struct BcgArgs {
-	MergeTables mt;
+	MergeTables mt;                    // warp tiles cut per instance (tile_d)
 	const int64_t *offsets;
 	const uint32_t *indices;
 	const double *values;
 	const double *b;
 	double *x, *r, *u0, *u1, *temp;
-	double *own, *span, *own2, *span2;  // [ntiles]
+	double *own, *own2;                // [ntiles] per-tile partials
 	const int32_t *tile_seg;           // [ntiles]
 	const int64_t *seg_tile;           // [nseg+1]
 	BcgInst *inst;                     // [nseg]
@@ -183,29 +187,31 @@ struct BcgArgs {
 	GridSync *gs;
 };
 
+constexpr int BCG_WARPS = 4;
+
+struct BcgWarpSmem {
+	WarpSmem<RF> tile;
+	double p0[WM_TILE];
+	double p1[WM_TILE];
+};
+
 struct BcgPrelude {
 	const BcgArgs *a;
+	BcgWarpSmem *sm;
+	int64_t base = 0;
 	double acc_rr = 0.0, acc_bb = 0.0;
-	__device__ __forceinline__ void terms(int64_t i, double v, bool has, double &rr, double &bb) {
+	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
+		base = i0;
+		for (int k = lane; k < nrows; k += 32) sm->p0[k] = a->b[i0 + k];
+	}
+	__device__ __forceinline__ void row(int64_t i, double v, bool has) {
 		const double t = has ? 0.0 + v : 0.0;
-		const double bi = a->b[i];
+		const double bi = sm->p0[i - base];
 		const double ri = (0.0 + bi) - t;
 		a->r[i] = ri;
 		a->u0[i] = 0.0;
-		rr = ri * ri;
-		bb = bi * bi;
-	}
-	__device__ __forceinline__ void row(int64_t i, double v, bool has) {
-		double rr, bb;
-		terms(i, v, has, rr, bb);
-		acc_rr += rr;
-		acc_bb += bb;
-	}
-	__device__ __forceinline__ void row_span(int64_t first, int64_t i, double v, bool has) {
-		double rr, bb;
-		terms(i, v, has, rr, bb);
-		a->span[first] = rr;
-		a->span2[first] = bb;
+		acc_rr += ri * ri;
+		acc_bb += bi * bi;
 	}
 };
 
@@ -219,81 +225,103 @@ struct BcgGather {
 
 struct BcgIter {
 	const BcgArgs *a;
+	BcgWarpSmem *sm;
 	const double *u_old;
 	double *u_new;
 	double gamma;
+	int64_t base = 0;
 	double acc = 0.0;
-	__device__ __forceinline__ double term(int64_t i, double v, bool has) {
+	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
+		base = i0;
+		for (int k = lane; k < nrows; k += 32) {
+			sm->p0[k] = __ldcg(a->r + i0 + k);
+			sm->p1[k] = __ldcg(u_old + i0 + k);
+		}
+	}
+	__device__ __forceinline__ void row(int64_t i, double v, bool has) {
 		const double t = has ? 0.0 + v : 0.0;
 		a->temp[i] = t;
-		const double un = __ldcg(a->r + i) + gamma * __ldcg(u_old + i);
+		const double un = sm->p0[i - base] + gamma * sm->p1[i - base];
 		u_new[i] = un;
-		return t * un;
-	}
-	__device__ __forceinline__ void row(int64_t i, double v, bool has) { acc += term(i, v, has); }
-	__device__ __forceinline__ void row_span(int64_t first, int64_t i, double v, bool has) {
-		a->span[first] = term(i, v, has);
+		acc += t * un;
 	}
 };
 
-// The last of instance s's tiles to arrive gets true; the caller then sums
-// the instance's tile partials.  Called by thread 0 after the tile's
-// partials are stored.
-__device__ __forceinline__ bool inst_arrive(BcgInst *in, int64_t ntiles_inst) {
-	__threadfence();
-	const int32_t prev = atomicAdd(&in->cnt, 1);
-	if (prev != ntiles_inst - 1) return false;
-	__threadfence();
-	in->cnt = 0;
-	return true;
-}
-
-__device__ __forceinline__ double sum_tiles(const double *own, const double *span, int64_t t0,
-	int64_t t1) {
-	double v = 0.0;
-	for (int64_t t = t0; t < t1; ++t)
-		v += ((const volatile double *) own)[t] + (span ? ((const volatile double *) span)[t] : 0.0);
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		const double w = __shfl_xor_sync(0xffffffffu, v, o);
+		v += w;
+	}
 	return v;
 }
 
-__global__ void __launch_bounds__(MP_BLOCK) k_batched_cg(BcgArgs a) {
-	__shared__ MergeSmem<RF> sm;
-	__shared__ double red[33];
-	const int64_t G = gridDim.x, nt = a.mt.ntiles;
-	for (int64_t t = blockIdx.x; t < nt; t += G) {
-		a.span[t] = 0.0;
-		a.span2[t] = 0.0;
+// Sum of the per-tile partials own[t0..t1) in a fixed order (lane-strided,
+// then the xor tree), the same in every lane.
+__device__ __forceinline__ double warp_sum_tiles(const double *own, int64_t t0, int64_t t1,
+	int lane) {
+	double v = 0.0;
+	for (int64_t k = t0 + lane; k < t1; k += 32) v += __ldcg(own + k);
+	return warp_sum(v);
+}
+
+// Arrival of one tile of an instance (its partial already stored by lane 0).
+// Every lane learns whether it was the instance's last tile.
+__device__ __forceinline__ bool inst_arrive(BcgInst *in, int64_t ntiles_inst, int lane) {
+	int last = 0;
+	if (lane == 0) {
+		__threadfence();
+		last = atomicAdd(&in->cnt, 1) == ntiles_inst - 1;
 	}
+	last = __shfl_sync(0xffffffffu, last, 0);
+	if (!last) return false;
+	__threadfence();
+	if (lane == 0) in->cnt = 0;  // next use is after a grid barrier
+	return true;
+}
+
+__global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
+	__shared__ BcgWarpSmem sm[BCG_WARPS];
+	const int64_t G = gridDim.x, nt = a.mt.ntiles;
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int64_t gw = int64_t(blockIdx.x) * BCG_WARPS + w, nw = G * BCG_WARPS;
+	int *err = &a.gs->err;
+	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nt;
+		 t += G * blockDim.x)
+		a.mt.ready[t] = 0;
 	if (!grid_sync(a.gs)) return;
+	int32_t epoch = 1;
 
 	// prelude per instance: r = b - A x, sigma = r.r, tol * ||b||
 	{
-		BcgPrelude epi{&a};
 		PlainX<double> xl{a.x};
-		for (int64_t t = blockIdx.x; t < nt; t += G) {
-			epi.acc_rr = epi.acc_bb = 0.0;
-			merge_tile<RF>(t, a.mt, a.offsets, a.indices, a.values, xl, epi, 0, sm);
-			const double s1 = block_sum(epi.acc_rr, red);
-			const double s2 = block_sum(epi.acc_bb, red);
-			if (threadIdx.x == 0) {
+		for (int64_t t = gw; t < nt; t += nw) {
+			BcgPrelude epi{&a, &sm[w]};
+			const WmMeta g = wm_meta(a.mt, t);
+			if (!warp_tile_ordered<RF>(t, g, a.mt, a.offsets, a.indices, a.values, xl, epi, 0,
+					sm[w].tile, epoch, err))
+				break;
+			const double s1 = warp_sum(epi.acc_rr), s2 = warp_sum(epi.acc_bb);
+			if (lane == 0) {
 				a.own[t] = s1;
 				a.own2[t] = s2;
 			}
 		}
 	}
-	if (!grid_sync(a.gs)) return;  // spanning terms of every instance are in place
-	for (int64_t s = blockIdx.x; s < a.nseg; s += G) {
-		if (threadIdx.x != 0) continue;
+	if (!grid_sync(a.gs)) return;
+	for (int64_t s = gw; s < a.nseg; s += nw) {
 		BcgInst *in = a.inst + s;
-		const double sigma = sum_tiles(a.own, a.span, a.seg_tile[s], a.seg_tile[s + 1]);
-		const double bnorm = sum_tiles(a.own2, a.span2, a.seg_tile[s], a.seg_tile[s + 1]);
-		in->sigma = sigma;
-		in->gamma = 0.0;
-		in->tol_abs = a.tol * sqrt(bnorm);
-		in->iterations = 0;
-		in->done = 0;
-		in->converged = 0;
-		in->cnt = 0;
+		const double sigma = warp_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], lane);
+		const double bnorm = warp_sum_tiles(a.own2, a.seg_tile[s], a.seg_tile[s + 1], lane);
+		if (lane == 0) {
+			in->sigma = sigma;
+			in->gamma = 0.0;
+			in->tol_abs = a.tol * sqrt(bnorm);
+			in->iterations = 0;
+			in->done = 0;
+			in->converged = 0;
+			in->cnt = 0;
+		}
 	}
 	if (!grid_sync(a.gs)) return;
 
@@ -301,46 +329,47 @@ __global__ void __launch_bounds__(MP_BLOCK) k_batched_cg(BcgArgs a) {
 	double *u_old = a.u0, *u_new = a.u1;
 	for (;;) {
 		++iter;
-		// phase A over the tiles of active instances
-		for (int64_t t = blockIdx.x; t < nt; t += G) {
+		++epoch;
+		// phase A over the tiles of active instances: temp = A u_new, beta
+		for (int64_t t = gw; t < nt; t += nw) {
 			const int32_t s = a.tile_seg[t];
 			BcgInst *in = a.inst + s;
 			if (((volatile int32_t *) &in->done)[0]) continue;
 			const double gamma = ((volatile double *) &in->gamma)[0];
-			BcgIter epi{&a, u_old, u_new, gamma};
+			BcgIter epi{&a, &sm[w], u_old, u_new, gamma};
 			BcgGather xl{a.r, u_old, gamma};
-			merge_tile<RF>(t, a.mt, a.offsets, a.indices, a.values, xl, epi, 0, sm);
-			const double sum = block_sum(epi.acc, red);
-			if (threadIdx.x == 0) {
-				a.own[t] = sum;
-				const int64_t t0 = a.seg_tile[s], t1 = a.seg_tile[s + 1];
-				if (inst_arrive(in, t1 - t0)) {
-					const double beta = sum_tiles(a.own, a.span, t0, t1);
-					in->alpha = in->sigma / beta;
-				}
+			const WmMeta g = wm_meta(a.mt, t);
+			if (!warp_tile_ordered<RF>(t, g, a.mt, a.offsets, a.indices, a.values, xl, epi, 0,
+					sm[w].tile, epoch, err))
+				break;
+			const double part = warp_sum(epi.acc);
+			if (lane == 0) a.own[t] = part;
+			const int64_t t0 = a.seg_tile[s], t1 = a.seg_tile[s + 1];
+			if (inst_arrive(in, t1 - t0, lane)) {
+				const double beta = warp_sum_tiles(a.own, t0, t1, lane);
+				if (lane == 0) in->alpha = in->sigma / beta;
 			}
 		}
 		if (!grid_sync(a.gs)) return;
-		// phase B: the rows owned by each active tile
-		for (int64_t t = blockIdx.x; t < nt; t += G) {
+		// phase B: the rows that end in each active tile
+		for (int64_t t = gw; t < nt; t += nw) {
 			const int32_t s = a.tile_seg[t];
 			BcgInst *in = a.inst + s;
 			if (((volatile int32_t *) &in->done)[0]) continue;
 			const double alpha = ((volatile double *) &in->alpha)[0];
 			double part = 0.0;
-			for (int64_t i = a.mt.tile_row[t] + threadIdx.x; i < a.mt.tile_row[t + 1];
-				 i += blockDim.x) {
+			for (int64_t i = a.mt.tile_row[t] + lane; i < a.mt.tile_row[t + 1]; i += 32) {
 				a.x[i] = a.x[i] + alpha * __ldcg(u_new + i);
 				const double ri = __ldcg(a.r + i) - alpha * __ldcg(a.temp + i);
 				a.r[i] = ri;
 				part += ri * ri;
 			}
-			part = block_sum(part, red);
-			if (threadIdx.x == 0) {
-				a.own[t] = part;
-				const int64_t t0 = a.seg_tile[s], t1 = a.seg_tile[s + 1];
-				if (inst_arrive(in, t1 - t0)) {
-					const double rr = sum_tiles(a.own, nullptr, t0, t1);
+			part = warp_sum(part);
+			if (lane == 0) a.own[t] = part;
+			const int64_t t0 = a.seg_tile[s], t1 = a.seg_tile[s + 1];
+			if (inst_arrive(in, t1 - t0, lane)) {
+				const double rr = warp_sum_tiles(a.own, t0, t1, lane);
+				if (lane == 0) {
 					in->rr = rr;
 					in->iterations = iter;
 					if (sqrt(rr) < in->tol_abs || iter >= a.max_iter) {
@@ -375,7 +404,7 @@ struct alpb_batched_cg_s {
 	const uint32_t *indices = nullptr;
 	const double *values = nullptr;
 	double *work = nullptr;     // r, u0, u1, temp
-	double *scratch = nullptr;  // own, span, own2, span2
+	double *scratch = nullptr;  // own, own2
 	BcgInst *inst = nullptr;
 	int32_t *active = nullptr;
 	GridSync *gs = nullptr;
@@ -413,9 +442,7 @@ static int bcg_launch(alpb_batched_cg_s *h, const double *b, double *x, int64_t 
 	a.u1 = h->work + 2 * h->n;
 	a.temp = h->work + 3 * h->n;
 	a.own = h->scratch;
-	a.span = h->scratch + nt;
-	a.own2 = h->scratch + 2 * nt;
-	a.span2 = h->scratch + 3 * nt;
+	a.own2 = h->scratch + nt;
 	a.tile_seg = h->st.tile_seg;
 	a.seg_tile = h->st.seg_tile;
 	a.inst = h->inst;
@@ -426,7 +453,7 @@ static int bcg_launch(alpb_batched_cg_s *h, const double *b, double *x, int64_t 
 	a.gs = h->gs;
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3(h->grid);
-	cfg.blockDim = dim3(MP_BLOCK);
+	cfg.blockDim = dim3(32 * BCG_WARPS);
 	cfg.stream = s;
 	cudaLaunchAttribute attr[1];
 	attr[0].id = cudaLaunchAttributeCooperative;
@@ -466,15 +493,14 @@ int alpb_batched_cg_create(alpb_batched_cg *out, int64_t n, int64_t nnz, const i
 		return rc;
 	}
 	const int64_t nt = h->plan.ntiles;
-	h->grid = cooperative_grid(k_batched_cg, MP_BLOCK, 0, 0);
-	if (h->grid > 2 * sm_count()) h->grid = 2 * sm_count();
+	h->grid = solver_grid(k_batched_cg, 32 * BCG_WARPS, nt, BCG_WARPS);
 	if (h->grid <= 0) {
 		alpb_batched_cg_destroy(h);
 		set_error("alpb_batched_cg_create: no cooperative occupancy");
 		return ALPB_PANIC;
 	}
 	if (cudaMalloc(&h->work, size_t(4 * n) * 8) != cudaSuccess ||
-		cudaMalloc(&h->scratch, size_t(4 * nt) * 8) != cudaSuccess ||
+		cudaMalloc(&h->scratch, size_t(2 * nt) * 8) != cudaSuccess ||
 		cudaMalloc(&h->inst, size_t(nseg) * sizeof(BcgInst)) != cudaSuccess ||
 		cudaMalloc(&h->active, 8) != cudaSuccess || cudaMalloc(&h->gs, sizeof(GridSync)) != cudaSuccess) {
 		cudaGetLastError();
@@ -501,6 +527,7 @@ int alpb_batched_cg_destroy(alpb_batched_cg h) {
 	cudaFree(h->plan.tail_val);
 	cudaFree(h->plan.head_has);
 	cudaFree(h->plan.tail_has);
+	cudaFree(h->plan.ready);
 	cudaFree(h->work);
 	cudaFree(h->scratch);
 	cudaFree(h->inst);
@@ -558,7 +585,7 @@ int alpb_batched_cg_results(alpb_batched_cg h, int64_t *iterations, double *resi
 		cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaMemcpyAsync(&gs, h->gs, sizeof(GridSync), cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
-	ALPB_CHECK(gs.err == 0, ALPB_PANIC, "alpb_batched_cg: grid barrier timed out");
+	ALPB_CHECK(gs.err == 0, ALPB_PANIC, "alpb_batched_cg: a grid barrier or tile wait timed out");
 	int all = 1;
 	for (size_t i = 0; i < v.size(); ++i) {
 		if (iterations) iterations[i] = v[i].iterations;

@@ -45,8 +45,13 @@ __device__ __forceinline__ double opd(int op, double a, double b) {
 	case ALPB_OP_RIGHT_ASSIGN: return b;
 	case ALPB_OP_LOR: return (a != 0.0 || b != 0.0) ? 1.0 : 0.0;
 	case ALPB_OP_LAND: return (a != 0.0 && b != 0.0) ? 1.0 : 0.0;
+	case ALPB_OP_LEFT_ASSIGN_IF: return a;  // callers test opd_skips first
 	}
 	return 0.0;
+}
+// True where op leaves its output unchanged (left_assign_if with b false).
+__device__ __forceinline__ bool opd_skips(int op, double b) {
+	return op == ALPB_OP_LEFT_ASSIGN_IF && b == 0.0;
 }
 
 struct VecArgs {
@@ -98,17 +103,24 @@ __global__ void k_vec(VecArgs a) {
 			if (!xh) break;
 			if (zh) {
 				const double zv = ld_val(a.z, a.zt, i);
+				if (opd_skips(a.op, a.kind == ALPB_VEC_FOLDL ? xv : zv)) break;
 				out = a.kind == ALPB_VEC_FOLDL ? opd(a.op, zv, xv) : opd(a.op, xv, zv);
 				write = true;
-			} else if (a.monoid && a.x != nullptr) {
-				// monoid fold into an absent entry: identity op x_i
+			} else if (a.monoid) {
+				// monoid fold into an absent entry: identity op x_i (a scalar x
+				// reaches every absent entry, reference/blas1.hpp:957-981)
 				out = a.kind == ALPB_VEC_FOLDL ? opd(a.op, a.identity, xv) : opd(a.op, xv, a.identity);
 				write = true;
 				assign = true;
 			}
 			break;
 		case ALPB_VEC_APPLY:  // z_i = x_i op y_i: operator = intersection, monoid = union
-			if (xh && yh) { out = opd(a.op, xv, yv); write = true; assign = true; }
+			if (xh && yh) {
+				if (opd_skips(a.op, yv)) break;
+				out = opd(a.op, xv, yv);
+				write = true;
+				assign = true;
+			}
 			else if (a.monoid && (xh || yh)) {
 				out = xh ? opd(a.op, xv, a.identity) : opd(a.op, a.identity, yv);
 				write = true;
@@ -116,7 +128,7 @@ __global__ void k_vec(VecArgs a) {
 			}
 			break;
 		case ALPB_VEC_MULADD: {  // z_i = z_i (+) (x_i (*) y_i) over the ring
-			if (!(xh && yh)) break;
+			if (!(xh && yh) || opd_skips(a.mul_op, yv)) break;
 			const double prod = opd(a.mul_op, xv, yv);
 			if (zh) out = opd(a.op, ld_val(a.z, a.zt, i), prod);
 			else { out = prod; assign = true; }
@@ -168,7 +180,9 @@ __global__ void k_vec_dot(int add_op, double ident, int mul_op, int64_t n, const
 		if (y && ya && !ya[i]) continue;
 		if (masked && !eval_mask(m, ma, mt, descr, i)) continue;
 		const double xv = ld_val(x, xt, i);
-		const double t = y ? opd(mul_op, xv, ld_val(y, yt, i)) : xv;
+		const double yv = y ? ld_val(y, yt, i) : 0.0;
+		if (y && opd_skips(mul_op, yv)) continue;
+		const double t = y ? opd(mul_op, xv, yv) : xv;
 		acc = any ? opd(add_op, acc, t) : opd(add_op, ident, t);
 		any = true;
 	}
@@ -195,7 +209,8 @@ int alpb_vec_reduce(double *result, int add_op, double identity, int mul_op, uin
 	int masked, void *stream) {
 	ALPB_CHECK(result != nullptr, ALPB_ILLEGAL, "alpb_vec_reduce: null result");
 	ALPB_CHECK(add_op >= ALPB_OP_ADD && add_op <= ALPB_OP_LAND && mul_op >= ALPB_OP_ADD &&
-		mul_op <= ALPB_OP_LAND, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op, mul_op);
+		mul_op <= ALPB_OP_LEFT_ASSIGN_IF, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op,
+		mul_op);
 	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
 	cudaStream_t s = as_stream(stream);
 	int64_t g64 = (n + 256 * 8 - 1) / (256 * 8);
@@ -234,7 +249,8 @@ int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_op, uint3
 	const void *y, int y_type, const uint8_t *y_assigned, double beta, void *stream) {
 	ALPB_CHECK(kind >= ALPB_VEC_SET && kind <= ALPB_VEC_MULADD, ALPB_ILLEGAL,
 		"alpb_vec_op: kind %d", kind);
-	ALPB_CHECK(op >= ALPB_OP_ADD && op <= ALPB_OP_LAND, ALPB_UNSUPPORTED, "alpb_vec_op: op %d", op);
+	ALPB_CHECK(op >= ALPB_OP_ADD && op <= ALPB_OP_LEFT_ASSIGN_IF, ALPB_UNSUPPORTED,
+		"alpb_vec_op: op %d", op);
 	ALPB_CHECK(type_size(z_type) > 0, ALPB_UNSUPPORTED, "alpb_vec_op: output type %d", z_type);
 	ALPB_CHECK(z_assigned == nullptr || z_nnz != nullptr, ALPB_ILLEGAL,
 		"alpb_vec_op: sparse output needs its nnz counter");

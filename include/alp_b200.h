@@ -300,7 +300,11 @@ enum alpb_op {
 	ALPB_OP_ADD = 0, ALPB_OP_SUB = 1, ALPB_OP_MUL = 2, ALPB_OP_DIV = 3,
 	ALPB_OP_MIN = 4, ALPB_OP_MAX = 5, ALPB_OP_ABS_DIFF = 6,
 	ALPB_OP_LEFT_ASSIGN = 7, ALPB_OP_RIGHT_ASSIGN = 8,
-	ALPB_OP_LOR = 9, ALPB_OP_LAND = 10
+	ALPB_OP_LOR = 9, ALPB_OP_LAND = 10,
+	/* operators::left_assign_if (base/internalops.hpp:485-570): a where b is
+	 * true; where b is false the output is left as it was, so the term is
+	 * skipped (dot, fold) or nothing is written (element-wise kinds). */
+	ALPB_OP_LEFT_ASSIGN_IF = 11
 };
 /* *result = *result (+) sum_i x_i (*) y_i with (+) = add_op, (*) = mul_op,
  * over entries assigned in both; result is a HOST double (synchronises). */

@@ -221,9 +221,10 @@ namespace grb {
 		(void) monoid;
 		if( phase == RESIZE ) { return SUCCESS; }
 		using namespace internal::b200rt;
+		// absent entries take beta (reference/blas1.hpp:957-981)
 		return vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDL,
-			monoid_code< Monoid >::value, false, 0.0, 0, x, nullptr, nullptr,
-			static_cast< double >( beta ), nullptr, 0.0 );
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, x, nullptr,
+			nullptr, static_cast< double >( beta ), nullptr, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Op, typename IOType,
@@ -242,6 +243,24 @@ namespace grb {
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
+		typename MaskType, typename InputType, typename Coords >
+	RC foldl( Vector< IOType, b200, Coords > &x, const Vector< MaskType, b200, Coords > &m,
+		const InputType beta, const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< IOType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType >::value &&
+			grb::is_monoid< Monoid >::value, void >::type * = nullptr
+	) {
+		(void) monoid;
+		if( size( m ) == 0 ) { return foldl< descr >( x, beta, monoid, phase ); }
+		if( size( m ) != size( x ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, IOType, IOType, IOType, MaskType >( ALPB_VEC_FOLDL,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, x, &m, nullptr,
+			static_cast< double >( beta ), nullptr, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
 		typename InputType, typename Coords >
 	RC foldr( const InputType &alpha, Vector< IOType, b200, Coords > &y,
 		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
@@ -253,8 +272,8 @@ namespace grb {
 		if( phase == RESIZE ) { return SUCCESS; }
 		using namespace internal::b200rt;
 		return vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDR,
-			monoid_code< Monoid >::value, false, 0.0, 0, y, nullptr, nullptr,
-			static_cast< double >( alpha ), nullptr, 0.0 );
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, y, nullptr,
+			nullptr, static_cast< double >( alpha ), nullptr, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class OP, typename IOType,
@@ -485,6 +504,116 @@ namespace grb {
 			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
 			op_code< typename Ring::MultiplicativeOperator >::value, z, nullptr, &x, 0.0, nullptr,
 			static_cast< double >( beta ) );
+	}
+
+	/** z = z (+) (alpha (*) beta): nothing when either is the ring's zero, else
+	 *  a fold of the product into z (reference/blas1.hpp:8824-8897). */
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
+		typename InputType2, typename OutputType, typename Coords >
+	RC eWiseMul( Vector< OutputType, b200, Coords > &z, const InputType1 alpha,
+		const InputType2 beta, const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_semiring< Ring >::value, void >::type * const = nullptr
+	) {
+		if( ( descr & descriptors::dense ) && nnz( z ) < size( z ) ) { return ILLEGAL; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		if( alpha == ring.template getZero< typename Ring::D1 >() ) { return SUCCESS; }
+		if( beta == ring.template getZero< typename Ring::D2 >() ) { return SUCCESS; }
+		typename Ring::D3 temp;
+		(void) grb::apply( temp, alpha, beta, ring.getMultiplicativeOperator() );
+		return foldl< descr >( z, temp, ring.getAdditiveMonoid(), phase );
+	}
+
+	/** Masked eWiseMul: z_i = z_i (+) (x_i (*) y_i) where the mask admits i and
+	 *  both operands are present (reference/blas1.hpp:8899-9260). */
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
+		typename InputType2, typename OutputType, typename MaskType, typename Coords >
+	RC eWiseMul( Vector< OutputType, b200, Coords > &z, const Vector< MaskType, b200, Coords > &m,
+		const Vector< InputType1, b200, Coords > &x, const Vector< InputType2, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			!grb::is_object< MaskType >::value && grb::is_semiring< Ring >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( m ) == 0 ) { return eWiseMul< descr >( z, x, y, ring, phase ); }
+		const size_t n = size( z );
+		if( size( m ) != n || size( x ) != n || size( y ) != n ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		if( nnz( x ) == 0 || nnz( y ) == 0 ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType1, InputType2, MaskType >( ALPB_VEC_MULADD,
+			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
+			op_code< typename Ring::MultiplicativeOperator >::value, z, &m, &x, 0.0, &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
+		typename InputType2, typename OutputType, typename MaskType, typename Coords >
+	RC eWiseMul( Vector< OutputType, b200, Coords > &z, const Vector< MaskType, b200, Coords > &m,
+		const InputType1 alpha, const Vector< InputType2, b200, Coords > &y,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			!grb::is_object< MaskType >::value && grb::is_semiring< Ring >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( m ) == 0 ) { return eWiseMul< descr >( z, alpha, y, ring, phase ); }
+		const size_t n = size( z );
+		if( size( m ) != n || size( y ) != n ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		if( nnz( y ) == 0 || alpha == ring.template getZero< typename Ring::D1 >() ) {
+			return SUCCESS;
+		}
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType2, InputType2, MaskType >( ALPB_VEC_MULADD,
+			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
+			op_code< typename Ring::MultiplicativeOperator >::value, z, &m, nullptr,
+			static_cast< double >( alpha ), &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
+		typename InputType2, typename OutputType, typename MaskType, typename Coords >
+	RC eWiseMul( Vector< OutputType, b200, Coords > &z, const Vector< MaskType, b200, Coords > &m,
+		const Vector< InputType1, b200, Coords > &x, const InputType2 beta,
+		const Ring &ring = Ring(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			!grb::is_object< MaskType >::value && grb::is_semiring< Ring >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( m ) == 0 ) { return eWiseMul< descr >( z, x, beta, ring, phase ); }
+		const size_t n = size( z );
+		if( size( m ) != n || size( x ) != n ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		if( nnz( x ) == 0 || beta == ring.template getZero< typename Ring::D2 >() ) {
+			return SUCCESS;
+		}
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType1, InputType1, MaskType >( ALPB_VEC_MULADD,
+			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
+			op_code< typename Ring::MultiplicativeOperator >::value, z, &m, &x, 0.0, nullptr,
+			static_cast< double >( beta ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
+		typename InputType2, typename OutputType, typename MaskType, typename Coords >
+	RC eWiseMul( Vector< OutputType, b200, Coords > &z, const Vector< MaskType, b200, Coords > &m,
+		const InputType1 alpha, const InputType2 beta, const Ring &ring = Ring(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			!grb::is_object< MaskType >::value && grb::is_semiring< Ring >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( m ) == 0 ) { return eWiseMul< descr >( z, alpha, beta, ring, phase ); }
+		if( size( m ) != size( z ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		if( alpha == ring.template getZero< typename Ring::D1 >() ) { return SUCCESS; }
+		if( beta == ring.template getZero< typename Ring::D2 >() ) { return SUCCESS; }
+		typename Ring::D3 temp;
+		(void) grb::apply( temp, alpha, beta, ring.getMultiplicativeOperator() );
+		return foldl< descr >( z, m, temp, ring.getAdditiveMonoid(), phase );
 	}
 
 	// ---------------------------------------------------------- eWiseMulAdd --

@@ -165,6 +165,20 @@ namespace grb {
 		return internal::b200rt::spmv< descr, true >( u, empty, A, v, empty, ring, phase );
 	}
 
+
+	/** eWiseLambda over a matrix: f( i, j, a_ij ) on the host for every stored
+	 *  entry; changed values reach both stored orientations.  Vectors among
+	 *  `args` are made readable on the host first. */
+	template< Descriptor descr = descriptors::no_operation, class Func, typename DataType,
+		typename RIT, typename CIT, typename NIT, typename... Args >
+	RC eWiseLambda( const Func f, const Matrix< DataType, b200, RIT, CIT, NIT > &A,
+		const Args &... args
+	) {
+		internal::b200rt::touch( args... );
+		Func g = f;
+		return const_cast< Matrix< DataType, b200, RIT, CIT, NIT > & >( A ).b200_host_lambda( g );
+	}
+
 }
 
 #endif

@@ -104,7 +104,19 @@ namespace grb {
 				const int mt = mask ? type_code< MaskType >::value : ALPB_VOID;
 				if( zt < 0 || mt < 0 ) { return UNSUPPORTED; }
 				x.b200_device_ready();
-				if( mask ) { mask->b200_device_ready(); }
+				if( mask ) {
+					mask->b200_device_ready();
+					// the output is replaced, not updated, unless the dense descriptor
+					// comes with a structurally dense mask (reference/io.hpp:509-520)
+					const bool mask_dense = ( descr & descriptors::structural ) &&
+						!( descr & descriptors::invert_mask ) &&
+						( ( descr & descriptors::dense ) || nnz( *mask ) == n );
+					if( ( descr & descriptors::dense ) && mask_dense ) {
+						return set_scalar< descr, DataType, MaskType, T, Coords >( x, nullptr, val );
+					}
+					const RC crc = clear( x );
+					if( crc != SUCCESS ) { return crc; }
+				}
 				if( !mask && !( descr & descriptors::use_index ) ) {
 					const RC rc = check( alpb_set_scalar( x.b200_values(), zt, n, static_cast< double >( val ),
 						x.b200_flags(), x.b200_counter(), stream() ), "set" );
@@ -130,6 +142,8 @@ namespace grb {
 		const typename std::enable_if< !grb::is_object< DataType >::value &&
 			!grb::is_object< T >::value, void >::type * const = nullptr
 	) {
+		// the dense descriptor promises a dense output (reference/io.hpp:404-406)
+		if( ( descr & descriptors::dense ) && nnz( x ) < size( x ) ) { return ILLEGAL; }
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::set_scalar< descr, DataType, bool, T, Coords >( x, nullptr, val );
 	}
@@ -143,6 +157,9 @@ namespace grb {
 	) {
 		if( size( m ) == 0 ) { return set< descr >( x, val, phase ); }
 		if( size( m ) != size( x ) ) { return MISMATCH; }
+		if( ( descr & descriptors::dense ) && ( nnz( x ) < size( x ) || nnz( m ) < size( x ) ) ) {
+			return ILLEGAL;  // reference/io.hpp:498-501
+		}
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::set_scalar< descr >( x, &m, val );
 	}
@@ -155,6 +172,7 @@ namespace grb {
 			!grb::is_object< T >::value, void >::type * const = nullptr
 	) {
 		if( i >= size( x ) ) { return MISMATCH; }
+		if( ( descr & descriptors::dense ) && nnz( x ) < size( x ) ) { return ILLEGAL; }
 		if( phase == RESIZE ) { return SUCCESS; }
 		x.b200_host_set( i, static_cast< DataType >( val ) );
 		return SUCCESS;
@@ -168,6 +186,9 @@ namespace grb {
 	) {
 		using namespace internal::b200rt;
 		if( size( x ) != size( y ) ) { return MISMATCH; }
+		if( ( descr & descriptors::dense ) && ( nnz( y ) < size( y ) || nnz( x ) < size( x ) ) ) {
+			return ILLEGAL;  // reference/io.hpp:698-702
+		}
 		if( phase == RESIZE ) { return SUCCESS; }
 		const size_t n = size( x );
 		if( n == 0 ) { return SUCCESS; }
@@ -188,8 +209,8 @@ namespace grb {
 		return rc;
 	}
 
-	/** x = y where the mask allows it; elsewhere x keeps its entries
-	 *  (reference/io.hpp masked set). */
+	/** x = y where the mask allows it; x's other entries are removed
+	 *  (reference/io.hpp:826-1000, masked set). */
 	template< Descriptor descr = descriptors::no_operation, typename OutputType,
 		typename MaskType, typename InputType, typename Coords >
 	RC set( Vector< OutputType, b200, Coords > &x, const Vector< MaskType, b200, Coords > &mask,
@@ -201,6 +222,10 @@ namespace grb {
 		using namespace internal::b200rt;
 		if( size( mask ) == 0 ) { return set< descr >( x, y, phase ); }
 		if( size( x ) != size( y ) || size( x ) != size( mask ) ) { return MISMATCH; }
+		if( ( descr & descriptors::dense ) && ( nnz( x ) < size( x ) || nnz( y ) < size( y ) ||
+				nnz( mask ) < size( mask ) ) ) {
+			return ILLEGAL;  // reference/io.hpp:865-871
+		}
 		if( phase == RESIZE ) { return SUCCESS; }
 		const size_t n = size( x );
 		const int zt = type_code< OutputType >::value, yt = type_code< InputType >::value,
@@ -209,6 +234,14 @@ namespace grb {
 		x.b200_device_ready();
 		y.b200_device_ready();
 		mask.b200_device_ready();
+		// the output is replaced, not updated, unless the dense descriptor comes
+		// with a structurally dense mask (reference/io.hpp:899-907)
+		const bool mask_dense = ( descr & descriptors::structural ) &&
+			!( descr & descriptors::invert_mask ) && nnz( mask ) == n;
+		if( !( ( descr & descriptors::dense ) && mask_dense ) ) {
+			const RC crc = clear( x );
+			if( crc != SUCCESS ) { return crc; }
+		}
 		const RC rc = check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0, descr, n,
 			x.b200_values(), zt, x.b200_flags(), x.b200_counter(), mask.b200_values(),
 			mask.b200_flags_or_dense(), mt, 1, y.b200_values(), yt, y.b200_flags_or_dense(), 0.0,

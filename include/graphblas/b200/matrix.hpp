@@ -17,6 +17,7 @@
 #include <stdexcept>
 #include <utility>
 #include <vector>
+#include <algorithm>
 
 #include <graphblas/base/matrix.hpp>
 #include <graphblas/b200/runtime.hpp>
@@ -217,6 +218,53 @@ namespace grb {
 			}
 
 			void b200_reserve( const size_t cap ) { if( cap > _cap ) { _cap = cap; } }
+
+			/** Runs f( i, j, v ) on the host for every stored entry, in CRS order,
+			 *  and writes the (possibly changed) values back to both orientations.
+			 *  Host lambdas cannot run on the device; this is the matrix form of
+			 *  eWiseLambda (reference/blas2.hpp, eWiseLambda over a matrix). */
+			template< class F >
+			RC b200_host_lambda( F &f ) {
+				using namespace internal::b200rt;
+				if( _nz == 0 ) { return SUCCESS; }
+				if( !_crs.values || !_ccs.values ) { return UNSUPPORTED; }
+				std::vector< int64_t > ro( _m + 1 ), co( _n + 1 );
+				std::vector< uint32_t > ri( _nz ), ci( _nz );
+				std::vector< storage_type > rv( _nz ), cv( _nz );
+				(void) alpb_memcpy_d2h( ro.data(), _crs.offsets, ( _m + 1 ) * 8, stream() );
+				(void) alpb_memcpy_d2h( ri.data(), _crs.indices, _nz * 4, stream() );
+				(void) alpb_memcpy_d2h( rv.data(), _crs.values, _nz * sizeof( storage_type ), stream() );
+				(void) alpb_memcpy_d2h( co.data(), _ccs.offsets, ( _n + 1 ) * 8, stream() );
+				(void) alpb_memcpy_d2h( ci.data(), _ccs.indices, _nz * 4, stream() );
+				RC rc = check( alpb_stream_sync( stream() ), "eWiseLambda (matrix)" );
+				if( rc != SUCCESS ) { return rc; }
+				for( size_t i = 0; i < _m; ++i ) {
+					for( int64_t k = ro[ i ]; k < ro[ i + 1 ]; ++k ) {
+						D v = static_cast< D >( rv[ k ] );
+						f( i, static_cast< size_t >( ri[ k ] ), v );
+						rv[ k ] = static_cast< storage_type >( v );
+					}
+				}
+				// the CCS holds the same entries: find each (j, i) in row i of the CRS
+				std::vector< std::pair< uint32_t, int64_t > > byrow( _nz );
+				for( size_t i = 0; i < _m; ++i ) {
+					for( int64_t k = ro[ i ]; k < ro[ i + 1 ]; ++k ) { byrow[ k ] = { ri[ k ], k }; }
+					std::sort( byrow.begin() + ro[ i ], byrow.begin() + ro[ i + 1 ] );
+				}
+				for( size_t j = 0; j < _n; ++j ) {
+					for( int64_t kk = co[ j ]; kk < co[ j + 1 ]; ++kk ) {
+						const uint32_t i = ci[ kk ];
+						const auto first = byrow.begin() + ro[ i ], last = byrow.begin() + ro[ i + 1 ];
+						const auto it = std::lower_bound( first, last,
+							std::make_pair( static_cast< uint32_t >( j ), int64_t( -1 ) ) );
+						if( it == last || it->first != j ) { return PANIC; }
+						cv[ kk ] = rv[ it->second ];
+					}
+				}
+				(void) alpb_memcpy_h2d( _crs.values, rv.data(), _nz * sizeof( storage_type ), stream() );
+				(void) alpb_memcpy_h2d( _ccs.values, cv.data(), _nz * sizeof( storage_type ), stream() );
+				return check( alpb_stream_sync( stream() ), "eWiseLambda (matrix)" );
+			}
 
 			/** Replace the contents by the (I, J, V) triples, in input order: both
 			 *  orientations are built on the device with the reference's in-row

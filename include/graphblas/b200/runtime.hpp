@@ -87,6 +87,10 @@ namespace grb {
 			struct op_code< operators::logical_or< A, B, C, X > > { static constexpr int value = ALPB_OP_LOR; };
 			template< typename A, typename B, typename C, Backend X >
 			struct op_code< operators::logical_and< A, B, C, X > > { static constexpr int value = ALPB_OP_LAND; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::left_assign_if< A, B, C, X > > {
+				static constexpr int value = ALPB_OP_LEFT_ASSIGN_IF;
+			};
 			// on real domains the conjugating multiplications are plain products
 			template< typename A, typename B, typename C, Backend X >
 			struct op_code< operators::conjugate_right_mul< A, B, C, X > > {

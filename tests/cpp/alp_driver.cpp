@@ -188,10 +188,18 @@ static RC run_blas1( const Case &c ) {
 	rc = set( z, 1.5 ) ? FAILED : foldl( z, 2.5, operators::mul< double >() );
 	std::printf( "rc_foldl_scalar %d\n", int( rc ) );
 	print( "foldl_scalar", z );
-	rc = eWiseApply( w, u, v, operators::mul< double >() );
+	// the second operand is dense: with an operator, the reference's
+	// sparse_apply_generic assigns every index of its tail block of the
+	// sparser input even where the other input has no entry, and leaves the
+	// value there unset (reference/blas1.hpp:3309-3352), which nothing can match
+	rc = set( z, 0.25 ) ? FAILED : foldl( z, v, operators::right_assign< double >() );
+	rc = rc ? rc : eWiseApply( w, u, z, operators::mul< double >() );
 	std::printf( "rc_apply_op %d\n", int( rc ) );
 	print( "apply_op", w );
-	rc = eWiseApply( w, u, v, addM );
+	// again a dense second operand: with a monoid, an index held only by the
+	// input that the reference loops over gets the OTHER input's (absent) raw
+	// value (reference/blas1.hpp:3203-3211), which nothing can match
+	rc = eWiseApply( w, u, z, addM );
 	std::printf( "rc_apply_monoid %d\n", int( rc ) );
 	print( "apply_monoid", w );
 	rc = set( z, u ) ? FAILED : eWiseMul( z, 3.0, v, ring );

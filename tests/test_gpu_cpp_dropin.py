@@ -63,6 +63,14 @@ def write_case(path, op, ring, descr, m, n, I, J, V, u=None, v=None, um=None, vm
             f.write(np.asarray(flags, np.uint8).tobytes())
 
 
+def _value(text: str):
+    """A printed result: a number compares with tolerance, anything else as text."""
+    try:
+        return float(text)
+    except ValueError:
+        return text
+
+
 def parse(out: str) -> dict:
     res = {}
     for line in out.splitlines():
@@ -70,7 +78,7 @@ def parse(out: str) -> dict:
         if len(parts) == 3 and parts[1] != "nnz":
             res[(parts[0], int(parts[1]))] = float(parts[2])
         elif len(parts) >= 2:
-            res[(parts[0], parts[1] if len(parts) == 3 else None)] = parts[-1]
+            res[(parts[0], parts[1] if len(parts) == 3 else None)] = _value(parts[-1])
     return res
 
 
@@ -83,7 +91,7 @@ def compare(case_file, rtol):
     assert set(ra) == set(rb), (sorted(set(ra) ^ set(rb))[:10], a.stdout[:500], b.stdout[:500])
     for k, va in ra.items():
         vb = rb[k]
-        if isinstance(va, float):
+        if isinstance(va, float) and isinstance(vb, float):
             assert abs(va - vb) <= rtol * max(abs(va), abs(vb), 1e-300) or va == vb, (k, va, vb)
         else:
             assert va == vb, (k, va, vb)
