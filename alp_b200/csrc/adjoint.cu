@@ -35,8 +35,15 @@ k_sddmm(MergeTables mt, const int64_t *__restrict__ offsets, const uint32_t *__r
 	for (int64_t t = int64_t(blockIdx.x) * SDDMM_WARPS + w; t < mt.ntiles;
 		 t += int64_t(gridDim.x) * SDDMM_WARPS) {
 		const int64_t i0 = mt.tile_row[t], i1 = mt.tile_row[t + 1];
-		int64_t d0 = t * WM_TILE, d1 = d0 + WM_TILE;
-		if (d1 > m + nnz) d1 = m + nnz;
+		int64_t d0, d1;
+		if (mt.tile_d) {  // row-aligned or per-segment tiles
+			d0 = mt.tile_d[t];
+			d1 = mt.tile_d[t + 1];
+		} else {
+			d0 = t * WM_TILE;
+			d1 = d0 + WM_TILE;
+			if (d1 > m + nnz) d1 = m + nnz;
+		}
 		const int64_t j0 = d0 - i0, j1 = d1 - i1;
 		const int nrows = int(i1 - i0), nnzt = int(j1 - j0);
 		for (int k = lane; k <= nrows + 1; k += 32) {

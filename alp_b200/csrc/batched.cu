@@ -2,17 +2,17 @@
 // solved together in ONE persistent cooperative launch.
 //
 // The instances are stored as one block-diagonal CRS (instance i owns rows
-// [seg_rows[i], seg_rows[i+1])).  The merge-path tiles are cut per instance
-// (merge_plan_segmented), so every tile belongs to exactly one instance and
-// every instance scalar (beta, alpha, r.r, gamma, sigma) is a sum over that
-// instance's tiles.  Each iteration has the two phases of the single-system
-// solver (cg.cu) and two grid barriers for the whole batch; the per-instance
-// reductions are finished by the last tile of the instance to arrive
-// (atomic arrival counter, sum in tile order: deterministic), so no extra
-// barrier is spent on them.  An instance that converges (its own relative
-// tolerance, as algorithms::conjugate_gradient tests it,
-// conjugate_gradient.hpp:377-378, :437) or exhausts the iteration budget is
-// masked out; the launch ends when no instance is active.
+// [seg_rows[i], seg_rows[i+1])).  Warp tiles are cut per instance
+// (merge_plan_segmented; whole-row tiles when the rows are short), so every
+// tile belongs to exactly one instance and every instance scalar (beta,
+// alpha, r.r, gamma, sigma) is a sum over that instance's tiles.  An
+// iteration is the single-system solver's two phases (cg.cu), each followed
+// by a per-instance reduction of the tile partials (one warp per instance,
+// fixed order: deterministic), with a grid barrier after each of the four
+// steps.  An instance that converges (its own relative tolerance, as
+// algorithms::conjugate_gradient tests it, conjugate_gradient.hpp:377-378,
+// :437) or exhausts the iteration budget is masked out; the launch ends when
+// no instance is active.
 #include "common.cuh"
 #include "merge.cuh"
 #include "wmerge.cuh"
@@ -29,14 +29,42 @@ namespace alpb {
 using RF = RingPlusTimesF64;
 
 // ------------------------------------------------------ segmented tables --
+// Tiles per instance: whole-row tiles of `rpt` rows when rpt > 0, else
+// merge-path tiles of `tile` items.  An instance without rows is flagged.
 __global__ void k_seg_tile_counts(const int64_t *offsets, const int64_t *seg_rows, int64_t nseg,
-	int64_t *counts, int64_t tile) {
+	int64_t *counts, int64_t tile, int64_t rpt, int32_t *empty) {
 	for (int64_t s = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s <= nseg;
 		 s += int64_t(gridDim.x) * blockDim.x) {
 		if (s == nseg) { counts[s] = 0; continue; }
 		const int64_t r0 = seg_rows[s], r1 = seg_rows[s + 1];
+		if (r1 <= r0) atomicExch(empty, 1);
 		const int64_t items = (r1 - r0) + (offsets[r1] - offsets[r0]);
-		counts[s] = (items + tile - 1) / tile;
+		counts[s] = rpt ? (r1 - r0 + rpt - 1) / rpt : (items + tile - 1) / tile;
+	}
+}
+
+// Whole-row tiles: tile t of instance s holds rows [r0 + k rpt, r0 + (k+1) rpt).
+__global__ void k_seg_aligned(const int64_t *offsets, const int64_t *seg_rows,
+	const int64_t *seg_tile, int64_t nseg, int64_t m, int64_t nnz, int64_t rpt, int64_t *tile_d,
+	int64_t *tile_row, int32_t *tile_seg, int64_t *head_first, int64_t *tail_first,
+	int32_t *span_len) {
+	for (int64_t s = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < nseg;
+		 s += int64_t(gridDim.x) * blockDim.x) {
+		const int64_t r0 = seg_rows[s], r1 = seg_rows[s + 1];
+		for (int64_t t = seg_tile[s]; t < seg_tile[s + 1]; ++t) {
+			int64_t r = r0 + (t - seg_tile[s]) * rpt;
+			if (r > r1) r = r1;
+			tile_row[t] = r;
+			tile_d[t] = r + offsets[r];
+			tile_seg[t] = int32_t(s);
+			head_first[t] = -1;
+			tail_first[t] = -1;
+			span_len[t] = 0;
+		}
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		tile_d[seg_tile[nseg]] = m + nnz;
+		tile_row[seg_tile[nseg]] = m;
 	}
 }
 
@@ -105,23 +133,36 @@ __global__ void k_seg_tables(const int64_t *offsets, int64_t m, int64_t ntiles,
 int merge_plan_segmented(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t nseg,
 	const int64_t *seg_rows, SegmentedTiles *st, cudaStream_t s) {
 	st->nseg = nseg;
+	double maxlen = 0, sumsq = 0;
+	int rc = row_profile(offsets, p->m, &maxlen, &sumsq, s);
+	if (rc != ALPB_SUCCESS) return rc;
+	const int64_t rpt = aligned_rows_per_tile(maxlen, p->m ? double(p->nnz) / double(p->m) : 0.0,
+		WM_TILE);
 	ALPB_CUDA(cudaMalloc(&st->seg_tile, size_t(nseg + 1) * 8));
 	int64_t *counts = nullptr;
+	int32_t *empty = nullptr;
 	void *tmp = nullptr;
 	size_t tb = 0;
 	ALPB_CUDA(cudaMallocAsync(&counts, size_t(nseg + 1) * 8, s));
+	ALPB_CUDA(cudaMallocAsync(&empty, 4, s));
+	ALPB_CUDA(cudaMemsetAsync(empty, 0, 4, s));
 	k_seg_tile_counts<<<grid_for(nseg + 1, 256), 256, 0, s>>>(offsets, seg_rows, nseg, counts,
-		WM_TILE);
+		WM_TILE, rpt, empty);
 	ALPB_LAUNCHED();
 	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, counts, st->seg_tile, nseg + 1, s));
 	ALPB_CUDA(cudaMallocAsync(&tmp, tb, s));
 	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, counts, st->seg_tile, nseg + 1, s));
 	g_launches.fetch_add(1);
 	int64_t nt = 0;
+	int32_t h_empty = 0;
 	ALPB_CUDA(cudaMemcpyAsync(&nt, st->seg_tile + nseg, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaMemcpyAsync(&h_empty, empty, 4, cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaFreeAsync(counts, s));
+	ALPB_CUDA(cudaFreeAsync(empty, s));
 	ALPB_CUDA(cudaFreeAsync(tmp, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
+	// an instance without rows would never finish its iterations
+	ALPB_CHECK(h_empty == 0, ALPB_ILLEGAL, "segmented plan: an instance has no rows");
 	ALPB_CHECK(nt > 0, ALPB_ILLEGAL, "segmented plan: no work");
 	p->ntiles = nt;
 	p->tile = WM_TILE;
@@ -140,15 +181,22 @@ int merge_plan_segmented(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t ns
 	ALPB_CUDA(cudaMalloc(&p->ready, n * 4));
 	ALPB_CUDA(cudaMemsetAsync(p->counter, 0, n * 4, s));
 	ALPB_CUDA(cudaMemsetAsync(p->ready, 0, n * 4, s));
-	k_seg_tile_d<<<grid_for(nseg, 256), 256, 0, s>>>(offsets, seg_rows, st->seg_tile, nseg, p->m,
-		p->nnz, st->tile_d, st->tile_seg, WM_TILE);
-	ALPB_LAUNCHED();
-	k_seg_tile_rows<<<grid_for(nt + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz, nt, st->tile_d,
-		p->tile_row);
-	ALPB_LAUNCHED();
-	k_seg_tables<<<grid_for(nt, 256), 256, 0, s>>>(offsets, p->m, nt, st->tile_d, p->tile_row,
-		p->head_first, p->tail_first, p->span_len);
-	ALPB_LAUNCHED();
+	if (rpt) {
+		k_seg_aligned<<<grid_for(nseg, 256), 256, 0, s>>>(offsets, seg_rows, st->seg_tile, nseg,
+			p->m, p->nnz, rpt, st->tile_d, p->tile_row, st->tile_seg, p->head_first, p->tail_first,
+			p->span_len);
+		ALPB_LAUNCHED();
+	} else {
+		k_seg_tile_d<<<grid_for(nseg, 256), 256, 0, s>>>(offsets, seg_rows, st->seg_tile, nseg,
+			p->m, p->nnz, st->tile_d, st->tile_seg, WM_TILE);
+		ALPB_LAUNCHED();
+		k_seg_tile_rows<<<grid_for(nt + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz, nt,
+			st->tile_d, p->tile_row);
+		ALPB_LAUNCHED();
+		k_seg_tables<<<grid_for(nt, 256), 256, 0, s>>>(offsets, p->m, nt, st->tile_d, p->tile_row,
+			p->head_first, p->tail_first, p->span_len);
+		ALPB_LAUNCHED();
+	}
 	st->seg_rows = const_cast<int64_t *>(seg_rows);
 	return ALPB_SUCCESS;
 }
@@ -265,21 +313,30 @@ __device__ __forceinline__ double warp_sum_tiles(const double *own, int64_t t0, 
 	return warp_sum(v);
 }
 
-// Arrival of one tile of an instance (its partial already stored by lane 0).
-// Every lane learns whether it was the instance's last tile.
-__device__ __forceinline__ bool inst_arrive(BcgInst *in, int64_t ntiles_inst, int lane) {
-	int last = 0;
-	if (lane == 0) {
-		__threadfence();
-		last = atomicAdd(&in->cnt, 1) == ntiles_inst - 1;
+// The instance of tile t and its state for the current phase, fetched one
+// tile ahead by the phase loops.
+struct BcgTileState {
+	int32_t seg = 0;
+	int32_t done = 1;
+	double scalar = 0.0;  // gamma in phase A, alpha in phase B
+};
+
+template <bool ALPHA>
+__device__ __forceinline__ BcgTileState bcg_tile_state(const BcgArgs &a, int64_t t) {
+	BcgTileState st;
+	if (t < a.mt.ntiles) {
+		st.seg = __ldg(a.tile_seg + t);
+		const BcgInst *in = a.inst + st.seg;
+		st.done = __ldcg(&in->done);
+		st.scalar = ALPHA ? __ldcg(&in->alpha) : __ldcg(&in->gamma);
 	}
-	last = __shfl_sync(0xffffffffu, last, 0);
-	if (!last) return false;
-	__threadfence();
-	if (lane == 0) in->cnt = 0;  // next use is after a grid barrier
-	return true;
+	return st;
 }
 
+// Each iteration: phase A (tiles: temp = A u_new, u_new, beta terms) |
+// per-instance alpha | phase B (rows: x, r, r.r terms) | per-instance
+// convergence, gamma; a grid barrier after each.  Per-tile partials are
+// reduced per instance by one warp in a fixed order (deterministic).
 __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 	__shared__ BcgWarpSmem sm[BCG_WARPS];
 	const int64_t G = gridDim.x, nt = a.mt.ntiles;
@@ -320,7 +377,6 @@ __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 			in->iterations = 0;
 			in->done = 0;
 			in->converged = 0;
-			in->cnt = 0;
 		}
 	}
 	if (!grid_sync(a.gs)) return;
@@ -330,57 +386,74 @@ __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 	for (;;) {
 		++iter;
 		++epoch;
-		// phase A over the tiles of active instances: temp = A u_new, beta
-		for (int64_t t = gw; t < nt; t += nw) {
-			const int32_t s = a.tile_seg[t];
-			BcgInst *in = a.inst + s;
-			if (((volatile int32_t *) &in->done)[0]) continue;
-			const double gamma = ((volatile double *) &in->gamma)[0];
-			BcgIter epi{&a, &sm[w], u_old, u_new, gamma};
-			BcgGather xl{a.r, u_old, gamma};
-			const WmMeta g = wm_meta(a.mt, t);
-			if (!warp_tile_ordered<RF>(t, g, a.mt, a.offsets, a.indices, a.values, xl, epi, 0,
-					sm[w].tile, epoch, err))
-				break;
-			const double part = warp_sum(epi.acc);
-			if (lane == 0) a.own[t] = part;
-			const int64_t t0 = a.seg_tile[s], t1 = a.seg_tile[s + 1];
-			if (inst_arrive(in, t1 - t0, lane)) {
-				const double beta = warp_sum_tiles(a.own, t0, t1, lane);
-				if (lane == 0) in->alpha = in->sigma / beta;
+		// phase A over the tiles of active instances
+		{
+			int64_t t = gw;
+			BcgTileState cur = bcg_tile_state<false>(a, t);
+			WmMeta g = wm_meta(a.mt, t);
+			while (t < nt) {
+				const BcgTileState nxt = bcg_tile_state<false>(a, t + nw);
+				const WmMeta gn = wm_meta(a.mt, t + nw);
+				if (!cur.done) {
+					BcgIter epi{&a, &sm[w], u_old, u_new, cur.scalar};
+					BcgGather xl{a.r, u_old, cur.scalar};
+					if (!warp_tile_ordered<RF>(t, g, a.mt, a.offsets, a.indices, a.values, xl, epi,
+							0, sm[w].tile, epoch, err))
+						break;
+					const double part = warp_sum(epi.acc);
+					if (lane == 0) a.own[t] = part;
+				}
+				t += nw;
+				cur = nxt;
+				g = gn;
 			}
 		}
 		if (!grid_sync(a.gs)) return;
-		// phase B: the rows that end in each active tile
-		for (int64_t t = gw; t < nt; t += nw) {
-			const int32_t s = a.tile_seg[t];
+		for (int64_t s = gw; s < a.nseg; s += nw) {
 			BcgInst *in = a.inst + s;
-			if (((volatile int32_t *) &in->done)[0]) continue;
-			const double alpha = ((volatile double *) &in->alpha)[0];
-			double part = 0.0;
-			for (int64_t i = a.mt.tile_row[t] + lane; i < a.mt.tile_row[t + 1]; i += 32) {
-				a.x[i] = a.x[i] + alpha * __ldcg(u_new + i);
-				const double ri = __ldcg(a.r + i) - alpha * __ldcg(a.temp + i);
-				a.r[i] = ri;
-				part += ri * ri;
-			}
-			part = warp_sum(part);
-			if (lane == 0) a.own[t] = part;
-			const int64_t t0 = a.seg_tile[s], t1 = a.seg_tile[s + 1];
-			if (inst_arrive(in, t1 - t0, lane)) {
-				const double rr = warp_sum_tiles(a.own, t0, t1, lane);
-				if (lane == 0) {
-					in->rr = rr;
-					in->iterations = iter;
-					if (sqrt(rr) < in->tol_abs || iter >= a.max_iter) {
-						in->converged = sqrt(rr) < in->tol_abs ? 1 : 0;
-						__threadfence();
-						in->done = 1;
-						atomicSub(a.active, 1);
-					} else {
-						in->gamma = rr / in->sigma;
-						in->sigma = rr;
+			if (__ldcg(&in->done)) continue;
+			const double beta = warp_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], lane);
+			if (lane == 0) in->alpha = in->sigma / beta;
+		}
+		if (!grid_sync(a.gs)) return;
+		// phase B: the rows that end in each active tile
+		{
+			int64_t t = gw;
+			BcgTileState cur = bcg_tile_state<true>(a, t);
+			while (t < nt) {
+				const BcgTileState nxt = bcg_tile_state<true>(a, t + nw);
+				if (!cur.done) {
+					const double alpha = cur.scalar;
+					double part = 0.0;
+					const int64_t r0 = a.mt.tile_row[t], r1 = a.mt.tile_row[t + 1];
+					for (int64_t i = r0 + lane; i < r1; i += 32) {
+						a.x[i] = a.x[i] + alpha * __ldcg(u_new + i);
+						const double ri = __ldcg(a.r + i) - alpha * __ldcg(a.temp + i);
+						a.r[i] = ri;
+						part += ri * ri;
 					}
+					part = warp_sum(part);
+					if (lane == 0) a.own[t] = part;
+				}
+				t += nw;
+				cur = nxt;
+			}
+		}
+		if (!grid_sync(a.gs)) return;
+		for (int64_t s = gw; s < a.nseg; s += nw) {
+			BcgInst *in = a.inst + s;
+			if (__ldcg(&in->done)) continue;
+			const double rr = warp_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], lane);
+			if (lane == 0) {
+				in->rr = rr;
+				in->iterations = iter;
+				if (sqrt(rr) < in->tol_abs || iter >= a.max_iter) {
+					in->converged = sqrt(rr) < in->tol_abs ? 1 : 0;
+					in->done = 1;
+					atomicSub(a.active, 1);
+				} else {
+					in->gamma = rr / in->sigma;
+					in->sigma = rr;
 				}
 			}
 		}

@@ -92,6 +92,58 @@ __global__ void k_merge_tables(const int64_t *offsets, int64_t m, int64_t nnz, i
 	}
 }
 
+// Row-aligned warp tiles: tile t holds rows [t R, (t+1) R) whole, R chosen so
+// that R rows never exceed one tile's items.  No row crosses a tile.
+__global__ void k_row_aligned_tiles(const int64_t *offsets, int64_t m, int64_t rows_per_tile,
+	int64_t ntiles, int64_t *tile_row, int64_t *tile_d, int64_t *head_first, int64_t *tail_first,
+	int32_t *span_len) {
+	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t <= ntiles;
+		 t += int64_t(gridDim.x) * blockDim.x) {
+		int64_t r = t * rows_per_tile;
+		if (r > m) r = m;
+		tile_row[t] = r;
+		tile_d[t] = r + offsets[r];
+		if (t < ntiles) {
+			head_first[t] = -1;
+			tail_first[t] = -1;
+			span_len[t] = 0;
+		}
+	}
+}
+
+// Rows per row-aligned warp tile for rows of at most `maxlen` (mean `mean`)
+// nonzeroes, or 0 when whole-row tiles would not stay at least half full.
+int64_t aligned_rows_per_tile(double maxlen, double mean, int64_t tile) {
+	if (maxlen > double(tile) / 8) return 0;
+	const int64_t r = tile / (int64_t(maxlen) + 1);
+	return double(r) * (mean + 1.0) >= 0.5 * double(tile) ? r : 0;
+}
+
+// Longest row and mean row length of a compressed storage (synchronises).
+int row_profile(const int64_t *offsets, int64_t m, double *maxlen, double *sumsq,
+	cudaStream_t s) {
+	unsigned long long *d_max = nullptr;
+	double *d_sq = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&d_max, 8, s));
+	ALPB_CUDA(cudaMallocAsync(&d_sq, 8, s));
+	ALPB_CUDA(cudaMemsetAsync(d_max, 0, 8, s));
+	ALPB_CUDA(cudaMemsetAsync(d_sq, 0, 8, s));
+	if (m > 0) {
+		k_row_stats<<<grid_for(m, 256, 4), 256, 0, s>>>(offsets, m, d_max, d_sq);
+		ALPB_LAUNCHED();
+	}
+	unsigned long long hmax = 0;
+	double hsq = 0;
+	ALPB_CUDA(cudaMemcpyAsync(&hmax, d_max, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaMemcpyAsync(&hsq, d_sq, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaFreeAsync(d_max, s));
+	ALPB_CUDA(cudaFreeAsync(d_sq, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	*maxlen = double(hmax);
+	if (sumsq) *sumsq = hsq;
+	return ALPB_SUCCESS;
+}
+
 MergeTables merge_tables(const alpb_spmv_plan_s &p) {
 	MergeTables t;
 	t.m = p.m;
@@ -107,6 +159,7 @@ MergeTables merge_tables(const alpb_spmv_plan_s &p) {
 	t.head_has = p.head_has;
 	t.tail_has = p.tail_has;
 	t.ready = p.ready;
+	t.tile_d = p.tile_d;
 	return t;
 }
 
@@ -467,7 +520,8 @@ int plan_build(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t tile, cudaSt
 	p->cv = p->mean > 0 ? sqrt(var > 0 ? var : 0.0) / p->mean : 0.0;
 	// merge-path tile table
 	p->tile = tile;
-	p->ntiles = (p->m + p->nnz + tile - 1) / tile;
+	const int64_t rpt = tile == WM_TILE ? aligned_rows_per_tile(p->maxlen, p->mean, tile) : 0;
+	p->ntiles = rpt ? (p->m + rpt - 1) / rpt : (p->m + p->nnz + tile - 1) / tile;
 	if (p->ntiles > 0) {
 		ALPB_CHECK(tile != MP_TILE || p->nnz + MP_TILE < (int64_t(1) << 31), ALPB_OVERFLW,
 			"alpb_spmv_plan_create: block merge tiles use 32-bit offsets (nnz %lld)",
@@ -485,12 +539,19 @@ int plan_build(alpb_spmv_plan_s *p, const int64_t *offsets, int64_t tile, cudaSt
 		ALPB_CUDA(cudaMalloc(&p->ready, nt * 4));
 		ALPB_CUDA(cudaMemsetAsync(p->counter, 0, nt * 4, s));
 		ALPB_CUDA(cudaMemsetAsync(p->ready, 0, nt * 4, s));
-		k_merge_tiles<<<grid_for(p->ntiles + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz,
-			p->ntiles, p->tile_row, tile);
-		ALPB_LAUNCHED();
-		k_merge_tables<<<grid_for(p->ntiles, 256), 256, 0, s>>>(offsets, p->m, p->nnz, p->ntiles,
-			p->tile_row, p->head_first, p->tail_first, p->span_len, tile);
-		ALPB_LAUNCHED();
+		if (rpt) {
+			ALPB_CUDA(cudaMalloc(&p->tile_d, (nt + 1) * 8));
+			k_row_aligned_tiles<<<grid_for(p->ntiles + 1, 256), 256, 0, s>>>(offsets, p->m, rpt,
+				p->ntiles, p->tile_row, p->tile_d, p->head_first, p->tail_first, p->span_len);
+			ALPB_LAUNCHED();
+		} else {
+			k_merge_tiles<<<grid_for(p->ntiles + 1, 256), 256, 0, s>>>(offsets, p->m, p->nnz,
+				p->ntiles, p->tile_row, tile);
+			ALPB_LAUNCHED();
+			k_merge_tables<<<grid_for(p->ntiles, 256), 256, 0, s>>>(offsets, p->m, p->nnz, p->ntiles,
+				p->tile_row, p->head_first, p->tail_first, p->span_len, tile);
+			ALPB_LAUNCHED();
+		}
 	}
 	return ALPB_SUCCESS;
 }
@@ -558,6 +619,7 @@ int alpb_spmv_plan_destroy(alpb_spmv_plan p) {
 	cudaFree(p->head_has);
 	cudaFree(p->tail_has);
 	cudaFree(p->ready);
+	cudaFree(p->tile_d);
 	delete p;
 	return ALPB_SUCCESS;
 }

@@ -23,6 +23,9 @@ struct alpb_spmv_plan_s {
 	uint8_t *head_has = nullptr;    // ntiles
 	uint8_t *tail_has = nullptr;    // ntiles
 	int32_t *ready = nullptr;       // ntiles (publication epochs, fused solvers)
+	// [ntiles+1] first merge diagonal of each tile when the tiles are cut at
+	// row boundaries (short rows: no row crosses a tile); null: t * tile
+	int64_t *tile_d = nullptr;
 	double mean = 0, maxlen = 0, cv = 0;
 	float tuned_ms = 0;
 };
@@ -65,6 +68,12 @@ int ring_value_type(int ring);
 constexpr int MP_BLOCK = 256;
 constexpr int MP_IPT = 8;
 constexpr int MP_TILE = MP_BLOCK * MP_IPT;
+
+// Rows per row-aligned warp tile for rows of at most `maxlen` (mean `mean`)
+// nonzeroes, or 0 when whole-row tiles would be poorly filled.
+int64_t aligned_rows_per_tile(double maxlen, double mean, int64_t tile);
+// Longest row (and sum of squared row lengths) of a compressed storage.
+int row_profile(const int64_t *offsets, int64_t m, double *maxlen, double *sumsq, cudaStream_t s);
 
 // Plan with merge tables of `tile` items per tile (MP_TILE for the block
 // engine, WM_TILE for the warp engine).
