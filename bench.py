@@ -412,6 +412,12 @@ def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024) -> dict:
             itp[k] = i1.value
     ms_p = timed(plain, 1, stream)
     diff = float(((xb - xp).abs().max() / xp.abs().max()).item())
+    # algorithmic bytes of one CG iteration of instance i: the matrix once
+    # (12 B per nonzero + offsets) and 10 vector passes of 8 B per row (phase
+    # A reads r, u_old and writes temp, u_new; phase B reads x, u_new, r,
+    # temp and writes x, r)
+    per_iter = 12 * nnzs + 8 * (rows + 1) + 80 * rows
+    moved = float((it * per_iter).sum())
     return {"systems": nseg, "rows": n, "nnz": nnz, "tol": tol, "rc": rc,
             "all_converged": bool(conv.all()), "iterations_max": int(it.max()),
             "iterations_sum": int(it.sum()), "plain_iterations_sum": int(itp.sum()),
@@ -419,6 +425,8 @@ def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024) -> dict:
             "batched_solves_per_s": round(nseg / (ms_b * 1e-3), 1),
             "plain_solves_per_s": round(nseg / (ms_p * 1e-3), 1),
             "speedup": round(ms_p / ms_b, 2),
+            "batched_GB/s": round(moved / ms_b / 1e6, 1),
+            "plain_GB/s": round(moved / ms_p / 1e6, 1),
             "max_rel_diff_batched_vs_plain": diff}
 
 

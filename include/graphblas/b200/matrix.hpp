@@ -307,6 +307,28 @@ namespace grb {
 			}
 	};
 
+
+	namespace internal {
+
+		/** Storage accessors under the names ALP's utilities use for the
+		 *  reference backend; a b200 matrix keeps both orientations on the
+		 *  device, so these give the device-side descriptors. */
+		template< typename D, typename RIT, typename CIT, typename NIT >
+		auto getCRS( const Matrix< D, b200, RIT, CIT, NIT > &A ) noexcept
+			-> decltype( A.b200_crs() )
+		{
+			return A.b200_crs();
+		}
+
+		template< typename D, typename RIT, typename CIT, typename NIT >
+		auto getCCS( const Matrix< D, b200, RIT, CIT, NIT > &A ) noexcept
+			-> decltype( A.b200_ccs() )
+		{
+			return A.b200_ccs();
+		}
+
+	}
+
 }
 
 #endif

@@ -173,3 +173,28 @@ def test_driver_pagerank_matches_reference(cuda, oracle):
         f = Path(d) / "case.bin"
         write_case(f, 3, 0, 0, n, n, I, J, np.ones(len(I)))
         compare(f, 1e-9)
+
+
+# ------------------------------------------------------------------ HPCG --
+def _hpcg_result(out: str):
+    import re
+    it = re.search(r"took (\d+) iterations to converge with residual ([0-9.eE+-]+)", out)
+    norm = re.search(r"Residual norm: ([0-9.eE+-]+)", out)
+    assert it and norm, out[-2000:]
+    return int(it.group(1)), float(it.group(2)), float(norm.group(1))
+
+
+def test_hpcg_smoke_matches_reference(cuda):
+    """ALP's HPCG smoke test (tests/smoke/hpcg.cpp: 16^3, multigrid V-cycle with
+    red-black Gauss-Seidel smoothing, CG outer loop), compiled unchanged on
+    b200 and on the reference backend: both print "Test OK", converge in the
+    same number of iterations (within one), and reach ||x - 1|| < 4e-14."""
+    args = ("--test-rep", 1, "--init-iter", 1)
+    a = _run(REF_BIN / "smoke_hpcg_ref", *args)
+    b = _run(B200_BIN / "smoke_hpcg_b200", *args)
+    assert a.returncode == 0 and "Test OK" in a.stdout, a.stdout[-2000:] + a.stderr[-2000:]
+    assert b.returncode == 0 and "Test OK" in b.stdout, b.stdout[-2000:] + b.stderr[-2000:]
+    ia, _, na = _hpcg_result(a.stdout)
+    ib, _, nb = _hpcg_result(b.stdout)
+    assert abs(ia - ib) <= 1, (ia, ib)
+    assert nb < 4e-14, nb
