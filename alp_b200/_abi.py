@@ -85,6 +85,11 @@ PROTOS: dict[str, list] = {
                  P, P, I32, I64,
                  P, P],
     "alpb_mxv_dense_noalloc": [I32, I32, I64, I64, I64, P, P, P, I32, P, P, P],
+    "alpb_hpcg_create": [C.POINTER(P), I64, I64, I64, D, D, I64, I64, I64, I32, P],
+    "alpb_hpcg_destroy": [P],
+    "alpb_hpcg_info": [P, PI64, PI64, PI64, PI],
+    "alpb_hpcg_matrix": [P, I64, C.POINTER(P), C.POINTER(P), C.POINTER(P), PI64, PI64],
+    "alpb_hpcg_solve": [P, P, P, I32, I64, I64, I64, D, P, P, P],
     "alpb_dot_f64": [PD, I32, I32, I64, P, P, P, P, P],
     "alpb_dot_f64_device": [P, I32, I32, I64, P, P, P],
     "alpb_set_scalar": [P, I32, I64, D, P, P, P],

@@ -399,6 +399,39 @@ ALPB_API int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr,
 	int64_t *iterations, double *residual, void *stream);
 
 /* ======================================================================
+ * HPCG: algorithms::hpcg (hpcg/hpcg.hpp:97-223) with its multigrid V-cycle
+ * (hpcg/multigrid_v_cycle.hpp:67-246) and multi-colour Gauss-Seidel smoother
+ * (hpcg/red_black_gauss_seidel.hpp:55-123) on the device, for the system
+ * build_hpcg_system makes (hpcg/system_building_utils.hpp:84-150).
+ * ====================================================================== */
+typedef struct alpb_hpcg_s *alpb_hpcg;
+/* The 3-D 27-point box stencil of nx x ny x nz (diagonal `diag`, the other
+ * 26 entries `off`, in the reference builder's in-row order) and its coarser
+ * levels: each halves every dimension, while the smallest coarse dimension
+ * stays >= min_size and at most max_levels are added; injection is the
+ * coarsening; `colors` static colours (row index modulo colors).  nrhs right-
+ * hand sides (1, 2, 4 or 8) are solved together. */
+ALPB_API int alpb_hpcg_create(alpb_hpcg *h, int64_t nx, int64_t ny, int64_t nz, double diag,
+	double off, int64_t colors, int64_t min_size, int64_t max_levels, int nrhs, void *stream);
+ALPB_API int alpb_hpcg_destroy(alpb_hpcg h);
+/* number of levels, finest rows and nonzeroes; fused_smoother = 1 when no two
+ * neighbouring rows share a colour on any level (each colour step then
+ * updates in place; otherwise it stores the products first). */
+ALPB_API int alpb_hpcg_info(alpb_hpcg h, int64_t *levels, int64_t *n_finest,
+	int64_t *nnz_finest, int *fused_smoother);
+/* device storage of one level's matrix (level 0 is the system) */
+ALPB_API int alpb_hpcg_matrix(alpb_hpcg h, int64_t level, const int64_t **offsets,
+	const uint32_t **indices, const double **values, int64_t *n, int64_t *nnz);
+/* b and x hold n * nrhs doubles, the nrhs values of a row side by side; x
+ * holds the initial guesses.  Each right-hand side runs the reference loop:
+ * stop after an iteration where iter >= max_iterations or
+ * ||r|| / ||r_0|| <= tolerance.  iterations[k] and residuals[k] (||r||, not
+ * squared) are host arrays of nrhs entries. */
+ALPB_API int alpb_hpcg_solve(alpb_hpcg h, const double *b, double *x, int with_preconditioning,
+	int64_t presmoother_steps, int64_t postsmoother_steps, int64_t max_iterations,
+	double tolerance, int64_t *iterations, double *residuals, void *stream);
+
+/* ======================================================================
  * Adjoint gradients of a CG solve (implicit function theorem; no iterate is
  * stored).  No counterpart exists in the reference: the reference checks
  * them by assembling -lambda_i x_j on the host after a reference CG on A^T.
