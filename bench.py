@@ -337,6 +337,7 @@ def extra_workloads(args, A, plan) -> dict:
                          "err_vs_ones_inf": float((x - 1).abs().max().item())}
     del S, ps, work
     out["batched_cg"] = batched_cg_workload(stream)
+    out["hpcg_256"] = hpcg_workload(stream)
     out["adjoint_cg"] = adjoint_workload(stream)
     return out
 
@@ -428,6 +429,54 @@ def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024) -> dict:
             "batched_GB/s": round(moved / ms_b / 1e6, 1),
             "plain_GB/s": round(moved / ms_p / 1e6, 1),
             "max_rel_diff_batched_vs_plain": diff}
+
+
+def hpcg_workload(stream, side: int = 256, coarse_levels: int = 3, nrhs: int = 8) -> dict:
+    """HPCG on the 27-point 256^3 system (diagonal 26, off-diagonals -1) with
+    three coarser levels (128^3, 64^3, 32^3), 27 static colours, one pre- and
+    one post-smoothing step, 8 right-hand sides ~ N(0, 1) solved together,
+    relative tolerance 1e-9, FP64 (alpb_hpcg_solve)."""
+    import ctypes as C
+    import torch
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+    sp = dev.stream_ptr(stream)
+    h = C.c_void_p()
+    abi.call("alpb_hpcg_create", C.byref(h), side, side, side, 26.0, -1.0, 27, 4, coarse_levels,
+             nrhs, sp)
+    lv, n, nnz, fused = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int()
+    abi.call("alpb_hpcg_info", h, C.byref(lv), C.byref(n), C.byref(nnz), C.byref(fused))
+    b = torch.empty(n.value * nrhs, dtype=torch.float64, device="cuda")
+    abi.call("alpb_gen_normal", dev.ptr(b), n.value * nrhs, 31, 1, sp)
+    x = torch.zeros_like(b)
+    it = (C.c_int64 * nrhs)()
+    res = (C.c_double * nrhs)()
+
+    def solve():
+        x.zero_()
+        abi.call("alpb_hpcg_solve", h, dev.ptr(b), dev.ptr(x), 1, 1, 1, 500, 1e-9, it, res, sp)
+    ms = timed(solve, 1, stream)
+    iters = max(it)
+    # algorithmic bytes of one CG iteration.  A smoother sweep runs the 27
+    # colours one after the other; a colour step reads its slice of the
+    # matrix, gathers x at the rows' neighbours (26 of the 27 colours
+    # neighbour it, so nearly all of x: 8 nrhs n bytes, which exceeds the L2
+    # at 256^3) and reads r and reads/writes x on its own rows.  Per V-cycle
+    # the finest level runs four sweeps (forward and backward, before and
+    # after the coarse correction); the CG adds one product and about ten
+    # vector passes; each coarser level adds about 1/8 of the finest.
+    vec = 8 * nrhs * n.value
+    sweep = 12 * nnz.value + 8 * (n.value + 1) + 27 * vec + 3 * vec
+    fine = 4 * sweep + (12 * nnz.value + 8 * (n.value + 1) + 2 * vec) + 10 * vec
+    per_iter = fine * 8 / 7
+    abi.lib().alpb_hpcg_destroy(h)
+    return {"rows": n.value, "nnz": nnz.value, "levels": lv.value, "rhs": nrhs,
+            "fused_smoother": bool(fused.value), "iterations": list(it),
+            "residuals": [float(r) for r in res], "ms_per_solve": round(ms, 2),
+            "ms_per_iteration": round(ms / max(iters, 1), 3),
+            "solves_per_s": round(nrhs / (ms * 1e-3), 3),
+            "GB/s": round(per_iter * iters / ms / 1e6, 1),
+            "bytes_per_iteration": int(per_iter)}
 
 
 def adjoint_workload(stream, side: int = 64) -> dict:
