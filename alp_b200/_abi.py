@@ -90,6 +90,13 @@ PROTOS: dict[str, list] = {
     "alpb_hpcg_info": [P, PI64, PI64, PI64, PI],
     "alpb_hpcg_matrix": [P, I64, C.POINTER(P), C.POINTER(P), C.POINTER(P), PI64, PI64],
     "alpb_hpcg_solve": [P, P, P, I32, I64, I64, I64, D, P, P, P],
+    "alpb_ppr_create": [C.POINTER(P), I64, I64, P, P, P, I32, P],
+    "alpb_ppr_destroy": [P],
+    "alpb_ppr_set_weights": [P, P, P],
+    "alpb_ppr_solve": [P, P, D, D, I64, P, I32, P, P, P],
+    "alpb_ppr_adjoint": [P, P, P, D, I64, P, P, P],
+    "alpb_ppr_grad_weights": [P, P, P, P, P],
+    "alpb_ppr_info": [P, PI64, PI64, PI64, PI64],
     "alpb_dot_f64": [PD, I32, I32, I64, P, P, P, P, P],
     "alpb_dot_f64_device": [P, I32, I32, I64, P, P, P],
     "alpb_set_scalar": [P, I32, I64, D, P, P, P],

@@ -459,6 +459,51 @@ ALPB_API int alpb_cg_grad(int64_t n, const int64_t *row_ptr, const uint32_t *col
 	alpb_spmv_plan plan_crs, alpb_spmv_plan plan_ccs, void *stream);
 
 /* ======================================================================
+ * Personalised PageRank over a weighted graph and its adjoint (differentiable
+ * PageRank).  Extends algorithms::simple_pagerank (simple_pagerank.hpp:146-533),
+ * whose teleport is uniform and whose normalisation is the out-degree count,
+ * to one-hot teleport vectors (seeds) and weighted out-degrees d_i =
+ * sum_j w_ij; with unit weights the normalisation is the reference's.  No
+ * counterpart of the seeds or of the adjoint exists in the reference.
+ *
+ * Per seed s (x_s row-major n x S, the S values of a row side by side):
+ *   x_s = alpha M x_s + (alpha * dangling(x_s) + 1 - alpha) e_seed,
+ *   M_ji = w_ij / d_i, dangling(x) = sum of x over rows with d_i = 0,
+ * by simple_pagerank's power iteration (input pre-scaled by alpha / d_i, L1
+ * residual, stop at residual <= conv; each seed stops on its own).
+ * ====================================================================== */
+typedef struct alpb_ppr_s *alpb_ppr;
+/* The graph is n x n CRS (row i -> column j, weight w_ij >= 0), held by
+ * reference: it must stay valid and unchanged while the handle lives.  nseeds
+ * in [1, 128].  Builds the transpose and the chunk tables. */
+ALPB_API int alpb_ppr_create(alpb_ppr *h, int64_t n, int64_t nnz, const int64_t *row_ptr,
+	const uint32_t *col_idx, const double *weights, int nseeds, void *stream);
+ALPB_API int alpb_ppr_destroy(alpb_ppr h);
+/* New weights on the same pattern (held by reference, like the create call's). */
+ALPB_API int alpb_ppr_set_weights(alpb_ppr h, const double *weights, void *stream);
+/* seeds: host array of nseeds rows.  x (device, n x nseeds) holds the initial
+ * guesses if init_given != 0, else starts at 1/n.  iterations and residuals:
+ * host arrays of nseeds (may be NULL).  ALPB_FAILED when a seed did not
+ * reach conv within max_iter iterations (x still holds the last iterate). */
+ALPB_API int alpb_ppr_solve(alpb_ppr h, const int64_t *seeds, double alpha, double conv,
+	int64_t max_iter, double *x, int init_given, int64_t *iterations, double *residuals,
+	void *stream);
+/* Adjoint of the last solve's fixed point for dl_dx = dL/dx (n x nseeds):
+ *   lambda_s = alpha M^T lambda_s + alpha [i dangling] lambda_s[seed_s] + dl_dx_s,
+ * iterated from lambda = dl_dx with the same per-seed L1 stopping rule.
+ * dL/d(teleport weight of seed s) = (1 - alpha) lambda_s[seed_s]. */
+ALPB_API int alpb_ppr_adjoint(alpb_ppr h, const double *dl_dx, double *lambda, double conv,
+	int64_t max_iter, int64_t *iterations, double *residuals, void *stream);
+/* grad[k] = dL/dw_ij for every stored edge k = (i, j), CRS order:
+ *   alpha / d_i * sum_s x_is (lambda_js - (M^T lambda_s)_i),  0 on dangling rows. */
+ALPB_API int alpb_ppr_grad_weights(alpb_ppr h, const double *x, const double *lambda,
+	double *grad, void *stream);
+/* chunk counts of the two storages (CCS: forward gather; CRS: adjoint) and
+ * how many rows span several chunks. */
+ALPB_API int alpb_ppr_info(alpb_ppr h, int64_t *chunks_ccs, int64_t *multi_ccs,
+	int64_t *chunks_crs, int64_t *multi_crs);
+
+/* ======================================================================
  * Batched CG: many independent SPD systems of uneven size, stored as one
  * block-diagonal CRS (instance i owns rows [seg_rows[i], seg_rows[i+1])),
  * solved in ONE persistent cooperative launch with per-instance convergence
