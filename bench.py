@@ -339,6 +339,7 @@ def extra_workloads(args, A, plan) -> dict:
     out["batched_cg"] = batched_cg_workload(stream)
     out["hpcg_256"] = hpcg_workload(stream)
     out["adjoint_cg"] = adjoint_workload(stream)
+    out["ppr_rmat24"] = ppr_workload(stream)
     return out
 
 
@@ -525,6 +526,67 @@ def adjoint_workload(stream, side: int = 64) -> dict:
             "adjoint_iterations": ita.value, "forward_ms": round(ms_f, 3),
             "gradient_ms": round(ms_g, 3), "gradient_over_forward": round(ms_g / ms_f, 3),
             "forward_solves_per_s": round(1e3 / ms_f, 2), "grads_per_s": round(1e3 / ms_g, 2)}
+
+
+def ppr_workload(stream, scale: int = 24, nseeds: int = 64) -> dict:
+    """Differentiable personalised PageRank on R-MAT scale 24 (edge factor 16,
+    U(0, 1) edge weights), 64 one-hot seeds, alpha 0.85, L1 tolerance 1e-9 per
+    seed: the forward solve (alpb_ppr_solve), the adjoint for dL/dx ~ N(0, 1)
+    (alpb_ppr_adjoint) and the gradient with respect to every edge weight
+    (alpb_ppr_grad_weights), each timed once after a two-iteration warm-up."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+    sp = dev.stream_ptr(stream)
+    A = dev.rmat(scale, vtype=abi.FP64, seed=42)
+    n, nnz, S = A.n, A.nnz, nseeds
+    h = C.c_void_p()
+    abi.call("alpb_ppr_create", C.byref(h), n, nnz, dev.ptr(A.offsets), dev.ptr(A.indices),
+             dev.ptr(A.values), S, sp)
+    seeds = np.ascontiguousarray(np.random.default_rng(scale).integers(0, n, S), np.int64)
+    x = torch.empty(n * S, dtype=torch.float64, device="cuda")
+    g = torch.empty_like(x)
+    abi.call("alpb_gen_normal", dev.ptr(g), n * S, 41, 1, sp)
+    lam = torch.empty_like(x)
+    grad = torch.empty(nnz, dtype=torch.float64, device="cuda")
+    itf, ita = (C.c_int64 * S)(), (C.c_int64 * S)()
+    res = (C.c_double * S)()
+    sd = seeds.ctypes.data_as(C.c_void_p)
+    abi.call("alpb_ppr_solve", h, sd, 0.85, 0.0, 2, dev.ptr(x), 0, itf, res, sp)   # warm-up
+    ms_f = timed(lambda: abi.call("alpb_ppr_solve", h, sd, 0.85, 1e-9, 1000, dev.ptr(x), 0, itf,
+                                  res, sp), 1, stream)
+    ms_a = timed(lambda: abi.call("alpb_ppr_adjoint", h, dev.ptr(g), dev.ptr(lam), 1e-9, 1000,
+                                  ita, res, sp), 1, stream)
+    ms_g = timed(lambda: abi.call("alpb_ppr_grad_weights", h, dev.ptr(x), dev.ptr(lam),
+                                  dev.ptr(grad), sp), 1, stream)
+    mass = float(x.view(n, S).sum(0).sub(1).abs().max())
+    abi.lib().alpb_ppr_destroy(h)
+    kf, ka = max(itf), max(ita)
+    # algorithmic bytes per iteration: the storage once (12 nnz + offsets),
+    # the gathered vector once, and the row-wise vector passes (forward: x
+    # read and written, next input written; adjoint: dL/dx read, next lambda
+    # written); the gathers themselves move 8 S bytes per nonzero, reported
+    # apart as the delivered rate
+    vec = 8 * n * S
+    b_f = 12 * nnz + 8 * (n + 1) + 4 * vec
+    b_a = 12 * nnz + 8 * (n + 1) + 3 * vec
+    b_g = (12 * nnz + 8 * (n + 1) + 2 * vec) + (12 * nnz + 2 * vec)
+    gathered = 8 * S * nnz
+    del A
+    return {"rows": n, "nnz": nnz, "seeds": S, "alpha": 0.85, "tol": 1e-9,
+            "forward_iterations_max": kf, "forward_iterations_min": min(itf),
+            "adjoint_iterations_max": ka, "forward_ms": round(ms_f, 2),
+            "adjoint_ms": round(ms_a, 2), "grad_ms": round(ms_g, 2),
+            "forward_ms_per_iteration": round(ms_f / kf, 3),
+            "adjoint_ms_per_iteration": round(ms_a / ka, 3),
+            "forward_GB/s": round(b_f * kf / ms_f / 1e6, 1),
+            "adjoint_GB/s": round(b_a * ka / ms_a / 1e6, 1),
+            "grad_GB/s": round(b_g / ms_g / 1e6, 1),
+            "forward_gathered_GB/s": round((b_f + gathered) * kf / ms_f / 1e6, 1),
+            "gradient_over_forward": round((ms_a + ms_g) / ms_f, 3),
+            "max_abs_mass_error": mass}
 
 
 # ------------------------------------------------------------ reference arm --
