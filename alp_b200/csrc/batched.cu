@@ -233,6 +233,13 @@ struct BcgArgs {
 	double tol;
 	int32_t *active;                   // instances still iterating
 	GridSync *gs;
+	// sliced storage of short-row systems (slices of 32 rows of one instance;
+	// entry q of the slice's lane-th row at sl_off[t] + 32 q + lane)
+	const int64_t *sl_row;             // [nslices+1] first row of each slice
+	const int64_t *sl_off;             // [nslices+1] first entry of each slice
+	const uint32_t *sl_idx;
+	const double *sl_val;
+	const uint8_t *sl_len;             // [n] row lengths
 };
 
 constexpr int BCG_WARPS = 4;
@@ -313,6 +320,58 @@ __device__ __forceinline__ double warp_sum_tiles(const double *own, int64_t t0, 
 	return warp_sum(v);
 }
 
+// One slice (32 rows of one instance, at most 32 nonzeroes per row) of the
+// sliced storage: lane l owns row sl_row[t] + l and sums its products in
+// storage order (product rounded, then added: the order of the restated
+// CG).  Entry q of all 32 rows is one contiguous line of indices and two of
+// values, so every load is coalesced; the loads of NB entries are issued
+// before their gathers and sums.
+template <class XF, class RowF>
+__device__ __forceinline__ void bcg_slice(const BcgArgs &a, int64_t t, int lane, const XF &xf,
+	RowF &&row) {
+	constexpr int NB = 4;
+	const int64_t r0 = __ldg(a.sl_row + t), r1 = __ldg(a.sl_row + t + 1);
+	const int64_t e0 = __ldg(a.sl_off + t);
+	const int w = int((__ldg(a.sl_off + t + 1) - e0) >> 5);
+	const int64_t i = r0 + lane;
+	const int len = i < r1 ? int(__ldg(a.sl_len + i)) : 0;
+	double acc = 0.0;
+	for (int q0 = 0; q0 < w; q0 += NB) {
+		uint32_t j[NB];
+		double v[NB], x[NB];
+#pragma unroll
+		for (int u = 0; u < NB; ++u) {
+			const int q = q0 + u;
+			const int64_t e = e0 + 32 * int64_t(q) + lane;
+			j[u] = q < w ? __ldcs(a.sl_idx + e) : 0u;
+			v[u] = q < w ? __ldcs(a.sl_val + e) : 0.0;
+		}
+#pragma unroll
+		for (int u = 0; u < NB; ++u) x[u] = q0 + u < len ? xf(j[u]) : 0.0;
+#pragma unroll
+		for (int u = 0; u < NB; ++u)
+			if (q0 + u < len) acc = __dadd_rn(acc, __dmul_rn(v[u], x[u]));
+	}
+	if (i < r1) row(i, acc);
+}
+
+// Sum of the per-tile partials own[t0..t1) by a whole block, in a fixed
+// order (eight interleaved accumulators per thread, then the block tree), the
+// same in every thread.  One block per instance keeps the scalar steps short
+// for the largest instances (thousands of tiles).
+__device__ __forceinline__ double block_sum_tiles(const double *own, int64_t t0, int64_t t1,
+	double *red) {
+	const int64_t nth = blockDim.x;
+	double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+	int64_t k = t0 + threadIdx.x;
+	for (; k + 7 * nth < t1; k += 8 * nth) {
+#pragma unroll
+		for (int u = 0; u < 8; ++u) v[u] += __ldcg(own + k + u * nth);
+	}
+	for (; k < t1; k += nth) v[0] += __ldcg(own + k);
+	return block_sum(((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7])), red);
+}
+
 // The instance of tile t and its state for the current phase, fetched one
 // tile ahead by the phase loops.
 struct BcgTileState {
@@ -333,24 +392,121 @@ __device__ __forceinline__ BcgTileState bcg_tile_state(const BcgArgs &a, int64_t
 	return st;
 }
 
+// Tiles of the instances still iterating, rebuilt by every block after each
+// convergence step (done flags change only there): the active instances in
+// increasing order and the exclusive prefix of their tile counts, so a warp's
+// work items k = gw, gw + nw, ... map to increasing tiles and converged
+// instances cost nothing.  Up to BCG_LIST_MAX instances; more use the walk
+// over all tiles.
+constexpr int BCG_LIST_MAX = 1024;
+constexpr int BCG_RB = 4;    // rows per lane whose loads phase B issues together
+#ifndef ALPB_BCG_ROWS_MINB
+#define ALPB_BCG_ROWS_MINB 8   // resident blocks per SM of the row-aligned variant
+#endif
+
+struct BcgList {
+	int32_t n;                         // active instances
+	int32_t seg[BCG_LIST_MAX];
+	int32_t off[BCG_LIST_MAX + 1];     // tile prefix; off[n] = active tiles
+};
+
+__device__ void bcg_build_list(const BcgArgs &a, BcgList &L, int32_t *scan) {
+	const int nseg = int(a.nseg), nth = blockDim.x, tid = threadIdx.x;
+	const int per = (nseg + nth - 1) / nth;
+	const int s0 = tid * per, s1 = s0 + per < nseg ? s0 + per : nseg;
+	int ci = 0, ct = 0;
+	for (int s = s0; s < s1; ++s) {
+		if (!__ldcg(&a.inst[s].done)) {
+			++ci;
+			ct += int(a.seg_tile[s + 1] - a.seg_tile[s]);
+		}
+	}
+	// block exclusive scan of (ci, ct) in thread order
+	scan[tid] = ci;
+	scan[nth + tid] = ct;
+	__syncthreads();
+	for (int o = 1; o < nth; o <<= 1) {
+		const int vi = tid >= o ? scan[tid - o] : 0;
+		const int vt = tid >= o ? scan[nth + tid - o] : 0;
+		__syncthreads();
+		scan[tid] += vi;
+		scan[nth + tid] += vt;
+		__syncthreads();
+	}
+	int pi = scan[tid] - ci, pt = scan[nth + tid] - ct;
+	for (int s = s0; s < s1; ++s) {
+		if (!__ldcg(&a.inst[s].done)) {
+			L.seg[pi] = s;
+			L.off[pi] = pt;
+			++pi;
+			pt += int(a.seg_tile[s + 1] - a.seg_tile[s]);
+		}
+	}
+	if (tid == nth - 1) {
+		L.n = scan[tid];
+		L.off[scan[tid]] = scan[nth + tid];
+	}
+	__syncthreads();
+}
+
+// Work item k of the active list -> tile and instance; j is the caller's
+// cursor into the list (items are visited in increasing order).
+__device__ __forceinline__ int64_t bcg_item_tile(const BcgArgs &a, const BcgList &L, int32_t k,
+	int &j, int32_t &seg) {
+	while (L.off[j + 1] <= k) ++j;
+	seg = L.seg[j];
+	return a.seg_tile[seg] + (k - L.off[j]);
+}
+
 // Each iteration: phase A (tiles: temp = A u_new, u_new, beta terms) |
 // per-instance alpha | phase B (rows: x, r, r.r terms) | per-instance
 // convergence, gamma; a grid barrier after each.  Per-tile partials are
 // reduced per instance by one warp in a fixed order (deterministic).
-__global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
-	__shared__ BcgWarpSmem sm[BCG_WARPS];
+struct BcgNoSmem {};
+template <bool ROWS> struct BcgTileSmem { typedef BcgWarpSmem type[BCG_WARPS]; };
+template <> struct BcgTileSmem<true> { typedef BcgNoSmem type[1]; };
+
+// ROWS: every tile is row-aligned (the plan's tile_d), so all phases run the
+// lane-per-row code and the merge engine's staging memory is not needed.
+template <bool LIST, bool ROWS>
+__global__ void __launch_bounds__(32 * BCG_WARPS, ROWS ? ALPB_BCG_ROWS_MINB : (LIST ? 5 : 6))
+k_batched_cg(BcgArgs a) {
+	__shared__ typename BcgTileSmem<ROWS>::type sm;
+	__shared__ BcgList L;
+	__shared__ int32_t scan[2 * 32 * BCG_WARPS];
+	__shared__ double red[33];
 	const int64_t G = gridDim.x, nt = a.mt.ntiles;
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	const int64_t gw = int64_t(blockIdx.x) * BCG_WARPS + w, nw = G * BCG_WARPS;
 	int *err = &a.gs->err;
-	for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nt;
-		 t += G * blockDim.x)
-		a.mt.ready[t] = 0;
+	if constexpr (!ROWS) {
+		for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nt;
+			 t += G * blockDim.x)
+			a.mt.ready[t] = 0;
+	}
 	if (!grid_sync(a.gs)) return;
 	int32_t epoch = 1;
 
 	// prelude per instance: r = b - A x, sigma = r.r, tol * ||b||
-	{
+	if constexpr (ROWS) {
+		for (int64_t t = gw; t < nt; t += nw) {
+			double rr = 0.0, bb = 0.0;
+			bcg_slice(a, t, lane, [&](uint32_t j) { return __ldcg(a.x + j); },
+				[&](int64_t i, double v) {
+					const double bi = a.b[i];
+					const double ri = (0.0 + bi) - v;
+					a.r[i] = ri;
+					a.u0[i] = 0.0;
+					rr += ri * ri;
+					bb += bi * bi;
+				});
+			const double s1 = warp_sum(rr), s2 = warp_sum(bb);
+			if (lane == 0) {
+				a.own[t] = s1;
+				a.own2[t] = s2;
+			}
+		}
+	} else {
 		PlainX<double> xl{a.x};
 		for (int64_t t = gw; t < nt; t += nw) {
 			BcgPrelude epi{&a, &sm[w]};
@@ -366,11 +522,11 @@ __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 		}
 	}
 	if (!grid_sync(a.gs)) return;
-	for (int64_t s = gw; s < a.nseg; s += nw) {
+	for (int64_t s = blockIdx.x; s < a.nseg; s += G) {
 		BcgInst *in = a.inst + s;
-		const double sigma = warp_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], lane);
-		const double bnorm = warp_sum_tiles(a.own2, a.seg_tile[s], a.seg_tile[s + 1], lane);
-		if (lane == 0) {
+		const double sigma = block_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], red);
+		const double bnorm = block_sum_tiles(a.own2, a.seg_tile[s], a.seg_tile[s + 1], red);
+		if (threadIdx.x == 0) {
 			in->sigma = sigma;
 			in->gamma = 0.0;
 			in->tol_abs = a.tol * sqrt(bnorm);
@@ -383,11 +539,54 @@ __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 
 	int64_t iter = 0;
 	double *u_old = a.u0, *u_new = a.u1;
+	if (LIST) bcg_build_list(a, L, scan);
 	for (;;) {
 		++iter;
 		++epoch;
 		// phase A over the tiles of active instances
-		{
+		if constexpr (LIST) {
+			const int32_t ntot = L.off[L.n];
+			int j = 0, jn = 0;
+			int32_t seg = 0, segn = 0;
+			int32_t k = int32_t(gw);
+			int64_t t = k < ntot ? bcg_item_tile(a, L, k, j, seg) : nt;
+			WmMeta g = ROWS ? WmMeta{0, 0, -1, -1} : wm_meta(a.mt, t);
+			double gamma = k < ntot ? __ldcg(&a.inst[seg].gamma) : 0.0;
+			while (k < ntot) {
+				const int32_t kn = k + int32_t(nw);
+				jn = j;
+				const int64_t tn = kn < ntot ? bcg_item_tile(a, L, kn, jn, segn) : nt;
+				const WmMeta gn = ROWS ? WmMeta{0, 0, -1, -1} : wm_meta(a.mt, tn);
+				const double gamman = kn < ntot && segn != seg ? __ldcg(&a.inst[segn].gamma) : gamma;
+				double part;
+				if constexpr (ROWS) {
+					double acc = 0.0;
+					bcg_slice(a, t, lane,
+						[&](uint32_t j) { return __ldcg(a.r + j) + gamma * __ldcg(u_old + j); },
+						[&](int64_t i, double v) {
+							a.temp[i] = v;
+							const double un = __ldcg(a.r + i) + gamma * __ldcg(u_old + i);
+							u_new[i] = un;
+							acc += v * un;
+						});
+					part = warp_sum(acc);
+				} else {
+					BcgIter epi{&a, &sm[w], u_old, u_new, gamma};
+					BcgGather xl{a.r, u_old, gamma};
+					if (!warp_tile_ordered<RF>(t, g, a.mt, a.offsets, a.indices, a.values, xl, epi,
+							0, sm[w].tile, epoch, err))
+						break;
+					part = warp_sum(epi.acc);
+				}
+				if (lane == 0) a.own[t] = part;
+				k = kn;
+				j = jn;
+				seg = segn;
+				t = tn;
+				g = gn;
+				gamma = gamman;
+			}
+		} else {
 			int64_t t = gw;
 			BcgTileState cur = bcg_tile_state<false>(a, t);
 			WmMeta g = wm_meta(a.mt, t);
@@ -409,15 +608,102 @@ __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 			}
 		}
 		if (!grid_sync(a.gs)) return;
-		for (int64_t s = gw; s < a.nseg; s += nw) {
+		for (int64_t j = blockIdx.x; j < (LIST ? int64_t(L.n) : a.nseg); j += G) {
+			const int64_t s = LIST ? L.seg[j] : j;
 			BcgInst *in = a.inst + s;
-			if (__ldcg(&in->done)) continue;
-			const double beta = warp_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], lane);
-			if (lane == 0) in->alpha = in->sigma / beta;
+			if (!LIST && __ldcg(&in->done)) continue;
+			const double beta = block_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], red);
+			if (threadIdx.x == 0) in->alpha = in->sigma / beta;
 		}
 		if (!grid_sync(a.gs)) return;
 		// phase B: the rows that end in each active tile
-		{
+		if constexpr (ROWS) {
+			// one row per lane and slice: PB slices per step, their loads together
+			constexpr int PB = 4;
+			const int32_t ntot = L.off[L.n];
+			int j = 0;
+			for (int32_t k0 = int32_t(gw); k0 < ntot; k0 += PB * int32_t(nw)) {
+				int64_t tt[PB], ii[PB];
+				double al[PB], xv[PB], uv[PB], rv[PB], tv[PB];
+				bool ok[PB];
+#pragma unroll
+				for (int u = 0; u < PB; ++u) {
+					const int32_t k = k0 + u * int32_t(nw);
+					ok[u] = false;
+					tt[u] = 0;
+					if (k < ntot) {
+						int32_t sg;
+						tt[u] = bcg_item_tile(a, L, k, j, sg);
+						al[u] = __ldcg(&a.inst[sg].alpha);
+						ii[u] = __ldg(a.sl_row + tt[u]) + lane;
+						ok[u] = ii[u] < __ldg(a.sl_row + tt[u] + 1);
+					}
+				}
+#pragma unroll
+				for (int u = 0; u < PB; ++u) {
+					if (ok[u]) {
+						xv[u] = __ldcg(a.x + ii[u]);
+						uv[u] = __ldcg(u_new + ii[u]);
+						rv[u] = __ldcg(a.r + ii[u]);
+						tv[u] = __ldcg(a.temp + ii[u]);
+					}
+				}
+#pragma unroll
+				for (int u = 0; u < PB; ++u) {
+					double part = 0.0;
+					if (ok[u]) {
+						a.x[ii[u]] = xv[u] + al[u] * uv[u];
+						const double ri = rv[u] - al[u] * tv[u];
+						a.r[ii[u]] = ri;
+						part = ri * ri;
+					}
+					if (k0 + u * int32_t(nw) < ntot) {
+						part = warp_sum(part);
+						if (lane == 0) a.own[tt[u]] = part;
+					}
+				}
+			}
+		} else if constexpr (LIST) {
+			const int32_t ntot = L.off[L.n];
+			int j = 0;
+			int32_t seg = -1, sg = 0;
+			double alpha = 0.0;
+			for (int32_t k = int32_t(gw); k < ntot; k += int32_t(nw)) {
+				const int64_t t = bcg_item_tile(a, L, k, j, sg);
+				if (sg != seg) {
+					seg = sg;
+					alpha = __ldcg(&a.inst[seg].alpha);
+				}
+				double part = 0.0;
+				const int64_t r0 = ROWS ? a.sl_row[t] : a.mt.tile_row[t];
+				const int64_t r1 = ROWS ? a.sl_row[t + 1] : a.mt.tile_row[t + 1];
+				for (int64_t i0 = r0; i0 < r1; i0 += 32 * BCG_RB) {
+					double xv[BCG_RB], uv[BCG_RB], rv[BCG_RB], tv[BCG_RB];
+#pragma unroll
+					for (int q = 0; q < BCG_RB; ++q) {
+						const int64_t i = i0 + lane + 32 * q;
+						if (i < r1) {
+							xv[q] = __ldcg(a.x + i);
+							uv[q] = __ldcg(u_new + i);
+							rv[q] = __ldcg(a.r + i);
+							tv[q] = __ldcg(a.temp + i);
+						}
+					}
+#pragma unroll
+					for (int q = 0; q < BCG_RB; ++q) {
+						const int64_t i = i0 + lane + 32 * q;
+						if (i < r1) {
+							a.x[i] = xv[q] + alpha * uv[q];
+							const double ri = rv[q] - alpha * tv[q];
+							a.r[i] = ri;
+							part += ri * ri;
+						}
+					}
+				}
+				part = warp_sum(part);
+				if (lane == 0) a.own[t] = part;
+			}
+		} else {
 			int64_t t = gw;
 			BcgTileState cur = bcg_tile_state<true>(a, t);
 			while (t < nt) {
@@ -440,11 +726,12 @@ __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 			}
 		}
 		if (!grid_sync(a.gs)) return;
-		for (int64_t s = gw; s < a.nseg; s += nw) {
+		for (int64_t j = blockIdx.x; j < (LIST ? int64_t(L.n) : a.nseg); j += G) {
+			const int64_t s = LIST ? L.seg[j] : j;
 			BcgInst *in = a.inst + s;
-			if (__ldcg(&in->done)) continue;
-			const double rr = warp_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], lane);
-			if (lane == 0) {
+			if (!LIST && __ldcg(&in->done)) continue;
+			const double rr = block_sum_tiles(a.own, a.seg_tile[s], a.seg_tile[s + 1], red);
+			if (threadIdx.x == 0) {
 				in->rr = rr;
 				in->iterations = iter;
 				if (sqrt(rr) < in->tol_abs || iter >= a.max_iter) {
@@ -459,6 +746,7 @@ __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 		}
 		if (!grid_sync(a.gs)) return;
 		if (((volatile int32_t *) a.active)[0] == 0) break;
+		if (LIST) bcg_build_list(a, L, scan);
 		double *tmp = u_old;
 		u_old = u_new;
 		u_new = tmp;
@@ -468,6 +756,68 @@ __global__ void __launch_bounds__(32 * BCG_WARPS, 6) k_batched_cg(BcgArgs a) {
 } // namespace alpb
 
 using namespace alpb;
+
+// ------------------------------------------------ sliced storage (ELL-32) --
+// Slices of 32 rows, cut per instance (the last slice of an instance may be
+// short); a slice's width is its longest row.  Built once per handle from the
+// CRS: the solver then reads entry q of 32 rows as one coalesced line.
+__global__ void k_sell_slices(const int64_t *seg_rows, int64_t nseg, int64_t *count) {
+	for (int64_t s = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s <= nseg;
+		 s += int64_t(gridDim.x) * blockDim.x)
+		count[s] = s < nseg ? (seg_rows[s + 1] - seg_rows[s] + 31) / 32 : 0;
+}
+
+__global__ void k_sell_rows(const int64_t *seg_rows, const int64_t *seg_slice, int64_t nseg,
+	int64_t *sl_row, int64_t nslices) {
+	for (int64_t s = blockIdx.x; s < nseg; s += gridDim.x) {
+		const int64_t t0 = seg_slice[s], t1 = seg_slice[s + 1], r0 = seg_rows[s];
+		for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) sl_row[t] = r0 + 32 * (t - t0);
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) sl_row[nslices] = seg_rows[nseg];
+}
+
+// one warp per slice: row lengths and the slice's entry count (32 x width)
+__global__ void k_sell_width(const int64_t *offsets, const int64_t *sl_row, int64_t nslices,
+	uint8_t *len, int64_t *count) {
+	const int lane = threadIdx.x & 31;
+	const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	for (int64_t t = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; t <= nslices;
+		 t += nw) {
+		if (t == nslices) {
+			if (lane == 0) count[t] = 0;
+			continue;
+		}
+		const int64_t i = sl_row[t] + lane;
+		int l = 0;
+		if (i < sl_row[t + 1]) {
+			l = int(offsets[i + 1] - offsets[i]);
+			len[i] = uint8_t(l);
+		}
+		for (int o = 16; o > 0; o >>= 1) {
+			const int v = __shfl_xor_sync(0xffffffffu, l, o);
+			l = v > l ? v : l;
+		}
+		if (lane == 0) count[t] = 32 * int64_t(l);
+	}
+}
+
+__global__ void k_sell_fill(const int64_t *offsets, const uint32_t *indices, const double *values,
+	const int64_t *sl_row, const int64_t *sl_off, int64_t nslices, uint32_t *idx, double *val) {
+	const int lane = threadIdx.x & 31;
+	const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	for (int64_t t = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; t < nslices;
+		 t += nw) {
+		const int64_t i = sl_row[t] + lane, e0 = sl_off[t];
+		const int w = int((sl_off[t + 1] - e0) >> 5);
+		const bool own = i < sl_row[t + 1];
+		const int64_t kb = own ? offsets[i] : 0, l = own ? offsets[i + 1] - kb : 0;
+		for (int q = 0; q < w; ++q) {
+			const int64_t e = e0 + 32 * int64_t(q) + lane;
+			idx[e] = q < l ? indices[kb + q] : 0u;
+			val[e] = q < l ? values[kb + q] : 0.0;
+		}
+	}
+}
 
 struct alpb_batched_cg_s {
 	alpb_spmv_plan_s plan;
@@ -482,12 +832,66 @@ struct alpb_batched_cg_s {
 	int32_t *active = nullptr;
 	GridSync *gs = nullptr;
 	int grid = 0;
+	bool list = false;          // active-tile list (nseg <= BCG_LIST_MAX)
+	bool rows = false;          // sliced storage (rows of at most 32 nonzeroes)
+	int64_t nslices = 0;
+	int64_t *seg_slice = nullptr, *sl_row = nullptr, *sl_off = nullptr;
+	uint32_t *sl_idx = nullptr;
+	double *sl_val = nullptr;
+	uint8_t *sl_len = nullptr;
 	cudaGraphExec_t graph = nullptr;
 	const double *g_b = nullptr;
 	double *g_x = nullptr;
 	int64_t g_max = 0;
 	double g_tol = 0;
 };
+
+static int sell_build(alpb_batched_cg_s *h, const int64_t *seg_rows, cudaStream_t s) {
+	const int64_t nseg = h->nseg;
+	int64_t *cnt = nullptr;
+	void *tmp = nullptr;
+	size_t tb = 0;
+	ALPB_CUDA(cudaMalloc(&h->seg_slice, size_t(nseg + 1) * 8));
+	ALPB_CUDA(cudaMallocAsync(&cnt, size_t(nseg + 1) * 8, s));
+	k_sell_slices<<<grid_for(nseg + 1, 256), 256, 0, s>>>(seg_rows, nseg, cnt);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, h->seg_slice, nseg + 1, s));
+	ALPB_CUDA(cudaMallocAsync(&tmp, tb, s));
+	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, h->seg_slice, nseg + 1, s));
+	g_launches.fetch_add(1);
+	ALPB_CUDA(cudaMemcpyAsync(&h->nslices, h->seg_slice + nseg, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	ALPB_CUDA(cudaFreeAsync(cnt, s));
+	ALPB_CUDA(cudaFreeAsync(tmp, s));
+	const int64_t ns = h->nslices;
+	ALPB_CUDA(cudaMalloc(&h->sl_row, size_t(ns + 1) * 8));
+	ALPB_CUDA(cudaMalloc(&h->sl_off, size_t(ns + 1) * 8));
+	ALPB_CUDA(cudaMalloc(&h->sl_len, size_t(h->n > 0 ? h->n : 1)));
+	k_sell_rows<<<unsigned(nseg < 4096 ? nseg : 4096), 256, 0, s>>>(seg_rows, h->seg_slice, nseg,
+		h->sl_row, ns);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cudaMallocAsync(&cnt, size_t(ns + 1) * 8, s));
+	k_sell_width<<<grid_for((ns + 1) * 32, 256), 256, 0, s>>>(h->offsets, h->sl_row, ns, h->sl_len,
+		cnt);
+	ALPB_LAUNCHED();
+	tb = 0;
+	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, h->sl_off, ns + 1, s));
+	ALPB_CUDA(cudaMallocAsync(&tmp, tb, s));
+	ALPB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, h->sl_off, ns + 1, s));
+	g_launches.fetch_add(1);
+	int64_t ne = 0;
+	ALPB_CUDA(cudaMemcpyAsync(&ne, h->sl_off + ns, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	ALPB_CUDA(cudaFreeAsync(cnt, s));
+	ALPB_CUDA(cudaFreeAsync(tmp, s));
+	ALPB_CUDA(cudaMalloc(&h->sl_idx, size_t(ne > 0 ? ne : 1) * 4));
+	ALPB_CUDA(cudaMalloc(&h->sl_val, size_t(ne > 0 ? ne : 1) * 8));
+	k_sell_fill<<<grid_for(ns * 32, 256), 256, 0, s>>>(h->offsets, h->indices, h->values, h->sl_row,
+		h->sl_off, ns, h->sl_idx, h->sl_val);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	return ALPB_SUCCESS;
+}
 
 __global__ void k_bcg_reset(GridSync *gs, int32_t *active, int32_t nseg) {
 	gs->count = 0;
@@ -498,7 +902,8 @@ __global__ void k_bcg_reset(GridSync *gs, int32_t *active, int32_t nseg) {
 
 static int bcg_launch(alpb_batched_cg_s *h, const double *b, double *x, int64_t max_iter,
 	double tol, cudaStream_t s) {
-	const int64_t nt = h->plan.ntiles;
+	// per-tile partials: as many as tiles or slices, whichever the solve uses
+	const int64_t nt = h->plan.ntiles > h->nslices ? h->plan.ntiles : h->nslices;
 	// kernels only (no host-memory copies), so the solve can be captured
 	k_bcg_reset<<<1, 1, 0, s>>>(h->gs, h->active, int32_t(h->nseg));
 	ALPB_LAUNCHED();
@@ -518,6 +923,15 @@ static int bcg_launch(alpb_batched_cg_s *h, const double *b, double *x, int64_t 
 	a.own2 = h->scratch + nt;
 	a.tile_seg = h->st.tile_seg;
 	a.seg_tile = h->st.seg_tile;
+	a.sl_row = h->sl_row;
+	a.sl_off = h->sl_off;
+	a.sl_idx = h->sl_idx;
+	a.sl_val = h->sl_val;
+	a.sl_len = h->sl_len;
+	if (h->rows) {   // the slices are the tiles
+		a.seg_tile = h->seg_slice;
+		a.mt.ntiles = h->nslices;
+	}
 	a.inst = h->inst;
 	a.nseg = h->nseg;
 	a.max_iter = max_iter;
@@ -533,7 +947,13 @@ static int bcg_launch(alpb_batched_cg_s *h, const double *b, double *x, int64_t 
 	attr[0].val.cooperative = 1;
 	cfg.attrs = attr;
 	cfg.numAttrs = 1;
-	ALPB_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg, a));
+	if (h->rows) {
+		ALPB_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg<true, true>, a));
+	} else if (h->list) {
+		ALPB_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg<true, false>, a));
+	} else {
+		ALPB_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg<false, false>, a));
+	}
 	ALPB_LAUNCHED();
 	return ALPB_SUCCESS;
 }
@@ -565,8 +985,23 @@ int alpb_batched_cg_create(alpb_batched_cg *out, int64_t n, int64_t nnz, const i
 		alpb_batched_cg_destroy(h);
 		return rc;
 	}
-	const int64_t nt = h->plan.ntiles;
-	h->grid = solver_grid(k_batched_cg, 32 * BCG_WARPS, nt, BCG_WARPS);
+	int64_t nt = h->plan.ntiles;
+	h->list = nseg <= BCG_LIST_MAX && nt < (int64_t(1) << 31);
+	if (h->list && h->st.tile_d) {   // whole-row tiles: rows of at most 32 nonzeroes
+		rc = sell_build(h, seg_rows, s);
+		if (rc != ALPB_SUCCESS) {
+			alpb_batched_cg_destroy(h);
+			return rc;
+		}
+		h->rows = h->nslices < (int64_t(1) << 31);
+		if (h->nslices > nt) nt = h->nslices;
+	}
+	if (h->rows)
+		h->grid = solver_grid(k_batched_cg<true, true>, 32 * BCG_WARPS, h->nslices, BCG_WARPS);
+	else if (h->list)
+		h->grid = solver_grid(k_batched_cg<true, false>, 32 * BCG_WARPS, nt, BCG_WARPS);
+	else
+		h->grid = solver_grid(k_batched_cg<false, false>, 32 * BCG_WARPS, nt, BCG_WARPS);
 	if (h->grid <= 0) {
 		alpb_batched_cg_destroy(h);
 		set_error("alpb_batched_cg_create: no cooperative occupancy");
@@ -591,6 +1026,12 @@ int alpb_batched_cg_destroy(alpb_batched_cg h) {
 	if (!h) return ALPB_SUCCESS;
 	if (h->graph) cudaGraphExecDestroy(h->graph);
 	segmented_free(&h->st);
+	cudaFree(h->seg_slice);
+	cudaFree(h->sl_row);
+	cudaFree(h->sl_off);
+	cudaFree(h->sl_idx);
+	cudaFree(h->sl_val);
+	cudaFree(h->sl_len);
 	cudaFree(h->plan.tile_row);
 	cudaFree(h->plan.head_first);
 	cudaFree(h->plan.tail_first);
