@@ -2,14 +2,20 @@
 // solved together in ONE persistent cooperative launch.
 //
 // The instances are stored as one block-diagonal CRS (instance i owns rows
-// [seg_rows[i], seg_rows[i+1])).  Warp tiles are cut per instance
-// (merge_plan_segmented; whole-row tiles when the rows are short), so every
-// tile belongs to exactly one instance and every instance scalar (beta,
-// alpha, r.r, gamma, sigma) is a sum over that instance's tiles.  An
-// iteration is the single-system solver's two phases (cg.cu), each followed
-// by a per-instance reduction of the tile partials (one warp per instance,
-// fixed order: deterministic), with a grid barrier after each of the four
-// steps.  An instance that converges (its own relative tolerance, as
+// [seg_rows[i], seg_rows[i+1])).  Tiles are cut per instance, so every tile
+// belongs to exactly one instance and every instance scalar (beta, alpha,
+// r.r, gamma, sigma) is a sum over that instance's tiles.  Two tilings:
+//   - systems whose rows hold at most 32 nonzeroes get a sliced copy of the
+//     matrix (ELL-32 per instance: entry q of 32 consecutive rows is one
+//     contiguous line), and a tile is a slice computed one row per lane;
+//   - other systems use warp tiles of the merge-path engine
+//     (merge_plan_segmented), rows crossing tiles handled by ordered waits.
+// An iteration is the single-system solver's two phases (cg.cu), each
+// followed by a per-instance reduction of the tile partials (one block per
+// instance, fixed order: deterministic), with a grid barrier after each of
+// the four steps.  Warps walk only the tiles of the instances still
+// iterating (a list every block rebuilds after each convergence step).  An
+// instance that converges (its own relative tolerance, as
 // algorithms::conjugate_gradient tests it, conjugate_gradient.hpp:377-378,
 // :437) or exhausts the iteration budget is masked out; the launch ends when
 // no instance is active.
