@@ -453,6 +453,16 @@ static int default_width(double mean) {
 	return w;
 }
 
+// Lanes per row for regular rows: about a sixth of the mean row length, so a
+// warp spans several rows (measured on B200: 2 lanes for the 5-point
+// Poisson rows, 4 for the 27-point stencil, each ~1.2-2.5x faster than one
+// lane per 1-2 nonzeroes or the merge path).
+static int regular_width(double mean) {
+	int w = 2;
+	while (w < 32 && w * 2 <= mean / 6) w *= 2;
+	return w;
+}
+
 template <class R>
 int run_spmv(const SpmvArgs &a, const alpb_spmv_plan_s *p, int force_sched, cudaStream_t s) {
 	if (a.trivial) {
@@ -588,18 +598,16 @@ int alpb::plan_create_tiles(alpb_spmv_plan_s **plan, int64_t m, int64_t nnz,
 		alpb_spmv_plan_destroy(p);
 		return rc;
 	}
+	// profile heuristic: regular rows -> vector, skewed rows -> merge path
+	const bool regular = p->cv < 0.5 && p->maxlen <= 4.0 * p->mean + 32;
 	if (vector_width > 0) {
 		int w = 1;
 		while (w < vector_width && w < 32) w *= 2;
 		p->vw = w;
 	} else {
-		p->vw = default_width(p->mean);
+		p->vw = regular ? regular_width(p->mean) : default_width(p->mean);
 	}
-	if (sched == ALPB_SCHED_AUTO) {
-		// profile heuristic: regular rows -> vector, skewed rows -> merge path
-		sched = (p->cv < 0.5 && p->maxlen <= 4.0 * p->mean + 32) ? ALPB_SCHED_VECTOR
-																	 : ALPB_SCHED_MERGE_PATH;
-	}
+	if (sched == ALPB_SCHED_AUTO) sched = regular ? ALPB_SCHED_VECTOR : ALPB_SCHED_MERGE_PATH;
 	p->sched = sched;
 	*plan = p;
 	return ALPB_SUCCESS;
