@@ -55,15 +55,24 @@ constexpr int HP_FIN_THREADS = 256;
 // nonzeroes [beg[c], beg[c+1]) of row row[c]; every row has at least one
 // chunk (possibly empty).  slot[c] >= 0 names the partial of a chunk of a row
 // of several chunks (the slots of one row are consecutive); multi lists those
-// rows with their first slot and chunk count.
+// rows with their first slot and chunk count.  A row of more than HP_GROUP
+// chunks (a power-law hub) has its slots summed in groups of HP_GROUP first
+// (one warp per group), so no warp sums thousands of partials alone: mgroup
+// names the row's first group (-1 without groups), group g covers slots
+// [gslot[g], gslot[g] + glen[g]).
+constexpr int HP_GROUP_CHUNKS = 32;
+
 struct HpChunks {
-	int64_t nchunks = 0, nmulti = 0, nslots = 0;
+	int64_t nchunks = 0, nmulti = 0, nslots = 0, ngroups = 0;
 	int64_t *beg = nullptr;       // [nchunks + 1]
 	uint32_t *row = nullptr;      // [nchunks]
 	int32_t *slot = nullptr;      // [nchunks]
 	uint32_t *mrow = nullptr;     // [nmulti]
 	int32_t *mslot = nullptr;     // [nmulti]
 	int32_t *mcount = nullptr;    // [nmulti]
+	int32_t *mgroup = nullptr;    // [nmulti]
+	int32_t *gslot = nullptr;     // [ngroups]
+	int32_t *glen = nullptr;      // [ngroups]
 };
 
 static void chunks_free(HpChunks *c) {
@@ -73,16 +82,20 @@ static void chunks_free(HpChunks *c) {
 	cudaFree(c->mrow);
 	cudaFree(c->mslot);
 	cudaFree(c->mcount);
+	cudaFree(c->mgroup);
+	cudaFree(c->gslot);
+	cudaFree(c->glen);
 	*c = HpChunks{};
 }
 
-// per row: chunk count, and the slot count and multi flag of rows of several
+// per row: chunk count, slot count and multi flag of rows of several chunks,
+// group count of rows of more than HP_GROUP_CHUNKS chunks
 __global__ void k_hp_count(const int64_t *offsets, int64_t n, int64_t *nch, int64_t *nsl,
-	int64_t *nmu) {
+	int64_t *nmu, int64_t *ngr) {
 	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i <= n;
 		 i += int64_t(gridDim.x) * blockDim.x) {
 		if (i == n) {
-			nch[i] = nsl[i] = nmu[i] = 0;
+			nch[i] = nsl[i] = nmu[i] = ngr[i] = 0;
 			continue;
 		}
 		const int64_t len = offsets[i + 1] - offsets[i];
@@ -91,11 +104,12 @@ __global__ void k_hp_count(const int64_t *offsets, int64_t n, int64_t *nch, int6
 		nch[i] = c;
 		nsl[i] = c > 1 ? c : 0;
 		nmu[i] = c > 1 ? 1 : 0;
+		ngr[i] = c > HP_GROUP_CHUNKS ? (c + HP_GROUP_CHUNKS - 1) / HP_GROUP_CHUNKS : 0;
 	}
 }
 
 __global__ void k_hp_fill(const int64_t *offsets, int64_t n, const int64_t *first,
-	const int64_t *slot0, const int64_t *mpos, HpChunks t) {
+	const int64_t *slot0, const int64_t *mpos, const int64_t *gfirst, HpChunks t) {
 	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
 		 i += int64_t(gridDim.x) * blockDim.x) {
 		const int64_t c0 = first[i], c1 = first[i + 1];
@@ -110,6 +124,14 @@ __global__ void k_hp_fill(const int64_t *offsets, int64_t n, const int64_t *firs
 			t.mrow[p] = uint32_t(i);
 			t.mslot[p] = int32_t(slot0[i]);
 			t.mcount[p] = int32_t(c1 - c0);
+			const int64_t g0 = gfirst[i], g1 = gfirst[i + 1];
+			t.mgroup[p] = g1 > g0 ? int32_t(g0) : -1;
+			for (int64_t g = g0; g < g1; ++g) {
+				const int64_t k0 = (g - g0) * HP_GROUP_CHUNKS;
+				const int64_t k1 = k0 + HP_GROUP_CHUNKS < c1 - c0 ? k0 + HP_GROUP_CHUNKS : c1 - c0;
+				t.gslot[g] = int32_t(slot0[i] + k0);
+				t.glen[g] = int32_t(k1 - k0);
+			}
 		}
 		if (i == n - 1) t.beg[c1] = offsets[n];
 	}
@@ -128,37 +150,44 @@ static int exclusive_scan(const T *in, T *out, int64_t count, cudaStream_t s) {
 }
 
 static int chunks_build(HpChunks *t, const int64_t *offsets, int64_t n, cudaStream_t s) {
-	int64_t *buf = nullptr;   // nch, nsl, nmu and their scans: 6 x (n + 1)
-	ALPB_CUDA(cudaMallocAsync(&buf, size_t(6) * (n + 1) * 8, s));
-	int64_t *nch = buf, *nsl = buf + (n + 1), *nmu = buf + 2 * (n + 1);
-	int64_t *first = buf + 3 * (n + 1), *slot0 = buf + 4 * (n + 1), *mpos = buf + 5 * (n + 1);
-	k_hp_count<<<grid_for(n + 1, 256), 256, 0, s>>>(offsets, n, nch, nsl, nmu);
+	int64_t *buf = nullptr;   // nch, nsl, nmu, ngr and their scans: 8 x (n + 1)
+	ALPB_CUDA(cudaMallocAsync(&buf, size_t(8) * (n + 1) * 8, s));
+	int64_t *nch = buf, *nsl = buf + (n + 1), *nmu = buf + 2 * (n + 1), *ngr = buf + 3 * (n + 1);
+	int64_t *first = buf + 4 * (n + 1), *slot0 = buf + 5 * (n + 1), *mpos = buf + 6 * (n + 1);
+	int64_t *gfirst = buf + 7 * (n + 1);
+	k_hp_count<<<grid_for(n + 1, 256), 256, 0, s>>>(offsets, n, nch, nsl, nmu, ngr);
 	ALPB_LAUNCHED();
 	int rc = exclusive_scan(nch, first, n + 1, s);
 	rc = rc ? rc : exclusive_scan(nsl, slot0, n + 1, s);
 	rc = rc ? rc : exclusive_scan(nmu, mpos, n + 1, s);
+	rc = rc ? rc : exclusive_scan(ngr, gfirst, n + 1, s);
 	if (rc) return rc;
-	int64_t tot[3];
+	int64_t tot[4];
 	ALPB_CUDA(cudaMemcpyAsync(&tot[0], first + n, 8, cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaMemcpyAsync(&tot[1], slot0 + n, 8, cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaMemcpyAsync(&tot[2], mpos + n, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaMemcpyAsync(&tot[3], gfirst + n, 8, cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
 	t->nchunks = tot[0];
 	t->nslots = tot[1];
 	t->nmulti = tot[2];
+	t->ngroups = tot[3];
 	ALPB_CHECK(t->nslots < (int64_t(1) << 31), ALPB_OVERFLW, "ppr: too many chunk partials");
 	if (cudaMalloc(&t->beg, size_t(t->nchunks + 1) * 8) != cudaSuccess ||
 		cudaMalloc(&t->row, size_t(t->nchunks) * 4) != cudaSuccess ||
 		cudaMalloc(&t->slot, size_t(t->nchunks) * 4) != cudaSuccess ||
 		cudaMalloc(&t->mrow, size_t(t->nmulti + 1) * 4) != cudaSuccess ||
 		cudaMalloc(&t->mslot, size_t(t->nmulti + 1) * 4) != cudaSuccess ||
-		cudaMalloc(&t->mcount, size_t(t->nmulti + 1) * 4) != cudaSuccess) {
+		cudaMalloc(&t->mcount, size_t(t->nmulti + 1) * 4) != cudaSuccess ||
+		cudaMalloc(&t->mgroup, size_t(t->nmulti + 1) * 4) != cudaSuccess ||
+		cudaMalloc(&t->gslot, size_t(t->ngroups + 1) * 4) != cudaSuccess ||
+		cudaMalloc(&t->glen, size_t(t->ngroups + 1) * 4) != cudaSuccess) {
 		cudaGetLastError();
 		cudaFreeAsync(buf, s);
 		set_error("ppr: out of device memory for the chunk tables");
 		return ALPB_OUTOFMEM;
 	}
-	k_hp_fill<<<grid_for(n, 256), 256, 0, s>>>(offsets, n, first, slot0, mpos, *t);
+	k_hp_fill<<<grid_for(n, 256), 256, 0, s>>>(offsets, n, first, slot0, mpos, gfirst, *t);
 	ALPB_LAUNCHED();
 	ALPB_CUDA(cudaFreeAsync(buf, s));
 	return ALPB_SUCCESS;
@@ -185,8 +214,11 @@ struct HpArgs {
 	const int32_t *cslot;
 	int64_t nchunks;
 	const uint32_t *mrow;
-	const int32_t *mslot, *mcount;
+	const int32_t *mslot, *mcount, *mgroup;
 	int64_t nmulti;
+	const int32_t *gslot, *glen;
+	int64_t ngroups;
+	double *gpart;      // [ngroups][S] group partials of hub rows
 	const uint32_t *idx;
 	const double *val;
 	// vectors (n x S)
@@ -439,8 +471,36 @@ __global__ void __launch_bounds__(32 * HP_WARPS, ALPB_HP_MINB) k_hp_chunks(HpArg
 	if (MODE != HP_MU) hp_block_partials(a, L, res, dng, blockIdx.x, red);
 }
 
-// Rows of several chunks: one warp per row sums its chunk partials in chunk
-// order and runs the row epilogue.  Block partials go after the main kernel's
+// Groups of HP_GROUP_CHUNKS consecutive chunk partials of a hub row: one warp
+// per group sums them in chunk order (all the group's loads issued first).
+template <int G, int SPL>
+__global__ void __launch_bounds__(32 * HP_WARPS) k_hp_group(HpArgs a) {
+	const HpLanes<G, SPL> L;
+	const int S = a.S;
+	const int64_t nw = int64_t(gridDim.x) * HP_WARPS;
+	for (int64_t g = int64_t(blockIdx.x) * HP_WARPS + (threadIdx.x >> 5); g < a.ngroups; g += nw) {
+		const int64_t s0 = __ldg(a.gslot + g);
+		const int len = __ldg(a.glen + g);
+		if (!L.lead()) continue;
+#pragma unroll
+		for (int q = 0; q < SPL; ++q) {
+			const int s = L.seed(q);
+			if (s >= S) continue;
+			double v[HP_GROUP_CHUNKS];
+#pragma unroll
+			for (int k = 0; k < HP_GROUP_CHUNKS; ++k)
+				v[k] = k < len ? __ldcg(a.part + (s0 + k) * S + s) : 0.0;
+			double acc = 0.0;
+#pragma unroll
+			for (int k = 0; k < HP_GROUP_CHUNKS; ++k)
+				if (k < len) acc += v[k];
+			__stcg(a.gpart + g * S + s, acc);
+		}
+	}
+}
+
+// Rows of several chunks: one warp per row sums its chunk partials (or, for
+// a hub row, its group partials) in order and runs the row epilogue.  Block partials go after the main kernel's
 // (block index offset bp_base).
 template <int MODE, int G, int SPL>
 __global__ void __launch_bounds__(32 * HP_WARPS) k_hp_multi(HpArgs a, int64_t bp_base) {
@@ -458,8 +518,11 @@ __global__ void __launch_bounds__(32 * HP_WARPS) k_hp_multi(HpArgs a, int64_t bp
 	const int64_t nw = int64_t(gridDim.x) * HP_WARPS;
 	for (int64_t m = int64_t(blockIdx.x) * HP_WARPS + (threadIdx.x >> 5); m < a.nmulti; m += nw) {
 		const int64_t r = __ldg(a.mrow + m);
-		const int64_t s0 = __ldg(a.mslot + m);
-		const int cnt = __ldg(a.mcount + m);
+		const int32_t g0 = __ldg(a.mgroup + m);
+		const int mc = __ldg(a.mcount + m);
+		// partials to sum: the row's groups, else its chunk slots
+		const double *src = g0 >= 0 ? a.gpart + int64_t(g0) * S : a.part + int64_t(__ldg(a.mslot + m)) * S;
+		const int cnt = g0 >= 0 ? (mc + HP_GROUP_CHUNKS - 1) / HP_GROUP_CHUNKS : mc;
 		HpEpiIn<SPL> e;
 		hp_epi_load<MODE>(a, L, r, e);
 		double acc[SPL];
@@ -468,7 +531,7 @@ __global__ void __launch_bounds__(32 * HP_WARPS) k_hp_multi(HpArgs a, int64_t bp
 		if (L.lead()) {
 #pragma unroll 4
 			for (int k = 0; k < cnt; ++k) {
-				const double *p = a.part + (s0 + k) * S;
+				const double *p = src + int64_t(k) * S;
 #pragma unroll
 				for (int q = 0; q < SPL; ++q) {
 					const int s = L.seed(q);
@@ -694,7 +757,7 @@ struct alpb_ppr_s {
 	double *deg = nullptr, *inv_d = nullptr, *rs = nullptr, *c = nullptr;
 	HpChunks crs, ccs;
 	double *y[2] = {nullptr, nullptr};
-	double *part = nullptr, *bp = nullptr;
+	double *part = nullptr, *bp = nullptr, *gpart = nullptr;
 	int64_t *seed = nullptr, *iters = nullptr;
 	double *term = nullptr, *res = nullptr;
 	int32_t *active = nullptr, *n_active = nullptr, *h_active = nullptr;
@@ -719,7 +782,12 @@ HpArgs args_over(alpb_ppr h, bool ccs) {
 	a.mrow = t.mrow;
 	a.mslot = t.mslot;
 	a.mcount = t.mcount;
+	a.mgroup = t.mgroup;
 	a.nmulti = t.nmulti;
+	a.gslot = t.gslot;
+	a.glen = t.glen;
+	a.ngroups = t.ngroups;
+	a.gpart = h->gpart;
 	a.idx = ccs ? h->ccs_idx : h->crs_idx;
 	a.val = ccs ? h->ccs_w : h->w;
 	a.part = h->part;
@@ -738,6 +806,10 @@ int hp_launch(const HpArgs &a, cudaStream_t s, int64_t *nblocks) {
 	k_hp_chunks<MODE, G, SPL><<<gm, 32 * HP_WARPS, 0, s>>>(a);
 	ALPB_LAUNCHED();
 	int64_t nb = gm;
+	if (a.ngroups > 0) {
+		k_hp_group<G, SPL><<<grid_for(a.ngroups * 32, 32 * HP_WARPS), 32 * HP_WARPS, 0, s>>>(a);
+		ALPB_LAUNCHED();
+	}
 	if (a.nmulti > 0) {
 		const unsigned gx = grid_for(a.nmulti * 32, 32 * HP_WARPS);
 		k_hp_multi<MODE, G, SPL><<<gx, 32 * HP_WARPS, 0, s>>>(a, gm);
@@ -848,6 +920,7 @@ int alpb_ppr_destroy(alpb_ppr h) {
 	cudaFree(h->y[0]);
 	cudaFree(h->y[1]);
 	cudaFree(h->part);
+	cudaFree(h->gpart);
 	cudaFree(h->bp);
 	cudaFree(h->seed);
 	cudaFree(h->iters);
@@ -927,7 +1000,9 @@ int alpb_ppr_create(alpb_ppr *out, int64_t n, int64_t nnz, const int64_t *row_pt
 	rc = rc ? rc : chunks_build(&h->ccs, h->ccs_ptr, n, s);
 	if (rc == ALPB_SUCCESS) {
 		const int64_t slots = h->crs.nslots > h->ccs.nslots ? h->crs.nslots : h->ccs.nslots;
-		if (cudaMalloc(&h->part, size_t(slots > 0 ? slots : 1) * nseeds * 8) != cudaSuccess) {
+		const int64_t groups = h->crs.ngroups > h->ccs.ngroups ? h->crs.ngroups : h->ccs.ngroups;
+		if (cudaMalloc(&h->part, size_t(slots > 0 ? slots : 1) * nseeds * 8) != cudaSuccess ||
+			cudaMalloc(&h->gpart, size_t(groups > 0 ? groups : 1) * nseeds * 8) != cudaSuccess) {
 			cudaGetLastError();
 			set_error("alpb_ppr_create: out of device memory");
 			rc = ALPB_OUTOFMEM;

@@ -13,6 +13,7 @@ e2e     the same metric through the C-ABI with host buffers: each step copies
         x from pinned host memory, runs alpb_mxv, copies u back.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --only batched_cg|hpcg|adjoint_cg|ppr [size options]   (one workload)
 
 --impl reference runs the unmodified ALP reference_omp backend (compiled
 from the reference sources into oracle/_ref) on the host cores, on the same
@@ -668,6 +669,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale (22 is the benchmark; smaller for profiling captures)")
+    ap.add_argument("--only", choices=["batched_cg", "hpcg", "adjoint_cg", "ppr"],
+                    help="run one secondary workload alone and print its line (profiling)")
+    ap.add_argument("--hpcg-side", type=int, default=256)
+    ap.add_argument("--hpcg-levels", type=int, default=3)
+    ap.add_argument("--ppr-scale", type=int, default=24)
+    ap.add_argument("--ppr-seeds", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -677,6 +684,20 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(reference_arm(args)), flush=True)
+        return
+
+    if args.only:
+        import torch
+        from alp_b200 import _abi as abi
+        torch.cuda.set_device(local_rank)
+        abi.call("alpb_init", local_rank)
+        stream = torch.cuda.current_stream()
+        run = {"batched_cg": lambda: batched_cg_workload(stream),
+               "hpcg": lambda: hpcg_workload(stream, args.hpcg_side, args.hpcg_levels),
+               "adjoint_cg": lambda: adjoint_workload(stream),
+               "ppr": lambda: ppr_workload(stream, args.ppr_scale, args.ppr_seeds)}[args.only]
+        if rank == 0:
+            print(json.dumps({"workload": args.only, **run()}), flush=True)
         return
 
     if world > 1:
