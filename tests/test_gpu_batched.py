@@ -109,3 +109,76 @@ def test_batched_cg_budget_masks_instances(cuda):
     assert rc == abi.FAILED
     assert conv[0] == 1 and conv[2] == 1 and conv[1] == 0
     assert it[1] == 40 and it[0] < 40
+
+
+def host_block_diagonal(blocks):
+    """Block-diagonal CRS from a list of dense SPD blocks (numpy)."""
+    rp, col, val, seg = [0], [], [], [0]
+    base = 0
+    for Bk in blocks:
+        m = Bk.shape[0]
+        for r in range(m):
+            nz = np.flatnonzero(Bk[r])
+            col.extend((nz + base).tolist())
+            val.extend(Bk[r, nz].tolist())
+            rp.append(len(col))
+        base += m
+        seg.append(base)
+    return (np.asarray(rp, np.int64), np.asarray(col, np.uint32), np.asarray(val),
+            np.asarray(seg, np.int64))
+
+
+def check_against_restatement(oracle, rp, col, val, seg, hb, hx, it, sample):
+    for s in sample:
+        r0, r1 = int(seg[s]), int(seg[s + 1])
+        srp = rp[r0:r1 + 1] - rp[r0]
+        scol = (col[rp[r0]:rp[r1]].astype(np.int64) - r0).astype(np.uint32)
+        sval = val[rp[r0]:rp[r1]]
+        rc2, x2, it2, _ = oracle.cg(srp, scol, sval, hb[r0:r1], np.zeros(r1 - r0), 2000, 1e-8)
+        assert rc2 == 0
+        assert abs(int(it[s]) - it2) <= 1, (s, it[s], it2)
+        np.testing.assert_allclose(hx[r0:r1], x2, rtol=0, atol=1e-9 * max(1.0, np.abs(x2).max()))
+
+
+def test_batched_cg_long_rows_merge_tiles(cuda, oracle):
+    """Rows of more than 32 nonzeroes: the solver keeps the merge engine's warp
+    tiles (rows crossing tiles, ordered waits) instead of the sliced storage."""
+    import torch
+    from alp_b200 import device as dev
+    rng = np.random.default_rng(21)
+    blocks = []
+    for m in rng.integers(40, 220, 12):
+        band = 24
+        Bk = np.zeros((m, m))
+        for r in range(m):
+            for c in range(max(0, r - band), min(m, r + band + 1)):
+                if c != r:
+                    Bk[r, c] = -rng.uniform(0.1, 1.0) if c > r else 0.0
+        Bk = Bk + Bk.T
+        np.fill_diagonal(Bk, np.abs(Bk).sum(1) * 1.05 + rng.uniform(0.01, 0.5, m))
+        blocks.append(Bk)
+    rp, col, val, seg = host_block_diagonal(blocks)
+    assert np.diff(rp).max() > 32
+    A = dev.from_host(int(seg[-1]), int(seg[-1]), rp, col, val)
+    hb = rng.standard_normal(int(seg[-1]))
+    b = torch.from_numpy(hb).cuda()
+    tR = torch.from_numpy(seg).cuda()
+    rc, x, it, res, conv = batched_solve(A, b, tR, len(blocks), 2000, 1e-8)
+    assert rc == 0 and conv.all()
+    check_against_restatement(oracle, rp, col, val, seg, hb, x.cpu().numpy(), it,
+                              range(len(blocks)))
+
+
+def test_batched_cg_many_instances_tile_walk(cuda, oracle):
+    """More instances than the active list holds (1024): the solver walks all
+    tiles and skips converged instances."""
+    rng = np.random.default_rng(5)
+    nseg = 1100
+    sides = rng.integers(3, 9, nseg)
+    shifts = rng.uniform(0.05, 1.0, nseg)
+    A, b, tR, seg_rows = make_batch(sides, shifts)
+    rc, x, it, res, conv = batched_solve(A, b, tR, nseg, 2000, 1e-8)
+    assert rc == 0 and conv.all()
+    o, i, v = A.to_host()
+    check_against_restatement(oracle, o, i, v, seg_rows, b.cpu().numpy(), x.cpu().numpy(), it,
+                              list(range(0, nseg, 37)) + [nseg - 1])

@@ -326,3 +326,40 @@ def test_autograd_shim(cuda, oracle):
     P.close()
     np.testing.assert_allclose(wt.grad.cpu().numpy(), gro, rtol=1e-8,
                                atol=1e-8 * np.abs(gro).max())
+
+
+def test_hub_rows_summed_in_groups(cuda):
+    """A hub with ~3000 out-edges and ~3000 in-edges: its rows span more than
+    32 x 32 nonzeroes in both storages, so their chunk partials are summed in
+    groups before the row sum."""
+    import torch
+    rng = np.random.default_rng(17)
+    n = 3072
+    I = [0] * (n - 1) + list(range(1, n)) + rng.integers(0, n, 5 * n).tolist()
+    J = list(range(1, n)) + [0] * (n - 1) + rng.integers(0, n, 5 * n).tolist()
+    keys = np.unique(np.asarray(I, np.int64) * n + np.asarray(J, np.int64))
+    rows, cols = keys // n, keys % n
+    rp = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int64)
+    w = rng.uniform(0.5, 1.5, len(cols))
+    assert np.diff(rp).max() > 32 * 32 and np.bincount(cols, minlength=n).max() > 32 * 32
+    S = 8
+    seeds = np.concatenate([[0], rng.integers(1, n, S - 1)])
+    # a fixed number of iterations (tolerance 0): the grouped sums round
+    # differently from the restatement's sequential ones, which can move a
+    # residual that sits at the tolerance across it
+    P = Ppr(rp, cols, w, S)
+    x, it, _ = P.solve(seeds, conv=0.0, max_iter=300)
+    xo, ito, _ = O.forward(rp, cols, w, seeds, conv=0.0, max_iter=300)
+    np.testing.assert_array_equal(it, ito)
+    xh = host(x, n, S)
+    np.testing.assert_allclose(xh, xo, rtol=1e-11, atol=1e-11 * np.abs(xo).max())
+    g = rng.standard_normal((n, S))
+    lam, ita, _ = P.adjoint(torch.from_numpy(g.reshape(-1)).cuda(), conv=0.0, max_iter=300)
+    lo, itao, _ = O.adjoint(rp, cols, w, seeds, g, conv=0.0, max_iter=300)
+    np.testing.assert_array_equal(ita, itao)
+    lh = host(lam, n, S)
+    np.testing.assert_allclose(lh, lo, rtol=1e-11, atol=1e-11 * np.abs(lo).max())
+    gr = P.grad(x, lam)
+    gro = O.grad_weights(rp, cols, w, xh, lh)
+    P.close()
+    np.testing.assert_allclose(gr, gro, rtol=1e-9, atol=1e-9 * np.abs(gro).max())
