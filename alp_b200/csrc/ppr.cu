@@ -161,7 +161,10 @@ static int chunks_build(HpChunks *t, const int64_t *offsets, int64_t n, cudaStre
 	rc = rc ? rc : exclusive_scan(nsl, slot0, n + 1, s);
 	rc = rc ? rc : exclusive_scan(nmu, mpos, n + 1, s);
 	rc = rc ? rc : exclusive_scan(ngr, gfirst, n + 1, s);
-	if (rc) return rc;
+	if (rc) {
+		cudaFreeAsync(buf, s);
+		return rc;
+	}
 	int64_t tot[4];
 	ALPB_CUDA(cudaMemcpyAsync(&tot[0], first + n, 8, cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaMemcpyAsync(&tot[1], slot0 + n, 8, cudaMemcpyDeviceToHost, s));
@@ -1020,8 +1023,16 @@ int alpb_ppr_create(alpb_ppr *out, int64_t n, int64_t nnz, const int64_t *row_pt
 int alpb_ppr_set_weights(alpb_ppr h, const double *weights, void *stream) {
 	ALPB_CHECK(h != nullptr, ALPB_ILLEGAL, "alpb_ppr_set_weights: null handle");
 	ALPB_CHECK(weights || h->nnz == 0, ALPB_ILLEGAL, "alpb_ppr_set_weights: null weights");
+	const double *old = h->w;
 	h->w = weights;
-	return hp_weights(h, as_stream(stream));
+	const int rc = hp_weights(h, as_stream(stream));
+	if (rc == ALPB_ILLEGAL) {   // rejected weights: keep the previous ones
+		h->w = old;
+		const int rc2 = hp_weights(h, as_stream(stream));
+		if (rc2 != ALPB_SUCCESS) return rc2;
+		set_error("ppr: edge weights must be finite and non-negative");
+	}
+	return rc;
 }
 
 int alpb_ppr_solve(alpb_ppr h, const int64_t *seeds, double alpha, double conv, int64_t max_iter,

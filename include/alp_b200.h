@@ -479,7 +479,9 @@ typedef struct alpb_ppr_s *alpb_ppr;
 ALPB_API int alpb_ppr_create(alpb_ppr *h, int64_t n, int64_t nnz, const int64_t *row_ptr,
 	const uint32_t *col_idx, const double *weights, int nseeds, void *stream);
 ALPB_API int alpb_ppr_destroy(alpb_ppr h);
-/* New weights on the same pattern (held by reference, like the create call's). */
+/* New weights on the same pattern (held by reference, like the create call's).
+ * ALPB_ILLEGAL when a weight is negative or not finite; the handle then keeps
+ * its previous weights. */
 ALPB_API int alpb_ppr_set_weights(alpb_ppr h, const double *weights, void *stream);
 /* seeds: host array of nseeds rows.  x (device, n x nseeds) holds the initial
  * guesses if init_given != 0, else starts at 1/n.  iterations and residuals:

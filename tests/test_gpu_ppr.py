@@ -271,11 +271,15 @@ def test_errors(cuda, oracle):
     # dl_dx and lambda the same buffer
     assert abi.lib().alpb_ppr_adjoint(P.h, dev.ptr(lam), dev.ptr(lam), 1e-9, 10, it, res,
                                       dev.stream_ptr()) == 4
-    # negative weight
+    # negative weight: rejected, and the handle keeps the previous weights
     wn = w.copy()
     wn[3] = -1.0
     wt = torch.from_numpy(wn).cuda()
     assert abi.lib().alpb_ppr_set_weights(P.h, dev.ptr(wt), dev.stream_ptr()) == 7
+    x2, it2, _ = P.solve([1, 2], expect_rc=0)
+    xo, ito, _ = O.forward(rp, col, w, [1, 2], conv=1e-9)
+    np.testing.assert_array_equal(it2, ito)
+    np.testing.assert_allclose(host(x2, P.n, 2), xo, rtol=1e-11, atol=1e-15)
     P.close()
     h = C.c_void_p()
     assert abi.lib().alpb_ppr_create(C.byref(h), P.n, P.nnz, dev.ptr(P.rp), dev.ptr(P.col),
