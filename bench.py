@@ -68,6 +68,24 @@ def profiled_traffic(kernel_tag: str):
     return float(m.group(1)) if m else None
 
 
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The slowest rank's time (every rank calls this the same number of
+    times); one rank returns its own."""
+    if world == 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(bytes_per_step: int, ms_per_step: float, world: int) -> float:
+    """Whole-job GB/s of `world` replicas that each moved bytes_per_step per
+    step, timed by the slowest rank."""
+    return world * bytes_per_step / (ms_per_step * 1e-3) / 1e9
+
+
 class ClockSampler:
     """nvidia-smi sampling of SM clocks and throttle reasons."""
 
@@ -183,11 +201,8 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
             step()
         torch.cuda.synchronize()
     clock_rows = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * nbytes / (ms * 1e-3) / 1e9
+    ms = max_over_ranks(ms, world, "cuda")
+    value = replica_rate(nbytes, ms, world)
 
     # end to end through the C-ABI with host buffers, pipelined over three
     # streams: step k copies its x from pinned host memory (copy-in stream),
@@ -238,12 +253,8 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
     stream.wait_event(ev_o[(state["k"] - 1) & 1])   # the last step's copy-out
     e1.record(stream)
     barrier()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * nbytes / (e2e_ms * 1e-3) / 1e9
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, "cuda")
+    e2e_value = replica_rate(nbytes, e2e_ms, world)
 
     peaks = measured_peaks()
     kernel_tag = (f"spmv_wmerge_rmat{args.scale}" if sched == abi.SCHED_MERGE_PATH
@@ -251,7 +262,9 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
     traffic = profiled_traffic(kernel_tag)
     achieved = nbytes / (ms * 1e-3) / 1e9
     extra = {}
-    if rank == 0 and not args.no_extra:
+    # secondary workloads: one GPU only (with replicas the other ranks would
+    # wait at the final barrier for as long as they run)
+    if rank == 0 and world == 1 and not args.no_extra:
         extra = extra_workloads(args, A, plan)
     result = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
