@@ -386,6 +386,11 @@ def extra_workloads(args, A, plan) -> dict:
     out["hpcg_256"] = hpcg_workload(stream)
     out["adjoint_cg"] = adjoint_workload(stream)
     out["ppr_rmat24"] = ppr_workload(stream)
+    # each rate next to its fraction of the measured HBM copy bandwidth
+    peak = measured_peaks()["hbm_gbs"]
+    for v in out.values():
+        for k in [k for k in v if k.endswith("GB/s") and isinstance(v[k], (int, float))]:
+            v[k.replace("GB/s", "frac_of_measured_hbm")] = round(v[k] / peak, 4)
     return out
 
 
