@@ -60,8 +60,8 @@ namespace grb {
 	template< typename D, typename RIT, typename CIT, typename NIT >
 	class Matrix< D, b200, RIT, CIT, NIT > {
 
-		static_assert( sizeof( RIT ) <= 4 && sizeof( CIT ) <= 4,
-			"the b200 backend stores 32-bit row and column indices" );
+		static_assert( sizeof( RIT ) <= 8 && sizeof( CIT ) <= 8,
+			"row and column index types of at most 64 bits" );
 
 		public:
 
@@ -75,6 +75,10 @@ namespace grb {
 			storage_t _crs, _ccs;
 
 			void init( const size_t m, const size_t n, const size_t cap ) {
+				// the device stores 32-bit row and column indices, whatever RIT/CIT
+				if( m > 0xFFFFFFFFull || n > 0xFFFFFFFFull ) {
+					throw std::runtime_error( "grb::Matrix< b200 >: dimensions beyond 32-bit indices" );
+				}
 				_m = m;
 				_n = n;
 				_cap = cap;
@@ -269,6 +273,39 @@ namespace grb {
 			/** Replace the contents by the (I, J, V) triples, in input order: both
 			 *  orientations are built on the device with the reference's in-row
 			 *  order (alpb_coo_to_crs). */
+			/** Both orientations from a host CRS kept in its given in-row order
+			 *  (the CCS by a stable device transpose). */
+			RC b200_set_crs( const std::vector< int64_t > &off, const std::vector< uint32_t > &col,
+				const std::vector< storage_type > &val
+			) {
+				using namespace internal::b200rt;
+				const size_t nz = col.size();
+				const int vt = type_code< D >::value;
+				if( vt < 0 ) { return UNSUPPORTED; }
+				if( off.size() != _m + 1 ) { return MISMATCH; }
+				_crs.release_all();
+				_ccs.release_all();
+				init( _m, _n, nz > _cap ? nz : _cap );
+				(void) alpb_memcpy_h2d( _crs.offsets, off.data(), ( _m + 1 ) * 8, stream() );
+				if( nz > 0 ) {
+					_crs.indices = alloc< uint32_t >( nz );
+					_ccs.indices = alloc< uint32_t >( nz );
+					(void) alpb_memcpy_h2d( _crs.indices, col.data(), nz * 4, stream() );
+					if( vt != ALPB_VOID ) {
+						_crs.values = alloc< storage_type >( nz );
+						_ccs.values = alloc< storage_type >( nz );
+						(void) alpb_memcpy_h2d( _crs.values, val.data(), nz * sizeof( storage_type ),
+							stream() );
+					}
+				}
+				const RC rc = nz == 0 ? SUCCESS : check( alpb_crs_transpose( _m, _n, nz, _crs.offsets,
+					_crs.indices, _crs.values, vt, _ccs.offsets, _ccs.indices, _ccs.values, stream() ),
+					"wrapCRSMatrix (CCS)" );
+				(void) alpb_stream_sync( stream() );
+				if( rc == SUCCESS ) { _nz = nz; }
+				return rc;
+			}
+
 			RC b200_build( const std::vector< uint32_t > &I, const std::vector< uint32_t > &J,
 				const std::vector< storage_type > &V
 			) {
@@ -309,6 +346,56 @@ namespace grb {
 
 
 	namespace internal {
+
+		/**
+		 * A b200 matrix holding a copy of the host CRS (value_array,
+		 * index_array, offst_array) of an m x n matrix, in the given in-row
+		 * order; the CCS is built on the device.  Serves
+		 * internal::wrapCRSMatrix (reference/matrix.hpp:65-88), whose reference
+		 * form views the caller's arrays: the device cannot, so the b200 form
+		 * copies them (the transition API, src/transition/solver.cpp:169,
+		 * keeps the arrays unchanged while its handle lives).  Throws when the
+		 * value type has no device storage.
+		 */
+		template<
+			typename ValType, typename ColType, typename IndType,
+			Backend backend = config::default_backend
+		>
+		const grb::Matrix< ValType, backend, ColType, ColType, IndType > wrapCRSMatrix(
+			const ValType *__restrict__ const value_array,
+			const ColType *__restrict__ const index_array,
+			const IndType *__restrict__ const offst_array,
+			const size_t m, const size_t n
+		) {
+			static_assert( backend == b200, "the b200 form of wrapCRSMatrix" );
+			using namespace internal::b200rt;
+			typedef grb::Matrix< ValType, backend, ColType, ColType, IndType > M;
+			typedef typename M::storage_type S;
+			const int vt = type_code< ValType >::value;
+			if( vt < 0 ) {
+				throw std::runtime_error( "grb::internal::wrapCRSMatrix< b200 >: value type "
+					"without device storage" );
+			}
+			const size_t nz = static_cast< size_t >( offst_array[ m ] );
+			M A( m, n, nz );
+			std::vector< int64_t > off( m + 1 );
+			for( size_t i = 0; i <= m; ++i ) { off[ i ] = static_cast< int64_t >( offst_array[ i ] ); }
+			std::vector< uint32_t > col( nz );
+			for( size_t k = 0; k < nz; ++k ) {
+				if( static_cast< size_t >( index_array[ k ] ) >= n ) {
+					throw std::runtime_error( "grb::internal::wrapCRSMatrix< b200 >: column index "
+						"out of range" );
+				}
+				col[ k ] = static_cast< uint32_t >( index_array[ k ] );
+			}
+			std::vector< S > val( vt == ALPB_VOID ? 0 : nz );
+			for( size_t k = 0; k < val.size(); ++k ) { val[ k ] = static_cast< S >( value_array[ k ] ); }
+			const RC rc = A.b200_set_crs( off, col, val );
+			if( rc != SUCCESS ) {
+				throw std::runtime_error( "grb::internal::wrapCRSMatrix< b200 >: device build failed" );
+			}
+			return A;
+		}
 
 		/** Storage accessors under the names ALP's utilities use for the
 		 *  reference backend; a b200 matrix keeps both orientations on the

@@ -47,6 +47,7 @@ namespace grb {
 			int64_t * _count = nullptr;      // managed [1]
 			bool _dense = false;
 			mutable bool _host_touched = false;
+			D * _wrap_back = nullptr;        // caller's array a wrapped vector writes back to
 
 			void allocate( const size_t n ) {
 				_n = n;
@@ -70,6 +71,11 @@ namespace grb {
 			}
 
 			void free_all() noexcept {
+				if( _wrap_back && _n > 0 ) {   // a wrapped caller array gets the final values
+					b200_host_ready();
+					for( size_t i = 0; i < _n; ++i ) { _wrap_back[ i ] = static_cast< D >( _val[ i ] ); }
+				}
+				_wrap_back = nullptr;
 				internal::b200rt::release( _val );
 				internal::b200rt::release( _flags );
 				internal::b200rt::release( _count );
@@ -156,9 +162,11 @@ namespace grb {
 					_count = o._count;
 					_dense = o._dense;
 					_host_touched = o._host_touched;
+					_wrap_back = o._wrap_back;
 					o._val = nullptr;
 					o._flags = nullptr;
 					o._count = nullptr;
+					o._wrap_back = nullptr;
 					o._n = 0;
 					o._dense = false;
 				}
@@ -230,6 +238,21 @@ namespace grb {
 			/** Before the host reads this vector. */
 			void b200_host_ready() const { (void) alpb_stream_sync( internal::b200rt::stream() ); }
 
+			/** Every entry from a host array (managed memory: written in place). */
+			void b200_load_host( const D * const src ) {
+				b200_host_ready();
+				for( size_t i = 0; i < _n; ++i ) {
+					_val[ i ] = static_cast< storage_type >( src[ i ] );
+					_flags[ i ] = 1;
+				}
+				if( _n > 0 ) { *_count = static_cast< int64_t >( _n ); }
+				_dense = _n > 0;
+				_host_touched = true;
+			}
+
+			/** Copy the final values back to `dst` when this vector is destroyed. */
+			void b200_write_back_to( D * const dst ) noexcept { _wrap_back = dst; }
+
 			/** Host-side single-entry update (setElement). */
 			void b200_host_set( const size_t i, const D &v ) {
 				b200_host_ready();
@@ -244,6 +267,46 @@ namespace grb {
 	};
 
 	namespace internal {
+
+		/** Host pointer to a vector's values (reference/vector.hpp:117-121):
+		 *  managed memory, valid once the device work before it finished; host
+		 *  writes are moved back before the next primitive. */
+		template< typename D, typename C >
+		inline D * getRaw( Vector< D, b200, C > &x ) noexcept { return x.raw(); }
+
+		template< typename D, typename C >
+		inline const D * getRaw( const Vector< D, b200, C > &x ) noexcept { return x.raw(); }
+
+		/**
+		 * A dense b200 vector over the caller's host array
+		 * (reference/vector.hpp:150-180).  The reference form uses the array as
+		 * its storage; the device cannot, so the b200 form copies it in and,
+		 * for a non-const array, copies the final values back when the vector
+		 * is destroyed (so a solver's result lands in the caller's array, as in
+		 * sparse_cg_solve, src/transition/solver.cpp:770-780).
+		 */
+		template< typename D, Backend backend = config::default_backend >
+		grb::Vector< D, backend, internal::Coordinates<
+			config::IMPLEMENTATION< backend >::coordinatesBackend() > >
+		wrapRawVector( const size_t n, D *__restrict__ const raw ) {
+			static_assert( backend == b200, "the b200 form of wrapRawVector" );
+			grb::Vector< D, backend, internal::Coordinates<
+				config::IMPLEMENTATION< backend >::coordinatesBackend() > > v( n );
+			v.b200_load_host( raw );
+			v.b200_write_back_to( raw );
+			return v;
+		}
+
+		template< typename D, Backend backend = config::default_backend >
+		const grb::Vector< D, backend, internal::Coordinates<
+			config::IMPLEMENTATION< backend >::coordinatesBackend() > >
+		wrapRawVector( const size_t n, const D *__restrict__ const raw ) {
+			static_assert( backend == b200, "the b200 form of wrapRawVector" );
+			grb::Vector< D, backend, internal::Coordinates<
+				config::IMPLEMENTATION< backend >::coordinatesBackend() > > v( n );
+			v.b200_load_host( raw );
+			return v;
+		}
 
 		/** Device size helper used by the b200 primitives. */
 		template< typename D, typename C >
