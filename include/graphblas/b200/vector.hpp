@@ -119,6 +119,12 @@ namespace grb {
 					value_type operator*() const {
 						return value_type( _i, static_cast< D >( _v->_val[ _i ] ) );
 					}
+					/** it->first, it->second on the (index, value) pair, held by value */
+					struct arrow {
+						value_type v;
+						const value_type * operator->() const { return &v; }
+					};
+					arrow operator->() const { return arrow{ **this }; }
 					const_iterator & operator++() { ++_i; skip(); return *this; }
 			};
 
