@@ -23,6 +23,8 @@ __device__ __forceinline__ double apply_op(int op, double a, double b) {
 	case ALPB_OP_RIGHT_ASSIGN: return b;
 	case ALPB_OP_LOR: return (a != 0.0 || b != 0.0) ? 1.0 : 0.0;
 	case ALPB_OP_LAND: return (a != 0.0 && b != 0.0) ? 1.0 : 0.0;
+	case ALPB_OP_EQUAL: return a == b ? 1.0 : 0.0;
+	case ALPB_OP_NOT_EQUAL: return a != b ? 1.0 : 0.0;
 	}
 	return 0.0;
 }
@@ -41,7 +43,10 @@ static bool is_monoid(int op) {
 	return op == ALPB_OP_ADD || op == ALPB_OP_MUL || op == ALPB_OP_MIN || op == ALPB_OP_MAX ||
 		op == ALPB_OP_LOR || op == ALPB_OP_LAND;
 }
-static bool valid_op(int op) { return op >= ALPB_OP_ADD && op <= ALPB_OP_LAND; }
+static bool valid_op(int op) {
+	return (op >= ALPB_OP_ADD && op <= ALPB_OP_LAND) || op == ALPB_OP_EQUAL ||
+		op == ALPB_OP_NOT_EQUAL;
+}
 
 constexpr int RB = 256;  // reduction block
 

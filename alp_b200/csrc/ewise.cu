@@ -46,6 +46,8 @@ __device__ __forceinline__ double opd(int op, double a, double b) {
 	case ALPB_OP_LOR: return (a != 0.0 || b != 0.0) ? 1.0 : 0.0;
 	case ALPB_OP_LAND: return (a != 0.0 && b != 0.0) ? 1.0 : 0.0;
 	case ALPB_OP_LEFT_ASSIGN_IF: return a;  // callers test opd_skips first
+	case ALPB_OP_EQUAL: return a == b ? 1.0 : 0.0;
+	case ALPB_OP_NOT_EQUAL: return a != b ? 1.0 : 0.0;
 	}
 	return 0.0;
 }
@@ -209,7 +211,7 @@ int alpb_vec_reduce(double *result, int add_op, double identity, int mul_op, uin
 	int masked, void *stream) {
 	ALPB_CHECK(result != nullptr, ALPB_ILLEGAL, "alpb_vec_reduce: null result");
 	ALPB_CHECK(add_op >= ALPB_OP_ADD && add_op <= ALPB_OP_LAND && mul_op >= ALPB_OP_ADD &&
-		mul_op <= ALPB_OP_LEFT_ASSIGN_IF, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op,
+		mul_op <= ALPB_OP_NOT_EQUAL, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op,
 		mul_op);
 	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
 	cudaStream_t s = as_stream(stream);
@@ -249,7 +251,7 @@ int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_op, uint3
 	const void *y, int y_type, const uint8_t *y_assigned, double beta, void *stream) {
 	ALPB_CHECK(kind >= ALPB_VEC_SET && kind <= ALPB_VEC_MULADD, ALPB_ILLEGAL,
 		"alpb_vec_op: kind %d", kind);
-	ALPB_CHECK(op >= ALPB_OP_ADD && op <= ALPB_OP_LEFT_ASSIGN_IF, ALPB_UNSUPPORTED,
+	ALPB_CHECK(op >= ALPB_OP_ADD && op <= ALPB_OP_NOT_EQUAL, ALPB_UNSUPPORTED,
 		"alpb_vec_op: op %d", op);
 	ALPB_CHECK(type_size(z_type) > 0, ALPB_UNSUPPORTED, "alpb_vec_op: output type %d", z_type);
 	ALPB_CHECK(z_assigned == nullptr || z_nnz != nullptr, ALPB_ILLEGAL,

@@ -304,7 +304,10 @@ enum alpb_op {
 	/* operators::left_assign_if (base/internalops.hpp:485-570): a where b is
 	 * true; where b is false the output is left as it was, so the term is
 	 * skipped (dot, fold) or nothing is written (element-wise kinds). */
-	ALPB_OP_LEFT_ASSIGN_IF = 11
+	ALPB_OP_LEFT_ASSIGN_IF = 11,
+	/* operators::equal / not_equal (ops.hpp:375-430): 1 where a == b
+	 * (a != b), else 0 */
+	ALPB_OP_EQUAL = 12, ALPB_OP_NOT_EQUAL = 13
 };
 /* *result = *result (+) sum_i x_i (*) y_i with (+) = add_op, (*) = mul_op,
  * over entries assigned in both; result is a HOST double (synchronises). */

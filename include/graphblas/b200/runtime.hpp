@@ -88,6 +88,12 @@ namespace grb {
 			template< typename A, typename B, typename C, Backend X >
 			struct op_code< operators::logical_and< A, B, C, X > > { static constexpr int value = ALPB_OP_LAND; };
 			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::equal< A, B, C, X > > { static constexpr int value = ALPB_OP_EQUAL; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::not_equal< A, B, C, X > > {
+				static constexpr int value = ALPB_OP_NOT_EQUAL;
+			};
+			template< typename A, typename B, typename C, Backend X >
 			struct op_code< operators::left_assign_if< A, B, C, X > > {
 				static constexpr int value = ALPB_OP_LEFT_ASSIGN_IF;
 			};
