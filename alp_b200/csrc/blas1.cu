@@ -25,6 +25,10 @@ __device__ __forceinline__ double apply_op(int op, double a, double b) {
 	case ALPB_OP_LAND: return (a != 0.0 && b != 0.0) ? 1.0 : 0.0;
 	case ALPB_OP_EQUAL: return a == b ? 1.0 : 0.0;
 	case ALPB_OP_NOT_EQUAL: return a != b ? 1.0 : 0.0;
+	case ALPB_OP_LESS: return a < b ? 1.0 : 0.0;
+	case ALPB_OP_LEQ: return a <= b ? 1.0 : 0.0;
+	case ALPB_OP_GREATER: return a > b ? 1.0 : 0.0;
+	case ALPB_OP_GEQ: return a >= b ? 1.0 : 0.0;
 	}
 	return 0.0;
 }
@@ -44,8 +48,8 @@ static bool is_monoid(int op) {
 		op == ALPB_OP_LOR || op == ALPB_OP_LAND;
 }
 static bool valid_op(int op) {
-	return (op >= ALPB_OP_ADD && op <= ALPB_OP_LAND) || op == ALPB_OP_EQUAL ||
-		op == ALPB_OP_NOT_EQUAL;
+	return (op >= ALPB_OP_ADD && op <= ALPB_OP_LAND) ||
+		(op >= ALPB_OP_EQUAL && op <= ALPB_OP_GEQ);
 }
 
 constexpr int RB = 256;  // reduction block
@@ -117,6 +121,8 @@ __global__ void k_set_scalar(void *x, int type, int64_t n, double value, uint8_t
 		case ALPB_BOOL: reinterpret_cast<uint8_t *>(x)[i] = value != 0.0 ? 1 : 0; break;
 		case ALPB_INT64: reinterpret_cast<int64_t *>(x)[i] = int64_t(value); break;
 		case ALPB_UINT32: reinterpret_cast<uint32_t *>(x)[i] = uint32_t(value); break;
+		case ALPB_UINT8: reinterpret_cast<uint8_t *>(x)[i] = uint8_t(int64_t(value)); break;
+		case ALPB_INT8: reinterpret_cast<int8_t *>(x)[i] = int8_t(int64_t(value)); break;
 		}
 		if (assigned) assigned[i] = 1;
 	}

@@ -136,6 +136,40 @@ struct RingPlusTimesI32 {
 	static __device__ __forceinline__ T mulr(T a, T x) { return int32_t(uint32_t(a) * uint32_t(x)); }
 	static __device__ __forceinline__ T mull(T x, T a) { return int32_t(uint32_t(x) * uint32_t(a)); }
 };
+// degree ring of interfaces/pregel.hpp:381-386: right_assign_if(p, q) = bool(p) ? q
+// : (nothing) over size_t (base/internalops.hpp:580-660), additive identity as the
+// "else"; unsigned 64-bit arithmetic on ALPB_INT64 storage
+struct RingPlusRightIfU64 {
+	using T = uint64_t;
+	static constexpr bool immutable = false;
+	static __device__ __forceinline__ T zero() { return 0; }
+	static __device__ __forceinline__ T one() { return 1; }
+	static __device__ __forceinline__ T add(T a, T b) { return a + b; }
+	static __device__ __forceinline__ T mulr(T a, T x) { return a != 0 ? x : 0; }
+	static __device__ __forceinline__ T mull(T x, T a) { return x != 0 ? a : 0; }
+};
+// Pregel message ring under max (connected components): max over size_t with
+// identity numeric_limits<size_t>::min() = 0, multiplied by left_assign_if
+struct RingMaxLeftIfU64 {
+	using T = uint64_t;
+	static constexpr bool immutable = false;
+	static __device__ __forceinline__ T zero() { return 0; }
+	static __device__ __forceinline__ T one() { return 1; }
+	static __device__ __forceinline__ T add(T a, T b) { return a > b ? a : b; }
+	static __device__ __forceinline__ T mulr(T a, T x) { return x != 0 ? a : 0; }
+	static __device__ __forceinline__ T mull(T x, T a) { return a != 0 ? x : 0; }
+};
+// multiplication as the additive monoid (identity 1), addition as the product
+// (identity 0)
+struct RingTimesPlusF64 {
+	using T = double;
+	static constexpr bool immutable = false;
+	static __device__ __forceinline__ T zero() { return 1.0; }
+	static __device__ __forceinline__ T one() { return 0.0; }
+	static __device__ __forceinline__ T add(T a, T b) { return a * b; }
+	static __device__ __forceinline__ T mulr(T a, T x) { return a + x; }
+	static __device__ __forceinline__ T mull(T x, T a) { return x + a; }
+};
 
 // mask evaluation of utils::interpretMask (utils.hpp:318-341)
 __device__ __forceinline__ bool mask_value_true(const void *vals, int type, int64_t i) {
@@ -145,6 +179,8 @@ __device__ __forceinline__ bool mask_value_true(const void *vals, int type, int6
 	case ALPB_INT32: return reinterpret_cast<const int32_t *>(vals)[i] != 0;
 	case ALPB_FP64: return reinterpret_cast<const double *>(vals)[i] != 0.0;
 	case ALPB_UINT32: return reinterpret_cast<const uint32_t *>(vals)[i] != 0;
+	case ALPB_UINT8: return reinterpret_cast<const uint8_t *>(vals)[i] != 0;
+	case ALPB_INT8: return reinterpret_cast<const int8_t *>(vals)[i] != 0;
 	case ALPB_INT64: return reinterpret_cast<const int64_t *>(vals)[i] != 0;
 	}
 	return false;

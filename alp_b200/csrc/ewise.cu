@@ -20,6 +20,8 @@ __device__ __forceinline__ double ld_val(const void *p, int type, int64_t i) {
 	case ALPB_BOOL: return reinterpret_cast<const uint8_t *>(p)[i] ? 1.0 : 0.0;
 	case ALPB_INT64: return double(reinterpret_cast<const int64_t *>(p)[i]);
 	case ALPB_UINT32: return double(reinterpret_cast<const uint32_t *>(p)[i]);
+	case ALPB_UINT8: return double(reinterpret_cast<const uint8_t *>(p)[i]);
+	case ALPB_INT8: return double(reinterpret_cast<const int8_t *>(p)[i]);
 	}
 	return 0.0;
 }
@@ -30,6 +32,8 @@ __device__ __forceinline__ void st_val(void *p, int type, int64_t i, double v) {
 	case ALPB_BOOL: reinterpret_cast<uint8_t *>(p)[i] = v != 0.0 ? 1 : 0; break;
 	case ALPB_INT64: reinterpret_cast<int64_t *>(p)[i] = int64_t(v); break;
 	case ALPB_UINT32: reinterpret_cast<uint32_t *>(p)[i] = uint32_t(int64_t(v)); break;
+	case ALPB_UINT8: reinterpret_cast<uint8_t *>(p)[i] = uint8_t(int64_t(v)); break;
+	case ALPB_INT8: reinterpret_cast<int8_t *>(p)[i] = int8_t(int64_t(v)); break;
 	}
 }
 __device__ __forceinline__ double opd(int op, double a, double b) {
@@ -48,6 +52,10 @@ __device__ __forceinline__ double opd(int op, double a, double b) {
 	case ALPB_OP_LEFT_ASSIGN_IF: return a;  // callers test opd_skips first
 	case ALPB_OP_EQUAL: return a == b ? 1.0 : 0.0;
 	case ALPB_OP_NOT_EQUAL: return a != b ? 1.0 : 0.0;
+	case ALPB_OP_LESS: return a < b ? 1.0 : 0.0;
+	case ALPB_OP_LEQ: return a <= b ? 1.0 : 0.0;
+	case ALPB_OP_GREATER: return a > b ? 1.0 : 0.0;
+	case ALPB_OP_GEQ: return a >= b ? 1.0 : 0.0;
 	}
 	return 0.0;
 }
@@ -211,7 +219,7 @@ int alpb_vec_reduce(double *result, int add_op, double identity, int mul_op, uin
 	int masked, void *stream) {
 	ALPB_CHECK(result != nullptr, ALPB_ILLEGAL, "alpb_vec_reduce: null result");
 	ALPB_CHECK(add_op >= ALPB_OP_ADD && add_op <= ALPB_OP_LAND && mul_op >= ALPB_OP_ADD &&
-		mul_op <= ALPB_OP_NOT_EQUAL, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op,
+		mul_op <= ALPB_OP_GEQ, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op,
 		mul_op);
 	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
 	cudaStream_t s = as_stream(stream);
@@ -251,7 +259,7 @@ int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_op, uint3
 	const void *y, int y_type, const uint8_t *y_assigned, double beta, void *stream) {
 	ALPB_CHECK(kind >= ALPB_VEC_SET && kind <= ALPB_VEC_MULADD, ALPB_ILLEGAL,
 		"alpb_vec_op: kind %d", kind);
-	ALPB_CHECK(op >= ALPB_OP_ADD && op <= ALPB_OP_NOT_EQUAL, ALPB_UNSUPPORTED,
+	ALPB_CHECK(op >= ALPB_OP_ADD && op <= ALPB_OP_GEQ, ALPB_UNSUPPORTED,
 		"alpb_vec_op: op %d", op);
 	ALPB_CHECK(type_size(z_type) > 0, ALPB_UNSUPPORTED, "alpb_vec_op: output type %d", z_type);
 	ALPB_CHECK(z_assigned == nullptr || z_nnz != nullptr, ALPB_ILLEGAL,

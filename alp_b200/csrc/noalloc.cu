@@ -173,6 +173,12 @@ extern "C" int alpb_mxv_dense_noalloc(int ring, int form, int64_t m_out, int64_t
 		return noalloc_run<RingPlusPatternF64>(mt, offsets, indices, values, v, u, left, s);
 	case ALPB_RING_PLUS_TIMES_I32:
 		return noalloc_run<RingPlusTimesI32>(mt, offsets, indices, values, v, u, left, s);
+	case ALPB_RING_PLUS_RIGHT_IF_U64:
+		return noalloc_run<RingPlusRightIfU64>(mt, offsets, indices, values, v, u, left, s);
+	case ALPB_RING_MAX_LEFT_IF_U64:
+		return noalloc_run<RingMaxLeftIfU64>(mt, offsets, indices, values, v, u, left, s);
+	case ALPB_RING_TIMES_PLUS_F64:
+		return noalloc_run<RingTimesPlusF64>(mt, offsets, indices, values, v, u, left, s);
 	}
 	return ALPB_UNSUPPORTED;
 }

@@ -39,6 +39,8 @@ size_t type_size(int type) {
 	case ALPB_FP64: return 8;
 	case ALPB_UINT32: return 4;
 	case ALPB_INT64: return 8;
+	case ALPB_UINT8: return 1;
+	case ALPB_INT8: return 1;
 	}
 	return 0;
 }

@@ -489,6 +489,9 @@ int dispatch_spmv(int ring, const SpmvArgs &a, const alpb_spmv_plan_s *p, int fo
 	case ALPB_RING_MIN_PLUS_I32: return run_spmv<RingMinPlusI32>(a, p, force_sched, s);
 	case ALPB_RING_PLUS_PATTERN_F64: return run_spmv<RingPlusPatternF64>(a, p, force_sched, s);
 	case ALPB_RING_PLUS_TIMES_I32: return run_spmv<RingPlusTimesI32>(a, p, force_sched, s);
+	case ALPB_RING_PLUS_RIGHT_IF_U64: return run_spmv<RingPlusRightIfU64>(a, p, force_sched, s);
+	case ALPB_RING_MAX_LEFT_IF_U64: return run_spmv<RingMaxLeftIfU64>(a, p, force_sched, s);
+	case ALPB_RING_TIMES_PLUS_F64: return run_spmv<RingTimesPlusF64>(a, p, force_sched, s);
 	}
 	set_error("alpb_mxv: semiring %d is not instantiated on the device", ring);
 	return ALPB_UNSUPPORTED;
@@ -501,6 +504,9 @@ int ring_value_type(int ring) {
 	case ALPB_RING_MIN_PLUS_I32: return ALPB_INT32;
 	case ALPB_RING_PLUS_PATTERN_F64: return ALPB_FP64;
 	case ALPB_RING_PLUS_TIMES_I32: return ALPB_INT32;
+	case ALPB_RING_PLUS_RIGHT_IF_U64: return ALPB_INT64;
+	case ALPB_RING_MAX_LEFT_IF_U64: return ALPB_INT64;
+	case ALPB_RING_TIMES_PLUS_F64: return ALPB_FP64;
 	}
 	return -1;
 }

@@ -75,7 +75,9 @@ enum alpb_type {
 	ALPB_INT32 = 2,
 	ALPB_FP64 = 3,
 	ALPB_UINT32 = 4,
-	ALPB_INT64 = 5
+	ALPB_INT64 = 5,
+	ALPB_UINT8 = 6,  /* unsigned char                                */
+	ALPB_INT8 = 7    /* char / signed char                           */
 };
 
 /*
@@ -93,6 +95,20 @@ enum alpb_type {
  *                     identities::zero, identities::logical_true>
  *                     -- the out-degree ring of simple_pagerank.hpp:224-237
  *   PLUS_TIMES_I32   <operators::add<int>, operators::mul<int>, zero, one>
+ *   PLUS_RIGHT_IF_U64 <operators::add<size_t>,
+ *                     operators::right_assign_if<bool,size_t,size_t>,
+ *                     identities::zero, identities::logical_true>
+ *                     -- the degree ring of interfaces/pregel.hpp:381-386
+ *   MAX_LEFT_IF_U64  <operators::max<size_t>,
+ *                     operators::left_assign_if<size_t,bool,size_t>,
+ *                     identities::negative_infinity, identities::logical_true>
+ *                     -- the message ring of the Pregel interface
+ *                     (pregel.hpp:714-720) under connected components
+ *                     (pregel_connected_components.hpp:148-151)
+ * The two U64 rings hold values as ALPB_INT64 storage, compared unsigned.
+ *   TIMES_PLUS_F64   <operators::mul<double>, operators::add<double>,
+ *                     identities::one, identities::zero> -- the switched ring
+ *                     of ALP's tests/unit/vmxa.cpp
  * Any other semiring is not instantiated and returns ALPB_UNSUPPORTED.
  */
 enum alpb_ring {
@@ -100,7 +116,10 @@ enum alpb_ring {
 	ALPB_RING_LOR_LAND_BOOL = 1,
 	ALPB_RING_MIN_PLUS_I32 = 2,
 	ALPB_RING_PLUS_PATTERN_F64 = 3,
-	ALPB_RING_PLUS_TIMES_I32 = 4
+	ALPB_RING_PLUS_TIMES_I32 = 4,
+	ALPB_RING_PLUS_RIGHT_IF_U64 = 5,
+	ALPB_RING_MAX_LEFT_IF_U64 = 6,
+	ALPB_RING_TIMES_PLUS_F64 = 7
 };
 
 /* SpMV schedules (the autotuner chooses among them per sparsity profile) */
@@ -307,7 +326,10 @@ enum alpb_op {
 	ALPB_OP_LEFT_ASSIGN_IF = 11,
 	/* operators::equal / not_equal (ops.hpp:375-430): 1 where a == b
 	 * (a != b), else 0 */
-	ALPB_OP_EQUAL = 12, ALPB_OP_NOT_EQUAL = 13
+	ALPB_OP_EQUAL = 12, ALPB_OP_NOT_EQUAL = 13,
+	/* operators::less_than / leq / greater_than / geq (ops.hpp:707-820):
+	 * 1 where a < b (a <= b, a > b, a >= b), else 0 */
+	ALPB_OP_LESS = 14, ALPB_OP_LEQ = 15, ALPB_OP_GREATER = 16, ALPB_OP_GEQ = 17
 };
 /* *result = *result (+) sum_i x_i (*) y_i with (+) = add_op, (*) = mul_op,
  * over entries assigned in both; result is a HOST double (synchronises). */

@@ -396,6 +396,18 @@ namespace grb {
 			grb::is_operator< OP >::value, void >::type * const = nullptr
 	) {
 		(void) op;
+		// aliased operands as the reference resolves them (reference/blas1.hpp:5260-5270)
+		if( static_cast< const void * >( &x ) == static_cast< const void * >( &y ) &&
+			grb::is_idempotent< OP >::value
+		) {
+			return set< descr >( z, x, phase );
+		}
+		if( static_cast< const void * >( &x ) == static_cast< const void * >( &z ) ) {
+			return foldl< descr >( z, y, op, phase );
+		}
+		if( static_cast< const void * >( &y ) == static_cast< const void * >( &z ) ) {
+			return foldr< descr >( x, z, op, phase );
+		}
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, OutputType, InputType1, InputType2, bool >(
 			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, nullptr, &x, 0.0,
@@ -445,10 +457,229 @@ namespace grb {
 			grb::is_operator< OP >::value, void >::type * const = nullptr
 	) {
 		(void) op;
+		// z aliasing y folds alpha into it (reference/blas1.hpp:5045-5047)
+		if( static_cast< const void * >( &y ) == static_cast< const void * >( &z ) ) {
+			return foldr< descr >( alpha, z, op, phase );
+		}
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, OutputType, InputType2, InputType2, bool >(
 			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, nullptr, nullptr,
 			static_cast< double >( alpha ), &y, 0.0 );
+	}
+
+	// two scalars: z is set to alpha (.) beta, everywhere or under the mask
+	// (reference/blas1.hpp:4083-4300)
+	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z, const InputType1 alpha,
+		const InputType2 beta, const OP &op = OP(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_operator< OP >::value, void >::type * const = nullptr
+	) {
+		if( ( descr & descriptors::dense ) && nnz( z ) < size( z ) ) { return ILLEGAL; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		typename OP::D3 val;
+		const RC rc = apply< descr >( val, alpha, beta, op );
+		return rc != SUCCESS ? rc : set< descr >( z, val );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
+		typename MaskType, typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &mask, const InputType1 alpha,
+		const InputType2 beta, const OP &op = OP(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && grb::is_operator< OP >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( mask ) == 0 ) { return eWiseApply< descr >( z, alpha, beta, op, phase ); }
+		if( size( mask ) != size( z ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		typename OP::D3 val;
+		const RC rc = apply< descr >( val, alpha, beta, op );
+		return rc != SUCCESS ? rc : set< descr >( z, mask, val );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z, const InputType1 alpha,
+		const InputType2 beta, const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_monoid< Monoid >::value, void >::type * const = nullptr
+	) {
+		return eWiseApply< descr >( z, alpha, beta, monoid.getOperator(), phase );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
+		typename MaskType, typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &mask, const InputType1 alpha,
+		const InputType2 beta, const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && grb::is_monoid< Monoid >::value,
+			void >::type * const = nullptr
+	) {
+		return eWiseApply< descr >( z, mask, alpha, beta, monoid.getOperator(), phase );
+	}
+
+	// masked eWiseApply: z is cleared, then z_i = x_i (.) y_i wherever the mask
+	// holds (reference/blas1.hpp:4307-4400, 5090-5180, 5343-5440); an empty mask
+	// is the unmasked primitive.  Operators take the intersection of the inputs'
+	// structures, monoids their union (reference/blas1.hpp:4658-4780).
+	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
+		typename MaskType, typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &mask, const Vector< InputType1, b200, Coords > &x,
+		const InputType2 beta, const OP &op = OP(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && grb::is_operator< OP >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( mask ) == 0 ) { return eWiseApply< descr >( z, x, beta, op, phase ); }
+		if( size( mask ) != size( z ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, OutputType, InputType1, InputType1, MaskType >(
+			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, &mask, &x, 0.0,
+			nullptr, static_cast< double >( beta ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
+		typename MaskType, typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &mask, const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &y, const OP &op = OP(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && grb::is_operator< OP >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( mask ) == 0 ) { return eWiseApply< descr >( z, alpha, y, op, phase ); }
+		if( size( mask ) != size( z ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, OutputType, InputType2, InputType2, MaskType >(
+			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, &mask, nullptr,
+			static_cast< double >( alpha ), &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
+		typename MaskType, typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &mask, const Vector< InputType1, b200, Coords > &x,
+		const Vector< InputType2, b200, Coords > &y, const OP &op = OP(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && grb::is_operator< OP >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( mask ) == 0 ) { return eWiseApply< descr >( z, x, y, op, phase ); }
+		if( size( mask ) != size( z ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		return internal::b200rt::vec_op< descr, OutputType, InputType1, InputType2, MaskType >(
+			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, &mask, &x, 0.0,
+			&y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
+		typename MaskType, typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &mask, const Vector< InputType1, b200, Coords > &x,
+		const Vector< InputType2, b200, Coords > &y, const Monoid &monoid = Monoid(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && grb::is_monoid< Monoid >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( mask ) == 0 ) { return eWiseApply< descr >( z, x, y, monoid, phase ); }
+		if( size( mask ) != size( z ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType1, InputType2, MaskType >( ALPB_VEC_APPLY,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, &mask, &x,
+			0.0, &y, 0.0 );
+	}
+
+	// monoid with a scalar operand: an absent x_i takes the identity, so the
+	// output is dense (reference/blas1.hpp:4502-4640), or dense under the mask
+	// (reference/blas1.hpp:4793-4960)
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< InputType1, b200, Coords > &x, const InputType2 beta,
+		const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_monoid< Monoid >::value, void >::type * const = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType1, InputType1, bool >( ALPB_VEC_APPLY,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, nullptr, &x,
+			0.0, nullptr, static_cast< double >( beta ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
+		typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z, const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &y, const Monoid &monoid = Monoid(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType1 >::value && !grb::is_object< InputType2 >::value &&
+			grb::is_monoid< Monoid >::value, void >::type * const = nullptr
+	) {
+		(void) monoid;
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType2, InputType2, bool >( ALPB_VEC_APPLY,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, nullptr,
+			nullptr, static_cast< double >( alpha ), &y, 0.0 );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
+		typename MaskType, typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &mask, const Vector< InputType1, b200, Coords > &x,
+		const InputType2 beta, const Monoid &monoid = Monoid(), const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && grb::is_monoid< Monoid >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( mask ) == 0 ) { return eWiseApply< descr >( z, x, beta, monoid, phase ); }
+		if( size( mask ) != size( z ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType1, InputType1, MaskType >( ALPB_VEC_APPLY,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, &mask, &x,
+			0.0, nullptr, static_cast< double >( beta ) );
+	}
+
+	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
+		typename MaskType, typename InputType1, typename InputType2, typename Coords >
+	RC eWiseApply( Vector< OutputType, b200, Coords > &z,
+		const Vector< MaskType, b200, Coords > &mask, const InputType1 alpha,
+		const Vector< InputType2, b200, Coords > &y, const Monoid &monoid = Monoid(),
+		const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< MaskType >::value && !grb::is_object< InputType1 >::value &&
+			!grb::is_object< InputType2 >::value && grb::is_monoid< Monoid >::value,
+			void >::type * const = nullptr
+	) {
+		if( size( mask ) == 0 ) { return eWiseApply< descr >( z, alpha, y, monoid, phase ); }
+		if( size( mask ) != size( z ) ) { return MISMATCH; }
+		if( phase == RESIZE ) { return SUCCESS; }
+		using namespace internal::b200rt;
+		return vec_op< descr, OutputType, InputType2, InputType2, MaskType >( ALPB_VEC_APPLY,
+			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, &mask,
+			nullptr, static_cast< double >( alpha ), &y, 0.0 );
 	}
 
 	// ------------------------------------------------------------- eWiseMul --

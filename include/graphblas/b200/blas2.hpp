@@ -48,6 +48,19 @@ namespace grb {
 				if( ring_id < 0 ) { return UNSUPPORTED; }
 				const int vt = type_code< InputType2 >::value;
 				const int ut = type_code< IOType >::value, xt = type_code< InputType1 >::value;
+				// vectors of another domain than the ring's are cast element-wise, as
+				// ALP's operators cast their operands: stage them through vectors of
+				// the ring's output domain, keeping their sparsity
+				typedef typename Ring::D4 RD;
+				constexpr int rt = type_code< RD >::value;
+				if( rt >= 0 && ut >= 0 && xt >= 0 && ( ut != rt || xt != rt ) ) {
+					Vector< RD, grb::b200, Coords > us( out_len ), vs( in_len );
+					RC rc = set( us, u );
+					rc = rc ? rc : set( vs, v );
+					rc = rc ? rc : spmv< descr, left >( us, u_mask, A, vs, v_mask, ring, phase );
+					rc = rc ? rc : set( u, us );
+					return rc;
+				}
 				const int mt = type_code< InputType3 >::value, vmt = type_code< InputType4 >::value;
 				if( vt < 0 || mt < 0 || vmt < 0 || ut != xt || ut < 0 ) { return UNSUPPORTED; }
 				if( vt != ALPB_VOID && vt != ut ) { return UNSUPPORTED; }
@@ -56,6 +69,13 @@ namespace grb {
 					const double z0 = static_cast< double >( ring.template getZero< IOType >() );
 					const double o1 = static_cast< double >( ring.template getOne< IOType >() );
 					if( ring_id == ALPB_RING_PLUS_TIMES_F64 && ( z0 != 0.0 || o1 != 1.0 ) ) {
+						return UNSUPPORTED;
+					}
+					if( ring_id == ALPB_RING_TIMES_PLUS_F64 && ( z0 != 1.0 || o1 != 0.0 ) ) {
+						return UNSUPPORTED;
+					}
+					if( ( ring_id == ALPB_RING_PLUS_RIGHT_IF_U64 ||
+						ring_id == ALPB_RING_MAX_LEFT_IF_U64 ) && z0 != 0.0 ) {
 						return UNSUPPORTED;
 					}
 				}

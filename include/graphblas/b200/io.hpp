@@ -258,20 +258,33 @@ namespace grb {
 		const fwd_iterator end, const IOMode mode, const Dup &dup = Dup()
 	) {
 		(void) mode;
-		(void) dup;
 		const size_t n = size( x );
 		x.b200_host_ready();
 		InputType * const raw = x.raw();
+		uint8_t * const fl = x.b200_flags();
 		size_t i = 0;
-		for( ; start != end && i < n; ++start, ++i ) { raw[ i ] = static_cast< InputType >( *start ); }
-		if( start != end ) { return MISMATCH; }
-		for( size_t k = 0; k < i; ++k ) { x.b200_flags()[ k ] = 1; }
+		RC ret = SUCCESS;
+		// an entry that exists already is folded with dup, or is an error under
+		// no_duplicates (reference/vector.hpp:482-495)
+		for( ; start != end && i < n; ++start, ++i ) {
+			const InputType v = static_cast< InputType >( *start );
+			if( fl[ i ] ) {
+				if( descr & descriptors::no_duplicates ) { ret = ILLEGAL; break; }
+				InputType out;
+				(void) grb::apply( out, raw[ i ], v, dup );
+				raw[ i ] = out;
+			} else {
+				raw[ i ] = v;
+				fl[ i ] = 1;
+			}
+		}
+		if( ret == SUCCESS && start != end ) { ret = MISMATCH; }
 		// entries beyond the input keep their assigned state
 		size_t cnt = 0;
-		for( size_t k = 0; k < n; ++k ) { cnt += x.b200_flags()[ k ] ? 1 : 0; }
+		for( size_t k = 0; k < n; ++k ) { cnt += fl[ k ] ? 1 : 0; }
 		*x.b200_counter() = static_cast< int64_t >( cnt );
 		if( cnt == n ) { x.b200_mark_dense(); } else { x.b200_mark_sparse(); }
-		return SUCCESS;
+		return ret;
 	}
 
 	template< Descriptor descr = descriptors::no_operation, typename InputType,
@@ -286,11 +299,13 @@ namespace grb {
 		x.b200_host_ready();
 		InputType * const raw = x.raw();
 		uint8_t * const fl = x.b200_flags();
+		RC ret = SUCCESS;
 		for( ; ind_start != ind_end && val_start != val_end; ++ind_start, ++val_start ) {
 			const size_t i = static_cast< size_t >( *ind_start );
-			if( i >= n ) { return MISMATCH; }
+			if( i >= n ) { ret = MISMATCH; break; }
 			const InputType v = static_cast< InputType >( *val_start );
 			if( fl[ i ] ) {
+				if( descr & descriptors::no_duplicates ) { ret = ILLEGAL; break; }
 				InputType out;
 				(void) grb::apply( out, raw[ i ], v, dup );
 				raw[ i ] = out;
@@ -303,7 +318,7 @@ namespace grb {
 		for( size_t k = 0; k < n; ++k ) { cnt += fl[ k ] ? 1 : 0; }
 		*x.b200_counter() = static_cast< int64_t >( cnt );
 		if( cnt == n ) { x.b200_mark_dense(); } else { x.b200_mark_sparse(); }
-		return SUCCESS;
+		return ret;
 	}
 
 	// --------------------------------------------------- buildMatrixUnique --

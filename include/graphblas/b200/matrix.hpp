@@ -75,6 +75,11 @@ namespace grb {
 			storage_t _crs, _ccs;
 
 			void init( const size_t m, const size_t n, const size_t cap ) {
+				// a capacity above m * n cannot be used (reference/matrix.hpp:1462-1472 throws
+				// ILLEGAL by name); the division form cannot overflow
+				if( m > 0 && n > 0 && ( cap / m > n || ( cap / m == n && cap % m > 0 ) ) ) {
+					throw std::runtime_error( toString( ILLEGAL ) );
+				}
 				// the device stores 32-bit row and column indices, whatever RIT/CIT
 				if( m > 0xFFFFFFFFull || n > 0xFFFFFFFFull ) {
 					throw std::runtime_error( "grb::Matrix< b200 >: dimensions beyond 32-bit indices" );

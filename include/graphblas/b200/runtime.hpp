@@ -54,6 +54,9 @@ namespace grb {
 			template<> struct type_code< long > { static constexpr int value = ALPB_INT64; };
 			template<> struct type_code< long long > { static constexpr int value = ALPB_INT64; };
 			template<> struct type_code< unsigned long > { static constexpr int value = ALPB_INT64; };
+			template<> struct type_code< unsigned char > { static constexpr int value = ALPB_UINT8; };
+			template<> struct type_code< signed char > { static constexpr int value = ALPB_INT8; };
+			template<> struct type_code< char > { static constexpr int value = ALPB_INT8; };
 			template<> struct type_code< void > { static constexpr int value = ALPB_VOID; };
 
 			/** Device storage type of a domain (bool is held as one byte). */
@@ -93,6 +96,16 @@ namespace grb {
 			struct op_code< operators::not_equal< A, B, C, X > > {
 				static constexpr int value = ALPB_OP_NOT_EQUAL;
 			};
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::less_than< A, B, C, X > > { static constexpr int value = ALPB_OP_LESS; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::leq< A, B, C, X > > { static constexpr int value = ALPB_OP_LEQ; };
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::greater_than< A, B, C, X > > {
+				static constexpr int value = ALPB_OP_GREATER;
+			};
+			template< typename A, typename B, typename C, Backend X >
+			struct op_code< operators::geq< A, B, C, X > > { static constexpr int value = ALPB_OP_GEQ; };
 			template< typename A, typename B, typename C, Backend X >
 			struct op_code< operators::left_assign_if< A, B, C, X > > {
 				static constexpr int value = ALPB_OP_LEFT_ASSIGN_IF;
@@ -134,6 +147,25 @@ namespace grb {
 			struct ring_code< operators::add< int, int, int, X >,
 				operators::mul< int, int, int, Y > > {
 				static constexpr int value = ALPB_RING_PLUS_TIMES_I32;
+			};
+
+			// the degree ring of the Pregel interface (interfaces/pregel.hpp:381-386)
+			template< Backend X, Backend Y >
+			struct ring_code< operators::add< size_t, size_t, size_t, X >,
+				operators::right_assign_if< bool, size_t, size_t, Y > > {
+				static constexpr int value = ALPB_RING_PLUS_RIGHT_IF_U64;
+			};
+			// Pregel messages under max (pregel.hpp:714-720 with operators::max<size_t>)
+			template< Backend X, Backend Y >
+			struct ring_code< operators::max< size_t, size_t, size_t, X >,
+				operators::left_assign_if< size_t, bool, size_t, Y > > {
+				static constexpr int value = ALPB_RING_MAX_LEFT_IF_U64;
+			};
+
+			template< Backend X, Backend Y >
+			struct ring_code< operators::mul< double, double, double, X >,
+				operators::add< double, double, double, Y > > {
+				static constexpr int value = ALPB_RING_TIMES_PLUS_F64;
 			};
 
 			/** Device allocation that reports OUTOFMEM through the C-ABI. */

@@ -128,7 +128,12 @@ namespace grb {
 					const_iterator & operator++() { ++_i; skip(); return *this; }
 			};
 
-			Vector( const size_t n, const size_t nz ) { (void) nz; allocate( n ); }
+			/** A capacity above the size is refused as the reference refuses it
+			 *  (reference/vector.hpp:365-371: ILLEGAL thrown by name). */
+			Vector( const size_t n, const size_t nz ) {
+				if( nz > n ) { throw std::runtime_error( toString( ILLEGAL ) ); }
+				allocate( n );
+			}
 
 			Vector( const size_t n ) { allocate( n ); }
 

@@ -78,3 +78,87 @@ def test_bicgstab_matches_reference(cuda):
     xs = re.search(r"First 10 nonzeroes of x are: \(([^)]*)\)", out).group(1).split()
     xr = re.search(r"First 10 nonzeroes of x are: \(([^)]*)\)", outr).group(1).split()
     assert [round(float(a), 4) for a in xs] == [round(float(b), 4) for b in xr]
+
+
+def write_inputs(d):
+    """Directed R-MAT scale-10 pattern (self loops dropped), its undirected
+    lower triangle, and the 27-point 12^3 system, as MatrixMarket files."""
+    import numpy as np
+    from oracle.oracle import VOID, Restatement, crs_to_coo
+    R = Restatement()
+    rp, col, _ = R.rmat(10, seed=5, vtype=VOID)
+    n = len(rp) - 1
+    r, c = crs_to_coo(rp, col)
+    keep = r != c
+    r, c = r[keep], c[keep]
+    g = Path(d) / "g.mtx"
+    g.write_text("%%MatrixMarket matrix coordinate pattern general\n"
+                 f"{n} {n} {len(r)}\n" + "".join(f"{a + 1} {b + 1}\n" for a, b in zip(r, c)))
+    und = sorted({(max(a, b), min(a, b)) for a, b in zip(r.tolist(), c.tolist())})
+    u = Path(d) / "u.mtx"
+    u.write_text("%%MatrixMarket matrix coordinate pattern symmetric\n"
+                 f"{n} {n} {len(und)}\n" + "".join(f"{a + 1} {b + 1}\n" for a, b in und))
+    I, J, V = R.stencil_coo((12, 12, 12))
+    s = Path(d) / "spd.mtx"
+    s.write_text("%%MatrixMarket matrix coordinate real general\n"
+                 f"{12 ** 3} {12 ** 3} {len(I)}\n" +
+                 "".join(f"{a + 1} {b + 1} {v}\n" for a, b, v in zip(I, J, V)))
+    return g, u, s
+
+
+def first_ten(out):
+    m = re.search(r"First 10 nonzeroes of \w+ are: \(([^)]*)\)", out)
+    assert m, out[-2000:]
+    return [float(v) for v in m.group(1).split()]
+
+
+def pairs(out):
+    return [(int(a), float(b)) for a, b in re.findall(r"^\s+(\d+), ([0-9.eE+-]+)$", out, re.M)]
+
+
+@pytest.fixture(scope="module")
+def inputs(tmp_path_factory):
+    return write_inputs(tmp_path_factory.mktemp("alp_inputs"))
+
+
+def test_simple_pagerank_matches_reference(cuda, inputs):
+    g, _, _ = inputs
+    out = run("simple_pagerank", g, "direct", 1, 1, 1000)
+    outr = run("simple_pagerank", g, "direct", 1, 1, 1000, backend="ref")
+    assert solver_result(out)[0] == solver_result(outr)[0]
+    assert first_ten(out) == pytest.approx(first_ten(outr), rel=1e-5)
+
+
+def test_pregel_pagerank_matches_reference(cuda, inputs):
+    g, _, _ = inputs
+    out = pairs(run("pregel_pagerank", g, "direct", 1, 1))
+    outr = pairs(run("pregel_pagerank", g, "direct", 1, 1, backend="ref"))
+    assert len(out) == len(outr) > 0
+    for (i, v), (ir, vr) in zip(out, outr):
+        assert i == ir and v == pytest.approx(vr, rel=1e-5)
+
+
+def test_pregel_connected_components_matches_reference(cuda, inputs):
+    _, u, _ = inputs
+    out = pairs(run("pregel_cc", u, "direct", 1, 1))
+    outr = pairs(run("pregel_cc", u, "direct", 1, 1, backend="ref"))
+    assert out == outr and len(out) > 0
+
+
+def test_kcore_decomposition_matches_reference(cuda, inputs):
+    _, u, _ = inputs
+    out = run("kcore", u, "direct", 1, 1)
+    outr = run("kcore", u, "direct", 1, 1, backend="ref")
+    lv = re.search(r"has (\d+) coreness levels", out).group(1)
+    assert lv == re.search(r"has (\d+) coreness levels", outr).group(1)
+    assert first_ten(out) == first_ten(outr)
+
+
+def test_conjugate_gradient_smoke_matches_reference(cuda, inputs):
+    _, _, s = inputs
+    out = run("conjugate_gradient", s, "direct", 1, 1, 1000, "false")
+    outr = run("conjugate_gradient", s, "direct", 1, 1, 1000, "false", backend="ref")
+    it, res = solver_result(out)
+    itr, resr = solver_result(outr)
+    assert abs(it - itr) <= 1 and res < 1e-8 and resr < 1e-8
+    assert first_ten(out) == pytest.approx(first_ten(outr), rel=1e-5)

@@ -28,7 +28,11 @@ ROOT = Path(__file__).resolve().parent.parent
 B200_BIN = ROOT / "_build" / "cpp"
 REF_BIN = ROOT / "oracle" / "_ref" / "cpp"
 UNIT = ["masked_mxv", "sparse_mxv", "masked_vxm", "dot", "set", "eWiseMul", "muladd",
-        "masked_muladd", "eWiseLambda"]
+        "masked_muladd", "eWiseLambda", "ewiseapply", "adapterIterator", "add15d", "add15m",
+        "buildVector", "clearMatrix", "copyAndAssignVectorIterator", "copyVector",
+        "doubleAssign", "emptyVector", "equals", "id", "iteratorFilter", "moveMatrix",
+        "moveVector", "mul15i", "mul15m", "stdMatrix", "stdVector", "swapVector",
+        "vectorFromListConstructor", "vectorToMatrix", "vmx", "vmxa", "wait"]
 
 
 def _run(exe: Path, *args, timeout=300):
@@ -44,6 +48,51 @@ def test_alp_unit_test_passes_on_b200(cuda, name):
     r = _run(B200_BIN / f"unit_{name}_b200")
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "Test OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+
+
+def _ok(r):
+    out = r.stdout + r.stderr
+    assert r.returncode == 0, out[-3000:]
+    assert "Test OK" in r.stdout and "Test FAILED" not in r.stdout, out[-3000:]
+
+
+def write_unsymmetric_mtx(path, n=497, nnz=1727, seed=497):
+    """A seeded n x n unsymmetric real matrix with the shape of the west0497
+    file ALP's unit tests read (497 rows, about 1.7 k nonzeroes).  Values are
+    positive, so the sums RBGaussSeidel checks to a few ULPs do not cancel."""
+    rng = np.random.default_rng(seed)
+    k = np.unique(rng.integers(0, n, nnz) * n + rng.integers(0, n, nnz))
+    I, J = k // n, k % n
+    V = rng.uniform(0.1, 1, len(k)).round(6)
+    with open(path, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate real general\n{n} {n} {len(k)}\n")
+        f.writelines(f"{a + 1} {b + 1} {float(v)!r}\n" for a, b, v in zip(I, J, V))
+
+
+@pytest.fixture(scope="module")
+def west_like(tmp_path_factory):
+    p = tmp_path_factory.mktemp("alp_unit") / "w497.mtx"
+    write_unsymmetric_mtx(p)
+    return p
+
+
+@pytest.mark.parametrize("n", [10, 1000])
+@pytest.mark.parametrize("case", [1, 2, 3, 4])
+def test_alp_sparse_vxm_unit_test(cuda, n, case):
+    """ALP's sparse_vxm as its unit-test script runs it (sizes 10 and 1000,
+    test cases 1-4, one inner and one outer repetition)."""
+    _ok(_run(B200_BIN / "unit_sparse_vxm_b200", n, case, 1, 1))
+
+
+@pytest.mark.parametrize("case", [1, 2, 3, 4])
+def test_alp_dense_spmv_unit_test(cuda, west_like, case):
+    """ALP's dense_spmv cases Ax, A^T x, xA, xA^T on a matrix of west0497's shape."""
+    _ok(_run(B200_BIN / "unit_dense_spmv_b200", west_like, "direct", case, 1, 1))
+
+
+def test_alp_red_black_gauss_seidel_unit_test(cuda, west_like):
+    """ALP's RBGaussSeidel: double-masked mxv / vxm with safe_overlap."""
+    _ok(_run(B200_BIN / "unit_RBGaussSeidel_b200", west_like))
 
 
 # ------------------------------------------------------------ differential --
