@@ -28,7 +28,8 @@ VOID, BOOL, INT32, FP64, UINT32, INT64 = range(6)
 # rings
 RING_PLUS_TIMES_F64, RING_LOR_LAND_BOOL, RING_MIN_PLUS_I32 = 0, 1, 2
 RING_PLUS_PATTERN_F64, RING_PLUS_TIMES_I32 = 3, 4
-RING_TYPE = {0: FP64, 1: BOOL, 2: INT32, 3: FP64, 4: INT32}
+RING_PLUS_RIGHT_IF_U64, RING_MAX_LEFT_IF_U64, RING_TIMES_PLUS_F64 = 5, 6, 7
+RING_TYPE = {0: FP64, 1: BOOL, 2: INT32, 3: FP64, 4: INT32, 5: INT64, 6: INT64, 7: FP64}
 # schedules
 SCHED_AUTO, SCHED_MERGE_PATH, SCHED_VECTOR = 0, 1, 2
 # ops

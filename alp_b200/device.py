@@ -15,8 +15,9 @@ import torch
 
 from . import _abi as abi
 
-TORCH_DTYPE = {abi.FP64: torch.float64, abi.INT32: torch.int32, abi.BOOL: torch.uint8}
-NP_DTYPE = {abi.FP64: np.float64, abi.INT32: np.int32, abi.BOOL: np.uint8}
+TORCH_DTYPE = {abi.FP64: torch.float64, abi.INT32: torch.int32, abi.BOOL: torch.uint8,
+               abi.INT64: torch.int64}
+NP_DTYPE = {abi.FP64: np.float64, abi.INT32: np.int32, abi.BOOL: np.uint8, abi.INT64: np.int64}
 
 
 def stream_ptr(stream: torch.cuda.Stream | None = None) -> C.c_void_p:

@@ -15,7 +15,19 @@
 
 /* type / ring / descriptor codes of include/alp_b200.h */
 enum { T_VOID = 0, T_BOOL = 1, T_INT32 = 2, T_FP64 = 3, T_UINT32 = 4, T_INT64 = 5 };
-enum { R_PT_F64 = 0, R_LORLAND = 1, R_MINPLUS_I32 = 2, R_PATTERN_F64 = 3, R_PT_I32 = 4 };
+enum {
+	R_PT_F64 = 0, R_LORLAND = 1, R_MINPLUS_I32 = 2, R_PATTERN_F64 = 3, R_PT_I32 = 4,
+	/* add<size_t> with right_assign_if<bool,size_t,size_t>: the degree ring of
+	 * interfaces/pregel.hpp:381-386 */
+	R_PLUS_RIGHTIF_U64 = 5,
+	/* max<size_t> with left_assign_if<size_t,bool,size_t>: Pregel's message ring
+	 * (pregel.hpp:714-720) under connected components
+	 * (pregel_connected_components.hpp:148-151) */
+	R_MAX_LEFTIF_U64 = 6,
+	/* mul<double> as the additive monoid (identity 1) with add<double> as the
+	 * product (identity 0): the switched ring of tests/unit/vmxa.cpp:62-67 */
+	R_TIMES_PLUS_F64 = 7
+};
 #define D_INVERT 1u
 #define D_STRUCTURAL 8u
 #define D_DENSE 16u
@@ -193,12 +205,13 @@ void alpo_crs_transpose(int64_t m, int64_t n, const int64_t *row_ptr, const uint
 }
 
 /* ---------------------------------------------------------- semirings -- */
-typedef union { double d; int32_t i; uint8_t b; } val_t;
+typedef union { double d; int32_t i; uint8_t b; uint64_t u; } val_t;
 
 static val_t rzero(int ring) {
 	val_t v;
 	memset(&v, 0, sizeof(v));
 	if (ring == R_MINPLUS_I32) v.i = INT_MAX;
+	if (ring == R_TIMES_PLUS_F64) v.d = 1.0;
 	return v;
 }
 static val_t rone(int ring) {
@@ -209,6 +222,8 @@ static val_t rone(int ring) {
 	case R_LORLAND: v.b = 1; break;
 	case R_MINPLUS_I32: v.i = 0; break;
 	case R_PT_I32: v.i = 1; break;
+	case R_PLUS_RIGHTIF_U64: case R_MAX_LEFTIF_U64: v.u = 1; break;
+	case R_TIMES_PLUS_F64: v.d = 0.0; break;
 	}
 	return v;
 }
@@ -220,6 +235,9 @@ static val_t radd(int ring, val_t a, val_t b) {
 	case R_LORLAND: v.b = (a.b || b.b) ? 1 : 0; break;
 	case R_MINPLUS_I32: v.i = a.i < b.i ? a.i : b.i; break;
 	case R_PT_I32: v.i = (int32_t) ((uint32_t) a.i + (uint32_t) b.i); break;
+	case R_PLUS_RIGHTIF_U64: v.u = a.u + b.u; break;
+	case R_MAX_LEFTIF_U64: v.u = a.u > b.u ? a.u : b.u; break;
+	case R_TIMES_PLUS_F64: v.d = a.d * b.d; break;
 	}
 	return v;
 }
@@ -236,20 +254,26 @@ static val_t rmul(int ring, val_t p, val_t q) {
 	/* left_assign_if(p, q): q ? p : unchanged (= the additive identity the
 	 * gather initialises the product with), base/internalops.hpp:485-520 */
 	case R_PATTERN_F64: v.d = q.d != 0.0 ? p.d : 0.0; break;
+	/* right_assign_if(p, q): p ? q : unchanged (base/internalops.hpp:580-660) */
+	case R_PLUS_RIGHTIF_U64: v.u = p.u != 0 ? q.u : 0; break;
+	case R_MAX_LEFTIF_U64: v.u = q.u != 0 ? p.u : 0; break;
+	case R_TIMES_PLUS_F64: v.d = p.d + q.d; break;
 	}
 	return v;
 }
 static int requal(int ring, val_t a, val_t b) {
 	switch (ring) {
-	case R_PT_F64: case R_PATTERN_F64: return a.d == b.d;
+	case R_PT_F64: case R_PATTERN_F64: case R_TIMES_PLUS_F64: return a.d == b.d;
 	case R_LORLAND: return a.b == b.b;
+	case R_PLUS_RIGHTIF_U64: case R_MAX_LEFTIF_U64: return a.u == b.u;
 	default: return a.i == b.i;
 	}
 }
 static int rtype(int ring) {
 	switch (ring) {
-	case R_PT_F64: case R_PATTERN_F64: return T_FP64;
+	case R_PT_F64: case R_PATTERN_F64: case R_TIMES_PLUS_F64: return T_FP64;
 	case R_LORLAND: return T_BOOL;
+	case R_PLUS_RIGHTIF_U64: case R_MAX_LEFTIF_U64: return T_INT64;
 	default: return T_INT32;
 	}
 }
@@ -259,18 +283,21 @@ static val_t load(int type, const void *p, int64_t k) {
 	if (type == T_FP64) v.d = ((const double *) p)[k];
 	else if (type == T_INT32) v.i = ((const int32_t *) p)[k];
 	else if (type == T_BOOL) v.b = ((const uint8_t *) p)[k] ? 1 : 0;
+	else if (type == T_INT64) v.u = ((const uint64_t *) p)[k];
 	return v;
 }
 static void store(int type, void *p, int64_t k, val_t v) {
 	if (type == T_FP64) ((double *) p)[k] = v.d;
 	else if (type == T_INT32) ((int32_t *) p)[k] = v.i;
 	else if (type == T_BOOL) ((uint8_t *) p)[k] = v.b;
+	else if (type == T_INT64) ((uint64_t *) p)[k] = v.u;
 }
 static val_t from_index(int ring, int64_t j) {
 	val_t v;
 	memset(&v, 0, sizeof(v));
 	if (rtype(ring) == T_FP64) v.d = (double) j;
 	else if (rtype(ring) == T_INT32) v.i = (int32_t) j;
+	else if (rtype(ring) == T_INT64) v.u = (uint64_t) j;
 	else v.b = j ? 1 : 0;
 	return v;
 }

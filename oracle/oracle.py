@@ -21,8 +21,9 @@ REF_SEQ_SO = HERE / "_ref" / "libalp_ref_seq.so"
 REF_OMP_SO = HERE / "_ref" / "libalp_ref_omp.so"
 
 VOID, BOOL, INT32, FP64 = 0, 1, 2, 3
-NP = {FP64: np.float64, INT32: np.int32, BOOL: np.uint8}
-RING_TYPE = {0: FP64, 1: BOOL, 2: INT32, 3: FP64, 4: INT32}
+INT64 = 5  # holds the unsigned 64-bit values of rings 5 and 6
+NP = {FP64: np.float64, INT32: np.int32, BOOL: np.uint8, INT64: np.uint64}
+RING_TYPE = {0: FP64, 1: BOOL, 2: INT32, 3: FP64, 4: INT32, 5: INT64, 6: INT64, 7: FP64}
 P = C.c_void_p
 
 

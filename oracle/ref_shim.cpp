@@ -29,7 +29,10 @@ using namespace grb;
 namespace {
 
 enum { T_VOID = 0, T_BOOL = 1, T_INT32 = 2, T_FP64 = 3 };
-enum { R_PT_F64 = 0, R_LORLAND = 1, R_MINPLUS_I32 = 2, R_PATTERN_F64 = 3, R_PT_I32 = 4 };
+enum {
+	R_PT_F64 = 0, R_LORLAND = 1, R_MINPLUS_I32 = 2, R_PATTERN_F64 = 3, R_PT_I32 = 4,
+	R_PLUS_RIGHTIF_U64 = 5, R_MAX_LEFTIF_U64 = 6, R_TIMES_PLUS_F64 = 7
+};
 
 bool g_init = false;
 void ensure_init() {
@@ -181,6 +184,23 @@ __attribute__((visibility("default"))) int refw_mxv(int ring, uint32_t descr, in
 	case R_PT_I32: {
 		Semiring<operators::add<int>, operators::mul<int>, identities::zero, identities::one> r;
 		return mxv_ring<int>(r, descr, vxm_form, m, n, nnz, I, J, V, u, u_assigned, u_mask,
+			u_mask_assigned, has_u_mask, v, v_assigned, v_mask, v_mask_assigned, has_v_mask, reps, ms);
+	}
+	case R_PLUS_RIGHTIF_U64: {  // interfaces/pregel.hpp:381-386
+		Semiring<operators::add<size_t>, operators::right_assign_if<bool, size_t, size_t>,
+			identities::zero, identities::logical_true> r;
+		return mxv_ring<size_t>(r, descr, vxm_form, m, n, nnz, I, J, V, u, u_assigned, u_mask,
+			u_mask_assigned, has_u_mask, v, v_assigned, v_mask, v_mask_assigned, has_v_mask, reps, ms);
+	}
+	case R_MAX_LEFTIF_U64: {  // pregel.hpp:714-720 under pregel_connected_components.hpp:148-151
+		Semiring<operators::max<size_t>, operators::left_assign_if<size_t, bool, size_t>,
+			identities::negative_infinity, identities::logical_true> r;
+		return mxv_ring<size_t>(r, descr, vxm_form, m, n, nnz, I, J, V, u, u_assigned, u_mask,
+			u_mask_assigned, has_u_mask, v, v_assigned, v_mask, v_mask_assigned, has_v_mask, reps, ms);
+	}
+	case R_TIMES_PLUS_F64: {  // tests/unit/vmxa.cpp:62-67
+		Semiring<operators::mul<double>, operators::add<double>, identities::one, identities::zero> r;
+		return mxv_ring<double>(r, descr, vxm_form, m, n, nnz, I, J, V, u, u_assigned, u_mask,
 			u_mask_assigned, has_u_mask, v, v_assigned, v_mask, v_mask_assigned, has_v_mask, reps, ms);
 	}
 #endif

@@ -13,8 +13,10 @@ import numpy as np
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 TRANSPOSE = 2
-FP64, INT32, BOOL = 3, 2, 1
-RING_TYPE = {0: FP64, 1: BOOL, 2: INT32, 3: FP64, 4: INT32}
+FP64, INT32, BOOL, INT64 = 3, 2, 1, 5
+# ring code -> value type (include/alp_b200.h enum alpb_ring); the two
+# unsigned 64-bit rings hold ALPB_INT64 storage
+RING_TYPE = {0: FP64, 1: BOOL, 2: INT32, 3: FP64, 4: INT32, 5: INT64, 6: INT64, 7: FP64}
 
 
 def load(name: str) -> dict:
@@ -61,3 +63,25 @@ def vector_args(c: dict, n: int):
     v_mask_count = -1 if vm is None else (int(vma.sum()) if vma is not None else n)
     v_count = int(va.sum()) if va is not None else n
     return u, ua, v, va, um, uma, u_mask_count, vm, vma, v_mask_count, v_count
+
+
+def new_ring_case(R, ring: int, scale: int, seed: int):
+    """R-MAT pattern with values of the ring's type: u64 values in {0, 1, 2}
+    (a zero is a false condition of right_assign_if / left_assign_if), FP64
+    values near 1 for the (times, plus) ring, whose row products must stay
+    finite."""
+    from oracle.oracle import VOID, crs_to_coo
+    rp, col, _ = R.rmat(scale, edge_factor=8, seed=seed, vtype=VOID)
+    n = len(rp) - 1
+    I, J = crs_to_coo(rp, col)
+    rng = np.random.default_rng(seed)
+    if RING_TYPE[ring] == INT64:
+        V = rng.integers(0, 3, len(I)).astype(np.uint64)
+        v = rng.integers(0, 1000, n).astype(np.uint64)
+        # small presets, so that the max ring's mxv form (products are A_ij) moves u too
+        u0 = rng.integers(0, 1000 if ring == 5 else 2, n).astype(np.uint64)
+    else:
+        V = rng.uniform(-0.01, 0.01, len(I))
+        v = rng.uniform(0.99, 1.01, n)
+        u0 = rng.uniform(0.5, 1.5, n)
+    return n, I, J, V, v, u0

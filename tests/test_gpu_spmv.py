@@ -164,6 +164,37 @@ def test_mxv_dense_parity(cuda, oracle, ring, sched, form):
     assert torch.equal(u, u2), "merge path must be deterministic"
 
 
+@pytest.mark.parametrize("ring", [5, 6, 7])
+@pytest.mark.parametrize("sched", SCHEDS, ids=[s[0] for s in SCHEDS])
+@pytest.mark.parametrize("form", [2, 1], ids=["mxv", "vxm"])
+@pytest.mark.parametrize("pattern", [False, True], ids=["valued", "void"])
+def test_mxv_pregel_and_switched_rings(cuda, oracle, ring, sched, form, pattern):
+    """The Pregel degree ring (add, right_assign_if over size_t), its message
+    ring under max (max, left_assign_if) and the switched (times, plus) ring on
+    R-MAT scale 13, every schedule, valued and pattern matrices: bit-exact for
+    the u64 rings, 1e-12 relative for the FP64 products (different order)."""
+    import torch
+    dev = _dev()
+    t = G.RING_TYPE[ring]
+    n, I, J, V, v, u0 = G.new_ring_case(oracle, ring, 13, 500 + ring)
+    vt = VOID if pattern else t
+    rp, col, vals = oracle.coo_to_crs(n, I, J, None if pattern else V, vt)
+    if form == 1:
+        rp, col, vals = oracle.transpose(n, n, rp, col, vals, vt)
+    view = (lambda a: a.view(np.int64)) if t == G.INT64 else (lambda a: a)
+    S = dev.from_host(n, n, rp, col, None if pattern else view(vals), vt)
+    x = torch.from_numpy(view(v).copy()).cuda()
+    u = torch.from_numpy(view(u0).copy()).cuda()
+    plan = dev.Plan(S, sched=sched[1], vector_width=sched[2])
+    dev.mxv(ring, S, u, x, form=form, plan=plan)
+    torch.cuda.synchronize()
+    want = u0.copy()
+    rc, _ = oracle.mxv(ring, 0, form, n, n, rp, col, vals, vt, want, v=v)
+    assert rc == 0
+    got = _np(u).view(np.uint64) if t == G.INT64 else _np(u)
+    assert_ring_equal(ring, got, want)
+
+
 @pytest.mark.parametrize("name", sorted(G.mxv_cases()[1].keys()))
 def test_mxv_golden_reference(cuda, oracle, name):
     import torch

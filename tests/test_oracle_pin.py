@@ -89,6 +89,30 @@ def test_restatement_matches_live_reference(oracle, reference, ring, scale):
         np.testing.assert_array_equal(u, uref)
 
 
+@pytest.mark.parametrize("ring", [5, 6, 7])
+@pytest.mark.parametrize("scale", [6, 10])
+@pytest.mark.parametrize("vxm_form", [0, 1], ids=["mxv", "vxm"])
+def test_new_rings_restatement_matches_live_reference(oracle, reference, ring, scale, vxm_form):
+    """The Pregel degree and message rings and the switched (times, plus)
+    ring: the C restatement against grb::mxv / grb::vxm of the compiled
+    reference on the same triples."""
+    t = G.RING_TYPE[ring]
+    n, I, J, V, v, u0 = G.new_ring_case(oracle, ring, scale, 300 + scale)
+    rp, col, vals = oracle.coo_to_crs(n, I, J, V, t)
+    if vxm_form:
+        rp, col, vals = oracle.transpose(n, n, rp, col, vals, t)
+    u = u0.copy()
+    rc, _ = oracle.mxv(ring, 0, 1 if vxm_form else 2, n, n, rp, col, vals, t, u, v=v)
+    uref = u0.copy()
+    rc2, _ = reference.mxv(ring, 0, vxm_form, n, n, I, J, V, uref, None, v)
+    assert rc == rc2 == 0
+    if t == G.FP64:
+        np.testing.assert_allclose(u, uref, rtol=1e-12, atol=0)
+    else:
+        np.testing.assert_array_equal(u, uref)
+    assert not np.array_equal(u, u0)
+
+
 def test_generators_are_deterministic(oracle):
     a = oracle.rmat(8, seed=9)
     b = oracle.rmat(8, seed=9)
