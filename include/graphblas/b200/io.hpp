@@ -88,6 +88,31 @@ namespace grb {
 		return SUCCESS;
 	}
 
+	/** C = A, structure and values cast to C's domain (reference/io.hpp
+	 *  set( Matrix, Matrix )); same signature as the base declaration, so that
+	 *  this b200 overload is the more specialised one. */
+	template< Descriptor descr = descriptors::no_operation, typename OutputType,
+		typename InputType, typename RIT, typename CIT, typename NIT >
+	RC set( Matrix< OutputType, b200, RIT, CIT, NIT > &C,
+		const Matrix< InputType, b200, RIT, CIT, NIT > &A, const Phase &phase = EXECUTE,
+		const typename std::enable_if< !grb::is_object< OutputType >::value &&
+			!grb::is_object< InputType >::value, void >::type * const = nullptr
+	) {
+		if( nrows( C ) != nrows( A ) || ncols( C ) != ncols( A ) ) { return MISMATCH; }
+		if( static_cast< const void * >( &C ) == static_cast< const void * >( &A ) ) {
+			return ILLEGAL;
+		}
+		if( phase == RESIZE ) {
+			C.b200_reserve( nnz( A ) );
+			return SUCCESS;
+		}
+		try {
+			return C.b200_assign_from( A );
+		} catch( ... ) {
+			return OUTOFMEM;
+		}
+	}
+
 	// ----------------------------------------------------------------- set --
 	namespace internal {
 		namespace b200rt {

@@ -201,6 +201,42 @@ namespace grb {
 			const_iterator end() const { return cend(); }
 
 			// ---- backend-internal access ----
+			/** This matrix becomes A: both orientations copied on the device, A's
+			 *  values cast to D (reference/io.hpp set( Matrix, Matrix )); a pattern
+			 *  (void) target keeps the structure only.  Values cannot come from a
+			 *  pattern A (UNSUPPORTED). */
+			template< typename D2, typename R2, typename C2, typename N2 >
+			RC b200_assign_from( const Matrix< D2, b200, R2, C2, N2 > &A ) {
+				using namespace internal::b200rt;
+				const int dt = type_code< D >::value, st = type_code< D2 >::value;
+				if( dt < 0 || st < 0 || ( dt != ALPB_VOID && st == ALPB_VOID ) ) { return UNSUPPORTED; }
+				const size_t m = A.b200_rows(), n = A.b200_cols(), nz = A.b200_nnz();
+				_crs.release_all();
+				_ccs.release_all();
+				init( m, n, nz > _cap ? nz : _cap );
+				RC rc = SUCCESS;
+				const auto one = [&]( storage_t &dst, const typename Matrix< D2, b200, R2, C2, N2 >::storage_t
+					&src, const size_t outer ) {
+					(void) alpb_memcpy_d2d( dst.offsets, src.offsets, ( outer + 1 ) * 8, stream() );
+					if( nz == 0 ) { return; }
+					dst.indices = alloc< uint32_t >( nz );
+					(void) alpb_memcpy_d2d( dst.indices, src.indices, nz * 4, stream() );
+					if( dt == ALPB_VOID ) { return; }
+					dst.values = alloc< storage_type >( nz );
+					const RC r = check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0, 0,
+						static_cast< int64_t >( nz ), dst.values, dt, nullptr, nullptr, nullptr, nullptr,
+						ALPB_VOID, 0, src.values, st, nullptr, 0.0, nullptr, st, nullptr, 0.0, stream() ),
+						"set (matrix)" );
+					if( rc == SUCCESS ) { rc = r; }
+				};
+				one( _crs, A.b200_crs(), m );
+				one( _ccs, A.b200_ccs(), n );
+				const RC s = check( alpb_stream_sync( stream() ), "set (matrix)" );
+				if( rc == SUCCESS ) { rc = s; }
+				if( rc == SUCCESS ) { _nz = nz; }
+				return rc;
+			}
+
 			size_t b200_rows() const noexcept { return _m; }
 			size_t b200_cols() const noexcept { return _n; }
 			size_t b200_nnz() const noexcept { return _nz; }

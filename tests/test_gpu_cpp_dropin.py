@@ -32,7 +32,8 @@ UNIT = ["masked_mxv", "sparse_mxv", "masked_vxm", "dot", "set", "eWiseMul", "mul
         "buildVector", "clearMatrix", "copyAndAssignVectorIterator", "copyVector",
         "doubleAssign", "emptyVector", "equals", "id", "iteratorFilter", "moveMatrix",
         "moveVector", "mul15i", "mul15m", "stdMatrix", "stdVector", "swapVector",
-        "vectorFromListConstructor", "vectorToMatrix", "vmx", "vmxa", "wait"]
+        "vectorFromListConstructor", "vectorToMatrix", "vmx", "vmxa", "wait", "copyVoidMatrices",
+        "eWiseMatrix"]
 
 
 def _run(exe: Path, *args, timeout=300):
