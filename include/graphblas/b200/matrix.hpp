@@ -19,6 +19,7 @@
 #include <vector>
 #include <algorithm>
 
+#include <graphblas/distribution.hpp>  // one process: ALP's base distribution
 #include <graphblas/base/matrix.hpp>
 #include <graphblas/b200/runtime.hpp>
 
@@ -193,6 +194,12 @@ namespace grb {
 						return value_type( std::make_pair( _row, static_cast< size_t >( _idx[ _k ] ) ),
 							_val.empty() ? D() : static_cast< D >( _val[ _k ] ) );
 					}
+					// it->first / it->second on the entry by value (a proxy holds it)
+					struct arrow {
+						value_type v;
+						const value_type * operator->() const { return &v; }
+					};
+					arrow operator->() const { return arrow{ **this }; }
 			};
 
 			const_iterator cbegin() const { return const_iterator( *this, false ); }

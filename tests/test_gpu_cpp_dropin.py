@@ -77,6 +77,12 @@ def west_like(tmp_path_factory):
     return p
 
 
+def test_alp_build_matrix_unique_unit_test(cuda):
+    """ALP's buildMatrixUnique: sequential and parallel ingestion of band and
+    random matrices, checked nonzero by nonzero through the matrix iterator."""
+    _ok(_run(B200_BIN / "unitu_buildMatrixUnique_b200", timeout=900))
+
+
 @pytest.mark.parametrize("n", [10, 1000])
 @pytest.mark.parametrize("case", [1, 2, 3, 4])
 def test_alp_sparse_vxm_unit_test(cuda, n, case):
