@@ -15,6 +15,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <stdexcept>
+#include <type_traits>
 #include <utility>
 #include <vector>
 #include <algorithm>
@@ -161,8 +162,25 @@ namespace grb {
 					std::vector< storage_type > _val;
 					size_t _row = 0, _k = 0;
 				public:
-					typedef std::pair< std::pair< size_t, size_t >, D > value_type;
+					// ((row, column), value); a pattern matrix yields (row, column), as
+					// the reference's pattern iterator does
+					typedef typename std::conditional< std::is_void< D >::value,
+						std::pair< size_t, size_t >,
+						std::pair< std::pair< size_t, size_t >,
+							typename std::conditional< std::is_void< D >::value, char, D >::type > >::type
+						value_type;
+					// the start-end iterator interface of ALP's matrix iterators
+					// (reference/compressed_storage.hpp: i(), j(), v() and their types)
+					typedef RIT RowIndexType;
+					typedef CIT ColumnIndexType;
+					typedef D ValueType;
 					const_iterator() = default;
+					RowIndexType i() const { return static_cast< RowIndexType >( _row ); }
+					ColumnIndexType j() const { return static_cast< ColumnIndexType >( _idx[ _k ] ); }
+					template< typename DD = D >
+					typename std::enable_if< !std::is_void< DD >::value, DD >::type v() const {
+						return _val.empty() ? DD() : static_cast< DD >( _val[ _k ] );
+					}
 					const_iterator( const Matrix &A, const bool at_end ) {
 						if( at_end ) { _k = A._nz; _row = A._m; return; }
 						_off.resize( A._m + 1 );
@@ -191,8 +209,14 @@ namespace grb {
 						return *this;
 					}
 					value_type operator*() const {
+						return entry( std::integral_constant< bool, std::is_void< D >::value >() );
+					}
+					value_type entry( std::true_type ) const {
+						return value_type( _row, static_cast< size_t >( _idx[ _k ] ) );
+					}
+					value_type entry( std::false_type ) const {
 						return value_type( std::make_pair( _row, static_cast< size_t >( _idx[ _k ] ) ),
-							_val.empty() ? D() : static_cast< D >( _val[ _k ] ) );
+							_val.empty() ? value_type().second : static_cast< D >( _val[ _k ] ) );
 					}
 					// it->first / it->second on the entry by value (a proxy holds it)
 					struct arrow {

@@ -83,6 +83,12 @@ def test_alp_build_matrix_unique_unit_test(cuda):
     _ok(_run(B200_BIN / "unitu_buildMatrixUnique_b200", timeout=900))
 
 
+def test_alp_matrix_iterator_unit_test(cuda):
+    """ALP's matrixIterator: copy, move and i()/j()/v() of the matrix
+    iterators of valued and pattern matrices against the input triples."""
+    _ok(_run(B200_BIN / "unitu_matrixIterator_b200"))
+
+
 @pytest.mark.parametrize("n", [10, 1000])
 @pytest.mark.parametrize("case", [1, 2, 3, 4])
 def test_alp_sparse_vxm_unit_test(cuda, n, case):
