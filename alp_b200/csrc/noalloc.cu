@@ -13,6 +13,8 @@
 #include "merge.cuh"
 #include "spmv.cuh"
 
+#include <cuda.h>
+
 #include <mutex>
 
 namespace alpb {
@@ -39,12 +41,50 @@ struct NoallocLayout {
 };
 static_assert(NoallocLayout::end <= kNoallocBytes, "scratch layout exceeds the array");
 
-// Device address of g_noalloc_scratch, resolved once per device with that
-// device current.  In host code the array's name only stands in for the
-// symbol -- it is not a device address -- so kernels always get this pointer.
+// Device address of g_noalloc_scratch, resolved once per device and context
+// with that device current.  In host code the array's name only stands in for
+// the symbol -- it is not a device address -- so kernels always get this
+// pointer.  The cache is keyed on the current context's process-unique id
+// (cuCtxGetId), not only on the device index: after cudaDeviceReset the
+// runtime makes a new context, the library's module loads again, possibly at
+// another address, and the first call in the new context resolves it anew.
 constexpr int kNoallocMaxDevices = 64;
+struct NoallocSlot {
+	unsigned long long ctx_id;
+	unsigned char *ptr;
+};
 static std::mutex g_noalloc_mutex;
-static unsigned char *g_noalloc_ptr[kNoallocMaxDevices] = {nullptr};
+static NoallocSlot g_noalloc_slot[kNoallocMaxDevices] = {};
+
+// Id of the calling thread's current context; 0 when there is none yet (or
+// the driver lacks cuCtxGetId).  The two driver calls are looked up through
+// the runtime, so the library does not link the driver library itself.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+static unsigned long long noalloc_context_id() {
+	static CtxGetCurrentFn get_current = nullptr;
+	static CtxGetIdFn get_id = nullptr;
+	static bool looked_up = false;
+	if (!looked_up) {   // under g_noalloc_mutex
+		void *f = nullptr, *g = nullptr;
+		cudaDriverEntryPointQueryResult q1, q2;
+		if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q1) == cudaSuccess &&
+			q1 == cudaDriverEntryPointSuccess &&
+			cudaGetDriverEntryPoint("cuCtxGetId", &g, cudaEnableDefault, &q2) == cudaSuccess &&
+			q2 == cudaDriverEntryPointSuccess) {
+			get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+			get_id = reinterpret_cast<CtxGetIdFn>(g);
+		}
+		(void) cudaGetLastError();
+		looked_up = true;
+	}
+	if (!get_current || !get_id) return 0;
+	CUcontext ctx = nullptr;
+	unsigned long long id = 0;
+	if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+	if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+	return id;
+}
 
 static int noalloc_scratch(unsigned char **out) {
 	int dev = 0;
@@ -53,17 +93,21 @@ static int noalloc_scratch(unsigned char **out) {
 		"alpb_mxv_dense_noalloc: device %d is beyond the %d devices it serves", dev,
 		kNoallocMaxDevices);
 	std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-	if (!g_noalloc_ptr[dev]) {
+	NoallocSlot &slot = g_noalloc_slot[dev];
+	unsigned long long id = noalloc_context_id();
+	if (id == 0 || slot.ptr == nullptr || slot.ctx_id != id) {
 		void *p = nullptr;
+		// also makes the device's primary context current if nothing had yet
 		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
 		if (e != cudaSuccess || p == nullptr) {
 			set_error("alpb_mxv_dense_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
 				cudaGetErrorString(e));
 			return ALPB_PANIC;
 		}
-		g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+		slot.ptr = static_cast<unsigned char *>(p);
+		slot.ctx_id = noalloc_context_id();   // 0 keeps the next call resolving again
 	}
-	*out = g_noalloc_ptr[dev];
+	*out = slot.ptr;
 	return ALPB_SUCCESS;
 }
 
@@ -125,8 +169,14 @@ extern "C" int alpb_mxv_dense_noalloc(int ring, int form, int64_t m_out, int64_t
 	ALPB_CHECK(m_out + nnz <= kNoallocMaxItems, ALPB_ILLEGAL,
 		"alpb_mxv_dense_noalloc: rows + nonzeroes = %lld exceeds the fixed scratch limit of %lld "
 		"(use alpb_mxv with a plan)", (long long) (m_out + nnz), (long long) kNoallocMaxItems);
-	ALPB_CHECK(u != v || u == nullptr, ALPB_OVERLAP,
-		"alpb_mxv_dense_noalloc: output and input vectors overlap");
+	{
+		// u holds m_out elements and v holds n_in: any shared byte is an overlap
+		const size_t es = type_size(ring_value_type(ring));
+		const uintptr_t ub = reinterpret_cast<uintptr_t>(u), vb = reinterpret_cast<uintptr_t>(v);
+		const uintptr_t ue = ub + size_t(m_out) * es, ve = vb + size_t(n_in) * es;
+		ALPB_CHECK(!(u && v && m_out > 0 && n_in > 0 && ub < ve && vb < ue), ALPB_OVERLAP,
+			"alpb_mxv_dense_noalloc: output and input vectors overlap");
+	}
 	if (m_out == 0 || nnz == 0 || n_in == 0) return ALPB_SUCCESS;  // no row gets a value
 	ALPB_CHECK(offsets && indices && u && v, ALPB_ILLEGAL, "alpb_mxv_dense_noalloc: null pointer");
 	unsigned char *base = nullptr;

@@ -300,8 +300,10 @@ ALPB_API int alpb_mxv(int ring, uint32_t descr, int form,
  * library (held by every GPU that loads it, until the process exits), so the
  * caller passes no plan and no scratch.  Limit: m_out + nnz <= 268,435,456
  * (131,072 tiles of 2048 merge items); larger inputs return ALPB_ILLEGAL with
- * an error message.  The first call on a device resolves the array's address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * an error message.  u and v may not share any byte (ALPB_OVERLAP).  The
+ * first call on a device resolves the array's address (cudaGetSymbolAddress),
+ * and so does the first call in a new context of that device (after
+ * cudaDeviceReset), so make that first call before any stream capture.
  * Every call, from any thread or stream, shares the one array: calls that
  * overlap in time on one device race and give wrong results; serialise them.
  */

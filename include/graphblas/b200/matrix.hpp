@@ -129,7 +129,10 @@ namespace grb {
 				init( rows, columns, nz );
 			}
 
-			Matrix( const size_t rows, const size_t columns ) : Matrix( rows, columns, 0 ) {}
+			/** Default capacity max( rows, columns ), as the reference's
+			 *  (reference/matrix.hpp:2110-2116). */
+			Matrix( const size_t rows, const size_t columns ) :
+				Matrix( rows, columns, rows > columns ? rows : columns ) {}
 
 			Matrix( const Matrix &o ) {
 				_m = o._m; _n = o._n; _cap = o._cap; _nz = o._nz;
@@ -233,39 +236,57 @@ namespace grb {
 
 			// ---- backend-internal access ----
 			/** This matrix becomes A: both orientations copied on the device, A's
-			 *  values cast to D (reference/io.hpp set( Matrix, Matrix )); a pattern
-			 *  (void) target keeps the structure only.  Values cannot come from a
-			 *  pattern A (UNSUPPORTED). */
+			 *  values cast to D (reference/io.hpp set( Matrix, Matrix ), execute
+			 *  phase of internal::set_copy, :1520-1548); a pattern (void) target
+			 *  keeps the structure only.  Values cannot come from a pattern A
+			 *  (UNSUPPORTED).  As in the reference: nothing happens for an empty
+			 *  dimension, an A without nonzeroes clears this matrix, and an A with
+			 *  more nonzeroes than this matrix's capacity clears it and returns
+			 *  ILLEGAL (only the RESIZE phase reserves).  A failed device copy also
+			 *  leaves this matrix cleared, with the error returned. */
 			template< typename D2, typename R2, typename C2, typename N2 >
 			RC b200_assign_from( const Matrix< D2, b200, R2, C2, N2 > &A ) {
 				using namespace internal::b200rt;
 				const int dt = type_code< D >::value, st = type_code< D2 >::value;
 				if( dt < 0 || st < 0 || ( dt != ALPB_VOID && st == ALPB_VOID ) ) { return UNSUPPORTED; }
 				const size_t m = A.b200_rows(), n = A.b200_cols(), nz = A.b200_nnz();
+				if( m == 0 || n == 0 ) { return SUCCESS; }
+				if( nz == 0 ) {
+					b200_clear();
+					return SUCCESS;
+				}
+				if( nz > _cap ) {
+					b200_clear();
+					return ILLEGAL;
+				}
 				_crs.release_all();
 				_ccs.release_all();
-				init( m, n, nz > _cap ? nz : _cap );
+				init( m, n, _cap );
 				RC rc = SUCCESS;
+				const auto keep = [&]( const RC r ) { if( rc == SUCCESS ) { rc = r; } };
 				const auto one = [&]( storage_t &dst, const typename Matrix< D2, b200, R2, C2, N2 >::storage_t
 					&src, const size_t outer ) {
-					(void) alpb_memcpy_d2d( dst.offsets, src.offsets, ( outer + 1 ) * 8, stream() );
-					if( nz == 0 ) { return; }
+					keep( check( alpb_memcpy_d2d( dst.offsets, src.offsets, ( outer + 1 ) * 8, stream() ),
+						"set (matrix offsets)" ) );
 					dst.indices = alloc< uint32_t >( nz );
-					(void) alpb_memcpy_d2d( dst.indices, src.indices, nz * 4, stream() );
+					keep( check( alpb_memcpy_d2d( dst.indices, src.indices, nz * 4, stream() ),
+						"set (matrix indices)" ) );
 					if( dt == ALPB_VOID ) { return; }
 					dst.values = alloc< storage_type >( nz );
-					const RC r = check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0, 0,
+					keep( check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0, 0,
 						static_cast< int64_t >( nz ), dst.values, dt, nullptr, nullptr, nullptr, nullptr,
 						ALPB_VOID, 0, src.values, st, nullptr, 0.0, nullptr, st, nullptr, 0.0, stream() ),
-						"set (matrix)" );
-					if( rc == SUCCESS ) { rc = r; }
+						"set (matrix values)" ) );
 				};
 				one( _crs, A.b200_crs(), m );
 				one( _ccs, A.b200_ccs(), n );
-				const RC s = check( alpb_stream_sync( stream() ), "set (matrix)" );
-				if( rc == SUCCESS ) { rc = s; }
-				if( rc == SUCCESS ) { _nz = nz; }
-				return rc;
+				keep( check( alpb_stream_sync( stream() ), "set (matrix)" ) );
+				if( rc != SUCCESS ) {
+					b200_clear();
+					return rc;
+				}
+				_nz = nz;
+				return SUCCESS;
 			}
 
 			size_t b200_rows() const noexcept { return _m; }

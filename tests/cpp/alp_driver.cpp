@@ -13,10 +13,13 @@
  * uint8 assigned[length] (length 0 = absent).
  *   op 0: mxv, 1: vxm, 2: conjugate_gradient (u = x0, v = b), 3: simple_pagerank,
  *   op 4: BLAS1 script on u, v (dot, folds, eWiseApply, eWiseMul, eWiseMulAdd, set)
+ *   op 5: matrix-to-matrix set and ALP's capacity contract (default capacity,
+ *         too small a capacity, the RESIZE phase, an empty source)
  *   ring 0: plus-times double, 1: lor-land bool, 2: min-plus int
  */
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <fstream>
 #include <iostream>
 #include <memory>
@@ -219,6 +222,47 @@ static RC run_blas1( const Case &c ) {
 	return SUCCESS;
 }
 
+template< typename T >
+static void print_matrix( const char *tag, const Matrix< T > &A ) {
+	std::vector< std::pair< std::pair< size_t, size_t >, double > > e;
+	for( const auto &t : A ) {
+		e.push_back( std::make_pair( std::make_pair( t.first.first, t.first.second ),
+			static_cast< double >( t.second ) ) );
+	}
+	std::sort( e.begin(), e.end() );
+	std::printf( "%s nnz %zu\n", tag, e.size() );
+	for( size_t k = 0; k < e.size(); ++k ) {
+		std::printf( "%s %zu %.17g\n", tag, k, e[ k ].second );
+		std::printf( "%s_row %zu %zu\n", tag, k, e[ k ].first.first );
+		std::printf( "%s_col %zu %zu\n", tag, k, e[ k ].first.second );
+	}
+}
+
+static RC run_matrix_set( const Case &c ) {
+	Matrix< double > A( c.m, c.n, c.nnz > 0 ? c.nnz : 1 );
+	RC rc = buildMatrixUnique( A, c.I.data(), c.J.data(), c.V.data(), c.nnz, SEQUENTIAL );
+	std::printf( "rc_build %d\nnnz_A %zu\n", int( rc ), nnz( A ) );
+	// the default capacity is max( rows, columns )
+	Matrix< double > D( c.m, c.n );
+	std::printf( "cap_default_ok %d\n", int( capacity( D ) >= std::max( c.m, c.n ) ) );
+	// too small a capacity: ILLEGAL, and the target is cleared
+	Matrix< double > C( c.m, c.n, 1 );
+	rc = buildMatrixUnique( C, c.I.data(), c.J.data(), c.V.data(), 1, SEQUENTIAL );
+	std::printf( "rc_build_C %d\nnnz_C0 %zu\n", int( rc ), nnz( C ) );
+	std::printf( "rc_set_small %d\n", int( set( C, A ) ) );
+	std::printf( "nnz_C_small %zu\n", nnz( C ) );
+	// RESIZE reserves; EXECUTE then copies
+	std::printf( "rc_set_resize %d\n", int( set( C, A, RESIZE ) ) );
+	std::printf( "cap_C_ok %d\n", int( capacity( C ) >= nnz( A ) ) );
+	std::printf( "rc_set %d\n", int( set( C, A ) ) );
+	print_matrix( "C", C );
+	// an empty source clears the target
+	Matrix< double > E( c.m, c.n );
+	std::printf( "rc_set_empty %d\n", int( set( C, E ) ) );
+	std::printf( "nnz_C_empty %zu\n", nnz( C ) );
+	return SUCCESS;
+}
+
 int main( int argc, char **argv ) {
 	if( argc != 2 ) {
 		std::cerr << "usage: " << argv[ 0 ] << " <case file>\n";
@@ -246,6 +290,8 @@ int main( int argc, char **argv ) {
 		rc = run_cg( c );
 	} else if( c.op == 3 ) {
 		rc = run_pagerank( c );
+	} else if( c.op == 5 ) {
+		rc = run_matrix_set( c );
 	} else {
 		rc = run_blas1( c );
 	}

@@ -237,6 +237,28 @@ def test_driver_pagerank_matches_reference(cuda, oracle):
         compare(f, 1e-9)
 
 
+def test_driver_matrix_set_capacity_matches_reference(cuda, oracle):
+    """Matrix-to-matrix set under ALP's capacity contract, against the
+    reference build: the default capacity is max(rows, columns); a source
+    with more nonzeroes than the target's capacity returns ILLEGAL and clears
+    the target (reference/io.hpp set_copy); the RESIZE phase reserves and
+    the EXECUTE phase then copies; an empty source clears the target."""
+    from oracle.oracle import crs_to_coo
+    rp, col, vals = oracle.rmat(7, edge_factor=6, seed=91, vtype=3)
+    I, J = crs_to_coo(rp, col)
+    n = len(rp) - 1
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "case.bin"
+        write_case(f, 5, 0, 0, n, n, I, J, vals)
+        compare(f, 0.0)
+        r = _run(B200_BIN / "alp_driver_b200", f)
+    out = parse(r.stdout)
+    assert out[("rc_set_small", None)] == 7          # ILLEGAL
+    assert out[("nnz_C_small", None)] == 0
+    assert out[("rc_set", None)] == 0 and out[("C", "nnz")] == len(I)
+    assert out[("nnz_C_empty", None)] == 0
+
+
 # ------------------------------------------------------------------ HPCG --
 def _hpcg_result(out: str):
     import re
