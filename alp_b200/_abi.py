@@ -111,6 +111,7 @@ PROTOS: dict[str, list] = {
     "alpb_vec_reduce": [PD, I32, D, I32, U32, I64, P, I32, P, P, I32, P, P, P, I32, I32, P],
     "alpb_cg_solve": [I64, P, P, P, P, P, I64, D, PI64, PD, P, P, P],
     "alpb_pagerank": [I64, P, P, P, P, P, P, P, I32, D, D, I64, PI64, PD, P],
+    "alpb_pagerank_planned": [I64, P, P, P, P, P, P, P, I32, D, D, I64, PI64, PD, P, P, P],
     "alpb_sddmm": [P, I64, I64, P, P, P, P, D, P, P],
     "alpb_cg_adjoint": [I64, P, P, P, P, P, P, P, P, P, P, I64, D, PI64, PD, P, P, P],
     "alpb_cg_grad": [I64, P, P, P, P, P, P, P, P, P, P, P, P, I64, D, PD, PI64, PI64, P, P, P],

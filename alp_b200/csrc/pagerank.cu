@@ -170,35 +170,35 @@ __global__ void __launch_bounds__(32 * PR_WARPS, 6) k_pagerank(PrArgs a) {
 	}
 }
 
-} // namespace alpb
-
-using namespace alpb;
-
-extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32_t *crs_col_idx,
-	const double *crs_values, const int64_t *ccs_col_ptr, const uint32_t *ccs_row_idx,
-	const double *ccs_values, double *pr, int init_given, double alpha, double conv,
-	int64_t max_iter, int64_t *iterations, double *residual, void *stream) {
-	(void) crs_col_idx;
-	ALPB_CHECK(alpha > 0 && alpha < 1, ALPB_ILLEGAL, "alpb_pagerank: alpha must be in (0, 1)");
-	ALPB_CHECK(max_iter > 0, ALPB_ILLEGAL, "alpb_pagerank: max must be positive");
-	ALPB_CHECK(iterations && residual, ALPB_ILLEGAL, "alpb_pagerank: null output");
-	ALPB_CHECK(n > 0, ALPB_ILLEGAL, "alpb_pagerank: empty graph");
-	cudaStream_t s = as_stream(stream);
-	int64_t nnz = 0;
-	ALPB_CUDA(cudaMemcpyAsync(&nnz, ccs_col_ptr + n, 8, cudaMemcpyDeviceToHost, s));
-	ALPB_CUDA(cudaStreamSynchronize(s));
-	alpb_spmv_plan plan = nullptr;
-	int rc = plan_create_tiles(&plan, n, nnz, ccs_col_ptr, ALPB_SCHED_MERGE_PATH, 0, WM_TILE, s);
-	if (rc != ALPB_SUCCESS) return rc;
+// The solve proper.  plan: a WM_TILE plan of the CCS offsets, or null (one is
+// made and destroyed here); work: 3n doubles of scratch, or null.
+static int pagerank_run(int64_t n, const int64_t *crs_row_ptr, const double *crs_values,
+	const int64_t *ccs_col_ptr, const uint32_t *ccs_row_idx, const double *ccs_values, double *pr,
+	int init_given, double alpha, double conv, int64_t max_iter, int64_t *iterations,
+	double *residual, double *work, alpb_spmv_plan plan, cudaStream_t s) {
+	alpb_spmv_plan own_plan = nullptr;
+	if (!plan) {
+		int64_t nnz = 0;
+		ALPB_CUDA(cudaMemcpyAsync(&nnz, ccs_col_ptr + n, 8, cudaMemcpyDeviceToHost, s));
+		ALPB_CUDA(cudaStreamSynchronize(s));
+		int rc = plan_create_tiles(&own_plan, n, nnz, ccs_col_ptr, ALPB_SCHED_MERGE_PATH, 0,
+			WM_TILE, s);
+		if (rc != ALPB_SUCCESS) return rc;
+		plan = own_plan;
+	}
 	const int grid = solver_grid(k_pagerank, 32 * PR_WARPS, plan->ntiles, PR_WARPS);
 	if (grid <= 0) {
-		alpb_spmv_plan_destroy(plan);
+		alpb_spmv_plan_destroy(own_plan);
 		set_error("alpb_pagerank: no cooperative occupancy");
 		return ALPB_PANIC;
 	}
-	double *scratch = nullptr;
+	double *vecs = work, *own_vecs = nullptr, *blk = nullptr;
 	PrState *st = nullptr;
-	ALPB_CUDA(cudaMallocAsync(&scratch, size_t(3 * n + 5 * int64_t(grid)) * 8, s));
+	if (!vecs) {
+		ALPB_CUDA(cudaMallocAsync(&own_vecs, size_t(3 * n) * 8, s));
+		vecs = own_vecs;
+	}
+	ALPB_CUDA(cudaMallocAsync(&blk, size_t(5 * int64_t(grid)) * 8, s));
 	ALPB_CUDA(cudaMallocAsync(&st, sizeof(PrState), s));
 	ALPB_CUDA(cudaMemsetAsync(st, 0, sizeof(PrState), s));
 	PrArgs a;
@@ -209,10 +209,10 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 	a.crs_ptr = crs_row_ptr;
 	a.crs_val = crs_values;
 	a.pr = pr;
-	a.rs = scratch;
-	a.next0 = scratch + n;
-	a.next1 = scratch + 2 * n;
-	a.blk = scratch + 3 * n;
+	a.rs = vecs;
+	a.next0 = vecs + n;
+	a.next1 = vecs + 2 * n;
+	a.blk = blk;
 	a.n = n;
 	a.max_iter = max_iter;
 	a.alpha = alpha;
@@ -225,10 +225,11 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 	ALPB_LAUNCHED();
 	PrState h;
 	ALPB_CUDA(cudaMemcpyAsync(&h, st, sizeof(PrState), cudaMemcpyDeviceToHost, s));
-	ALPB_CUDA(cudaFreeAsync(scratch, s));
+	ALPB_CUDA(cudaFreeAsync(blk, s));
 	ALPB_CUDA(cudaFreeAsync(st, s));
+	if (own_vecs) ALPB_CUDA(cudaFreeAsync(own_vecs, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
-	alpb_spmv_plan_destroy(plan);
+	alpb_spmv_plan_destroy(own_plan);
 	ALPB_CHECK(h.gs.err == 0, ALPB_PANIC, "alpb_pagerank: a grid barrier or tile wait timed out");
 	*iterations = h.iterations;
 	*residual = h.residual;
@@ -238,4 +239,45 @@ extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32
 		return ALPB_FAILED;
 	}
 	return ALPB_SUCCESS;
+}
+
+static int pagerank_checks(int64_t n, double alpha, int64_t max_iter, const int64_t *iterations,
+	const double *residual) {
+	ALPB_CHECK(alpha > 0 && alpha < 1, ALPB_ILLEGAL, "alpb_pagerank: alpha must be in (0, 1)");
+	ALPB_CHECK(max_iter > 0, ALPB_ILLEGAL, "alpb_pagerank: max must be positive");
+	ALPB_CHECK(iterations && residual, ALPB_ILLEGAL, "alpb_pagerank: null output");
+	ALPB_CHECK(n > 0, ALPB_ILLEGAL, "alpb_pagerank: empty graph");
+	return ALPB_SUCCESS;
+}
+
+} // namespace alpb
+
+using namespace alpb;
+
+extern "C" int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32_t *crs_col_idx,
+	const double *crs_values, const int64_t *ccs_col_ptr, const uint32_t *ccs_row_idx,
+	const double *ccs_values, double *pr, int init_given, double alpha, double conv,
+	int64_t max_iter, int64_t *iterations, double *residual, void *stream) {
+	(void) crs_col_idx;
+	const int rc = pagerank_checks(n, alpha, max_iter, iterations, residual);
+	if (rc != ALPB_SUCCESS) return rc;
+	return pagerank_run(n, crs_row_ptr, crs_values, ccs_col_ptr, ccs_row_idx, ccs_values, pr,
+		init_given, alpha, conv, max_iter, iterations, residual, nullptr, nullptr,
+		as_stream(stream));
+}
+
+extern "C" int alpb_pagerank_planned(int64_t n, const int64_t *crs_row_ptr,
+	const uint32_t *crs_col_idx, const double *crs_values, const int64_t *ccs_col_ptr,
+	const uint32_t *ccs_row_idx, const double *ccs_values, double *pr, int init_given,
+	double alpha, double conv, int64_t max_iter, int64_t *iterations, double *residual,
+	double *work, alpb_spmv_plan ccs_plan, void *stream) {
+	(void) crs_col_idx;
+	const int rc = pagerank_checks(n, alpha, max_iter, iterations, residual);
+	if (rc != ALPB_SUCCESS) return rc;
+	ALPB_CHECK(!ccs_plan || (ccs_plan->m == n && ccs_plan->offsets == ccs_col_ptr &&
+			ccs_plan->tile == WM_TILE), ALPB_MISMATCH,
+		"alpb_pagerank_planned: plan was made for another storage");
+	return pagerank_run(n, crs_row_ptr, crs_values, ccs_col_ptr, ccs_row_idx, ccs_values, pr,
+		init_given, alpha, conv, max_iter, iterations, residual, work, ccs_plan,
+		as_stream(stream));
 }

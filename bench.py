@@ -262,10 +262,15 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
     traffic = profiled_traffic(kernel_tag)
     achieved = nbytes / (ms * 1e-3) / 1e9
     extra = {}
+    cpu = rank == 0 and world == 1 and not args.no_cpu
     # secondary workloads: one GPU only (with replicas the other ranks would
     # wait at the final barrier for as long as they run)
     if rank == 0 and world == 1 and not args.no_extra:
-        extra = extra_workloads(args, A, plan)
+        extra = extra_workloads(args, A, plan, cpu)
+    cpu_line = None
+    if cpu:
+        o, i, v = A.to_host()
+        cpu_line = cpu_baseline_sample(o, i, v, x.cpu().numpy(), args.scale)
     result = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 5),
@@ -292,6 +297,8 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
     }
     if extra:
         result["extra"] = extra
+    if cpu_line is not None:
+        result["cpu_baseline"] = cpu_line
     return result
 
 
@@ -309,10 +316,13 @@ def timed(fn, reps: int, stream):
     return e0.elapsed_time(e1) / reps
 
 
-def extra_workloads(args, A, plan) -> dict:
+def extra_workloads(args, A, plan, cpu: bool) -> dict:
     """Secondary workloads of the same sweep, timed the same way (not part of
     `value`): boolean lor/land with a 50% dense output mask, int32 min-plus,
-    simple_pagerank on the scale-22 pattern, CG on the 27-point 32^3 grid."""
+    simple_pagerank on the scale-22 pattern, CG on the 27-point 32^3 grid,
+    batched CG, HPCG, the differentiated CG and personalised PageRank.  With
+    `cpu`, the unmodified reference_omp backend is timed beside CG, PageRank,
+    batched CG and HPCG on the host cores."""
     import ctypes as C
     import torch
     from alp_b200 import _abi as abi
@@ -355,12 +365,29 @@ def extra_workloads(args, A, plan) -> dict:
                                          dev.ptr(L.values), dev.ptr(LT.offsets), dev.ptr(LT.indices),
                                          dev.ptr(LT.values), dev.ptr(pr), 0, 0.85, 1e-9, 1000,
                                          C.byref(it), C.byref(res), dev.stream_ptr())
-    ms = timed(pagerank, 2, stream)   # one call: plan, setup and every iteration
+    ms_call = timed(pagerank, 2, stream)   # one call: plan, set-up and every iteration
+    # the same solve with the plan of the CCS and the scratch vectors made
+    # beforehand (what a caller that solves repeatedly on one graph does):
+    # one cooperative launch for the out-degrees and every iteration
+    pplan = dev.Plan(LT, sched=abi.SCHED_MERGE_PATH)
+    pwork = torch.empty(3 * A.n, dtype=torch.float64, device="cuda")
+
+    def pagerank_planned():
+        prc[0] = abi.lib().alpb_pagerank_planned(
+            L.m, dev.ptr(L.offsets), dev.ptr(L.indices), dev.ptr(L.values), dev.ptr(LT.offsets),
+            dev.ptr(LT.indices), dev.ptr(LT.values), dev.ptr(pr), 0, 0.85, 1e-9, 1000,
+            C.byref(it), C.byref(res), dev.ptr(pwork), pplan.h, dev.stream_ptr())
+    ms = timed(pagerank_planned, 3, stream)
     per_iter = (A.nnz * 12 + (A.n + 1) * 8 + 6 * A.n * 8)
     out["pagerank_rmat22"] = {"rc": prc[0], "iterations": it.value, "residual": res.value,
-                              "ms_per_call": round(ms, 3),
+                              "ms_per_solve": round(ms, 3),
                               "ms_per_iter": round(ms / max(it.value, 1), 4),
-                              "GB/s": round(per_iter * it.value / ms / 1e6, 1)}
+                              "ms_per_call_with_setup": round(ms_call, 3),
+                              "GB/s": round(per_iter * it.value / ms / 1e6, 1),
+                              "bytes_per_iteration": per_iter}
+    if cpu:
+        out["pagerank_rmat22"]["cpu_reference_omp"] = cpu_pagerank(L, ms)
+    del pplan, pwork
     del L, LT, pr
     # plain CG, 27-point 32^3 (the reference's CPU-runnable configuration)
     S = dev.stencil((32, 32, 32), 26.0, -1.0)
@@ -381,9 +408,11 @@ def extra_workloads(args, A, plan) -> dict:
                          "ms_per_solve": round(ms, 4),
                          "us_per_iteration": round(1e3 * ms / max(it.value, 1), 2),
                          "err_vs_ones_inf": float((x - 1).abs().max().item())}
+    if cpu:
+        out["cg_27pt_32"]["cpu_reference_omp"] = cpu_cg(S, b, ms)
     del S, ps, work
-    out["batched_cg"] = batched_cg_workload(stream)
-    out["hpcg_256"] = hpcg_workload(stream)
+    out["batched_cg"] = batched_cg_workload(stream, cpu=cpu)
+    out["hpcg_256"] = hpcg_workload(stream, cpu=cpu)
     out["adjoint_cg"] = adjoint_workload(stream)
     out["ppr_rmat24"] = ppr_workload(stream)
     # each rate next to its fraction of the measured HBM copy bandwidth
@@ -394,7 +423,7 @@ def extra_workloads(args, A, plan) -> dict:
     return out
 
 
-def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024) -> dict:
+def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024, cpu: bool = False) -> dict:
     """256 shifted 2-D 5-point Poisson systems, sides log-uniform in [32, 512],
     shift U(0.01, 1), b ~ N(0, 1), relative tolerance 1e-8, FP64: one
     graph-captured persistent launch against one alpb_cg_solve launch per
@@ -471,6 +500,32 @@ def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024) -> dict:
     # temp and writes x, r)
     per_iter = 12 * nnzs + 8 * (rows + 1) + 80 * rows
     moved = float((it * per_iter).sum())
+    cpu_res = None
+    if cpu:
+        # reference_omp solving the 256 systems one after the other (the same
+        # matrices and right-hand sides, copied from the device)
+        from oracle.oracle import crs_to_coo
+        ref = reference_omp()
+        if ref is None:
+            cpu_res = _cpu_unavailable()
+        else:
+            hrp, hci, hva = rp.cpu().numpy(), ci.cpu().numpy().view(np.uint32), va.cpu().numpy()
+            hb = b.cpu().numpy()
+            tot, its = 0.0, 0
+            for k in range(nseg):
+                r0, r1 = int(seg_rows[k]), int(seg_rows[k + 1])
+                srp = hrp[r0:r1 + 1] - hrp[r0]
+                I, J = crs_to_coo(srp, (hci[hrp[r0]:hrp[r1]].astype(np.int64) - r0)
+                                  .astype(np.uint32))
+                rcs, _, itk, _, ms_k = ref.cg(r1 - r0, I, J, hva[hrp[r0]:hrp[r1]], hb[r0:r1],
+                                              np.zeros(r1 - r0), max_iter, tol)
+                tot += ms_k
+                its += itk
+            cpu_res = {"ms": round(tot, 1), "iterations_sum": its, "threads": ref.threads(),
+                       "solves_per_s": round(nseg / (tot * 1e-3), 1),
+                       "gpu_batched_speedup": round(tot / ms_b, 1),
+                       "sample": "the whole workload: conjugate_gradient on each of the 256 "
+                                 "systems in turn, solves alone timed"}
     return {"systems": nseg, "rows": n, "nnz": nnz, "tol": tol, "rc": rc,
             "all_converged": bool(conv.all()), "iterations_max": int(it.max()),
             "iterations_sum": int(it.sum()), "plain_iterations_sum": int(itp.sum()),
@@ -480,14 +535,13 @@ def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024) -> dict:
             "speedup": round(ms_p / ms_b, 2),
             "batched_GB/s": round(moved / ms_b / 1e6, 1),
             "plain_GB/s": round(moved / ms_p / 1e6, 1),
-            "max_rel_diff_batched_vs_plain": diff}
+            "max_rel_diff_batched_vs_plain": diff,
+            **({"cpu_reference_omp": cpu_res} if cpu_res else {})}
 
 
-def hpcg_workload(stream, side: int = 256, coarse_levels: int = 3, nrhs: int = 8) -> dict:
-    """HPCG on the 27-point 256^3 system (diagonal 26, off-diagonals -1) with
-    three coarser levels (128^3, 64^3, 32^3), 27 static colours, one pre- and
-    one post-smoothing step, 8 right-hand sides ~ N(0, 1) solved together,
-    relative tolerance 1e-9, FP64 (alpb_hpcg_solve)."""
+def _hpcg_gpu(stream, side, coarse_levels, nrhs, seed):
+    """One device HPCG solve of `nrhs` right-hand sides ~ N(0, 1) on the
+    side^3 system; returns (ms, iterations, residuals, rows, nnz, levels, fused)."""
     import ctypes as C
     import torch
     from alp_b200 import _abi as abi
@@ -499,7 +553,7 @@ def hpcg_workload(stream, side: int = 256, coarse_levels: int = 3, nrhs: int = 8
     lv, n, nnz, fused = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int()
     abi.call("alpb_hpcg_info", h, C.byref(lv), C.byref(n), C.byref(nnz), C.byref(fused))
     b = torch.empty(n.value * nrhs, dtype=torch.float64, device="cuda")
-    abi.call("alpb_gen_normal", dev.ptr(b), n.value * nrhs, 31, 1, sp)
+    abi.call("alpb_gen_normal", dev.ptr(b), n.value * nrhs, seed, 1, sp)
     x = torch.zeros_like(b)
     it = (C.c_int64 * nrhs)()
     res = (C.c_double * nrhs)()
@@ -508,27 +562,58 @@ def hpcg_workload(stream, side: int = 256, coarse_levels: int = 3, nrhs: int = 8
         x.zero_()
         abi.call("alpb_hpcg_solve", h, dev.ptr(b), dev.ptr(x), 1, 1, 1, 500, 1e-9, it, res, sp)
     ms = timed(solve, 1, stream)
-    iters = max(it)
-    # algorithmic bytes of one CG iteration.  A smoother sweep runs the 27
-    # colours one after the other; a colour step reads its slice of the
-    # matrix, gathers x at the rows' neighbours (26 of the 27 colours
-    # neighbour it, so nearly all of x: 8 nrhs n bytes, which exceeds the L2
-    # at 256^3) and reads r and reads/writes x on its own rows.  Per V-cycle
-    # the finest level runs four sweeps (forward and backward, before and
-    # after the coarse correction); the CG adds one product and about ten
-    # vector passes; each coarser level adds about 1/8 of the finest.
-    vec = 8 * nrhs * n.value
-    sweep = 12 * nnz.value + 8 * (n.value + 1) + 27 * vec + 3 * vec
-    fine = 4 * sweep + (12 * nnz.value + 8 * (n.value + 1) + 2 * vec) + 10 * vec
-    per_iter = fine * 8 / 7
     abi.lib().alpb_hpcg_destroy(h)
-    return {"rows": n.value, "nnz": nnz.value, "levels": lv.value, "rhs": nrhs,
-            "fused_smoother": bool(fused.value), "iterations": list(it),
-            "residuals": [float(r) for r in res], "ms_per_solve": round(ms, 2),
-            "ms_per_iteration": round(ms / max(iters, 1), 3),
-            "solves_per_s": round(nrhs / (ms * 1e-3), 3),
-            "GB/s": round(per_iter * iters / ms / 1e6, 1),
-            "bytes_per_iteration": int(per_iter)}
+    return ms, list(it), [float(r) for r in res], n.value, nnz.value, lv.value, fused.value
+
+
+def hpcg_workload(stream, side: int = 256, coarse_levels: int = 3, nrhs: int = 8,
+                  cpu: bool = False) -> dict:
+    """HPCG on the 27-point 256^3 system (diagonal 26, off-diagonals -1) with
+    three coarser levels (128^3, 64^3, 32^3), 27 static colours, one pre- and
+    one post-smoothing step, 8 right-hand sides ~ N(0, 1) solved together,
+    relative tolerance 1e-9, FP64 (alpb_hpcg_solve).  With `cpu`, ALP's own
+    hpcg on reference_omp at 64^3 (one right-hand side; 256^3 takes the host
+    minutes) beside the device at 64^3 with 8 right-hand sides."""
+    ms, it, res, n, nnz, lv, fused = _hpcg_gpu(stream, side, coarse_levels, nrhs, 31)
+    iters = max(it)
+    # algorithmic bytes of one CG iteration.  A smoother sweep must read the
+    # matrix once, x once, r once and write x once (8 nrhs n bytes per vector
+    # pass); per V-cycle the finest level runs four sweeps (forward and
+    # backward, before and after the coarse correction), the CG adds one
+    # product and about ten vector passes, and each coarser level adds about
+    # 1/8 of the finest.  The device's colour steps gather x at the rows'
+    # neighbours once per colour (26 of the 27 colours neighbour each row),
+    # so they move about 27 copies of x per sweep: that delivered rate is
+    # reported apart.
+    vec = 8 * nrhs * n
+    mat = 12 * nnz + 8 * (n + 1)
+    fine = 4 * (mat + 3 * vec) + (mat + 3 * vec) + 10 * vec
+    per_iter = fine * 8 / 7
+    gathered = (4 * (mat + 30 * vec) + (mat + 3 * vec) + 10 * vec) * 8 / 7
+    out = {"rows": n, "nnz": nnz, "levels": lv, "rhs": nrhs,
+           "fused_smoother": bool(fused), "iterations": it,
+           "residuals": res, "ms_per_solve": round(ms, 2),
+           "ms_per_iteration": round(ms / max(iters, 1), 3),
+           "solves_per_s": round(nrhs / (ms * 1e-3), 3),
+           "GB/s": round(per_iter * iters / ms / 1e6, 1),
+           "bytes_per_iteration": int(per_iter),
+           "gathered_GB/s": round(gathered * iters / ms / 1e6, 1)}
+    if cpu:
+        ref = reference_omp()
+        if ref is None:
+            out["cpu_reference_omp"] = _cpu_unavailable()
+        else:
+            ms64, it64, _, _, _, _, _ = _hpcg_gpu(stream, 64, 3, 8, 32)
+            b = np.random.default_rng(64).standard_normal(64 ** 3)
+            rc, _, itc, _, msc, _ = ref.hpcg(64, 3, 27, b, 500, 1e-9)
+            out["cpu_reference_omp"] = {
+                "rc": rc, "iterations": itc, "ms_per_rhs": round(msc, 1),
+                "threads": ref.threads(),
+                "gpu_64_ms_per_rhs": round(ms64 / 8, 2), "gpu_64_iterations": it64,
+                "gpu_speedup_64": round(msc / (ms64 / 8), 1),
+                "sample": "grb::algorithms::hpcg on 64^3 with 3 coarser levels, one right-hand "
+                          "side (the device at 64^3 solves 8 together; ms per right-hand side)"}
+    return out
 
 
 def adjoint_workload(stream, side: int = 64) -> dict:
@@ -681,32 +766,78 @@ def reference_arm(args) -> dict:
     }
 
 
-def cpu_baseline_sample() -> dict | None:
-    """reference_omp on a bounded sample of the workload: the same generator
-    at scale 20 (1/4 of the rows), all host threads."""
+def reference_omp():
+    """The unmodified reference_omp backend (oracle/_ref), or None."""
     try:
-        from oracle.oracle import FP64, REF_OMP_SO, Reference, Restatement, crs_to_coo
+        from oracle.oracle import REF_OMP_SO, Reference
         if not REF_OMP_SO.exists():
             return None
         os.environ.setdefault("OMP_PROC_BIND", "true")
-        R = Restatement()
-        rp, col, vals = R.rmat(20, EDGE_FACTOR, seed=SEED, vtype=FP64)
-        n = len(rp) - 1
-        I, J = crs_to_coo(rp, col)
-        x = R.values(n, FP64, SEED + 7)
-        u = np.zeros(n)
-        ref = Reference(omp=True)
-        rc, ms = ref.mxv(0, 0, 0, n, n, I, J, vals, u, None, x, reps=20)
-        if rc != 0:
-            return None
-        nb = algorithmic_bytes(n, n, len(col))
-        return {"value": round(nb / (ms * 1e-3) / 1e9, 2), "unit": "GB/s", "cores": ref.threads(),
-                "kind": "reference",
-                "sample": f"grb::mxv (reference_omp) on R-MAT scale 20 ({len(col)} nnz), "
-                          "same generator and seed, mean of 20 calls"}
-    except Exception as e:  # a missing checker must not break the GPU line
+        return Reference(omp=True)
+    except Exception:  # a missing checker must not break the GPU line
+        return None
+
+
+def _cpu_unavailable():
+    return {"ms": None, "sample": "unavailable: oracle/_ref/libalp_ref_omp.so not built"}
+
+
+def cpu_pagerank(L, gpu_ms) -> dict:
+    """grb::algorithms::simple_pagerank on reference_omp, same graph and
+    parameters (alpha 0.85, conv 1e-9); the solve alone is timed."""
+    from oracle.oracle import crs_to_coo
+    ref = reference_omp()
+    if ref is None:
+        return _cpu_unavailable()
+    o, i, v = L.to_host()
+    I, J = crs_to_coo(o, i)
+    rc, pr, it, ms = ref.pagerank(L.m, I, J, v, alpha=0.85, conv=1e-9, max_iter=1000)
+    return {"rc": rc, "iterations": it, "ms": round(ms, 1), "threads": ref.threads(),
+            "gpu_speedup": round(ms / gpu_ms, 1),
+            "sample": "the whole workload: simple_pagerank on the same scale-22 graph, one solve"}
+
+
+def cpu_cg(S, b, gpu_ms) -> dict:
+    """grb::algorithms::conjugate_gradient on reference_omp, same system and
+    parameters (x0 = 0, tol 1e-10, max 500); mean of 5 solves."""
+    from oracle.oracle import crs_to_coo
+    ref = reference_omp()
+    if ref is None:
+        return _cpu_unavailable()
+    o, i, v = S.to_host()
+    I, J = crs_to_coo(o, i)
+    hb = b.cpu().numpy()
+    tot, it = 0.0, 0
+    for _ in range(5):
+        rc, _, it, _, ms = ref.cg(S.m, I, J, v, hb, np.zeros(S.m), 500, 1e-10)
+        tot += ms
+    return {"rc": rc, "iterations": it, "ms": round(tot / 5, 3), "threads": ref.threads(),
+            "gpu_speedup": round(tot / 5 / gpu_ms, 1),
+            "sample": "the whole workload (27-point 32^3), mean of 5 solves"}
+
+
+def cpu_baseline_sample(o, i, v, xh, scale) -> dict:
+    """reference_omp grb::mxv on the benchmark's own matrix (copied from the
+    device), all host threads, mean of 20 calls (about 1-2 s of CPU work after
+    the reference's matrix build)."""
+    from oracle.oracle import crs_to_coo
+    ref = reference_omp()
+    if ref is None:
         return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": f"failed: {e}"}
+                "sample": "unavailable: oracle/_ref/libalp_ref_omp.so not built"}
+    n = len(o) - 1
+    I, J = crs_to_coo(o, i)
+    u = np.zeros(n)
+    rc, ms = ref.mxv(0, 0, 0, n, n, I, J, v, u, None, xh, reps=20)
+    if rc != 0:
+        return {"value": None, "unit": "GB/s", "cores": ref.threads(), "kind": "reference",
+                "sample": f"reference mxv returned rc={rc}"}
+    nb = algorithmic_bytes(n, n, len(i))
+    return {"value": round(nb / (ms * 1e-3) / 1e9, 2), "unit": "GB/s", "cores": ref.threads(),
+            "kind": "reference", "ms_per_step": round(ms, 3),
+            "sample": f"grb::mxv (reference_omp, {ref.threads()} threads) on the full R-MAT "
+                      f"scale-{scale} matrix ({len(i)} nnz, the same matrix copied from the "
+                      "device), mean of 20 calls"}
 
 
 def main():
@@ -757,8 +888,6 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     res = gpu_arm(args, rank, world, local_rank)
-    if rank == 0 and world == 1 and not args.no_cpu:
-        res["cpu_baseline"] = cpu_baseline_sample()
     if rank == 0:
         print(json.dumps(res), flush=True)
     if world > 1:

@@ -425,6 +425,18 @@ ALPB_API int alpb_pagerank(int64_t n, const int64_t *crs_row_ptr,
 	double *pr, int init_given, double alpha, double conv, int64_t max_iter,
 	int64_t *iterations, double *residual, void *stream);
 
+/* alpb_pagerank with caller-held state, so that repeated solves on one graph
+ * skip the set-up: ccs_plan is a plan of the CCS offsets made by
+ * alpb_spmv_plan_create (any schedule; the solver uses its merge-path tables),
+ * or NULL; work is 3n doubles of device scratch, or NULL.  ALPB_MISMATCH when
+ * the plan was made for other offsets.  (No counterpart in the reference: its
+ * simple_pagerank keeps such state in the caller's vectors.) */
+ALPB_API int alpb_pagerank_planned(int64_t n, const int64_t *crs_row_ptr,
+	const uint32_t *crs_col_idx, const double *crs_values, const int64_t *ccs_col_ptr,
+	const uint32_t *ccs_row_idx, const double *ccs_values, double *pr, int init_given,
+	double alpha, double conv, int64_t max_iter, int64_t *iterations, double *residual,
+	double *work, alpb_spmv_plan ccs_plan, void *stream);
+
 /* ======================================================================
  * HPCG: algorithms::hpcg (hpcg/hpcg.hpp:97-223) with its multigrid V-cycle
  * (hpcg/multigrid_v_cycle.hpp:67-246) and multi-colour Gauss-Seidel smoother

@@ -54,6 +54,16 @@ int alpo_pagerank(int64_t n, const int64_t *crs_row_ptr, const uint32_t *crs_col
 	const double *ccs_val, double *pr, int init_given, double alpha, double conv,
 	int64_t max_iter, int64_t *iterations, double *residual);
 
+/* ppr_oracle.c: the C form of oracle/ppr.py (row-major n x S vectors) */
+int alpo_ppr_forward(int64_t n, const int64_t *rp, const uint32_t *col, const double *w,
+	int64_t S, const int64_t *seeds, double alpha, double conv, int64_t max_iter, int x_given,
+	double *x, int64_t *iters, double *res);
+int alpo_ppr_adjoint(int64_t n, const int64_t *rp, const uint32_t *col, const double *w,
+	int64_t S, const int64_t *seeds, const double *g, double alpha, double conv,
+	int64_t max_iter, double *lam, int64_t *iters, double *res);
+int alpo_ppr_grad(int64_t n, const int64_t *rp, const uint32_t *col, const double *w,
+	int64_t S, const double *x, const double *lam, double alpha, double *grad);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,9 @@ class Restatement:
                                P, P, P, P, P, I32, I64, P, P, I64, P, P, I32, I64]
         L.alpo_cg.argtypes = [I64, P, P, P, P, P, I64, D, P, P]
         L.alpo_pagerank.argtypes = [I64, P, P, P, P, P, P, P, I32, D, D, I64, P, P]
+        L.alpo_ppr_forward.argtypes = [I64, P, P, P, I64, P, D, D, I64, I32, P, P, P]
+        L.alpo_ppr_adjoint.argtypes = [I64, P, P, P, I64, P, P, D, D, I64, P, P, P]
+        L.alpo_ppr_grad.argtypes = [I64, P, P, P, I64, P, P, D, P]
         self.L = L
 
     # --- generators (bit-identical to the device ones) ---
@@ -144,6 +147,53 @@ class Restatement:
                                   int(pr0 is not None), alpha, conv, max_iter, _p(it), _p(res))
         return rc, pr, int(it[0]), float(res[0])
 
+    # --- personalised PageRank (ppr_oracle.c: oracle/ppr.py in C, OpenMP) ---
+    @staticmethod
+    def _crs(rp, col, w):
+        return (np.ascontiguousarray(rp, np.int64), np.ascontiguousarray(col, np.uint32),
+                np.ascontiguousarray(w, np.float64))
+
+    def ppr_forward(self, rp, col, w, seeds, alpha=0.85, conv=1e-9, max_iter=1000, x0=None):
+        """Same contract as oracle.ppr.forward: (x [n, S], iterations, residuals)."""
+        rp, col, w = self._crs(rp, col, w)
+        n = len(rp) - 1
+        seeds = np.ascontiguousarray(seeds, np.int64)
+        S = len(seeds)
+        x = np.empty((n, S)) if x0 is None else np.array(x0, np.float64, copy=True, order="C")
+        it = np.zeros(S, np.int64)
+        res = np.zeros(S)
+        rc = self.L.alpo_ppr_forward(n, _p(rp), _p(col), _p(w), S, _p(seeds), alpha, conv,
+                                     max_iter, int(x0 is not None), _p(x), _p(it), _p(res))
+        assert rc == 0, rc
+        return x, it, res
+
+    def ppr_adjoint(self, rp, col, w, seeds, g, alpha=0.85, conv=1e-9, max_iter=1000):
+        """Same contract as oracle.ppr.adjoint: (lambda [n, S], iterations, residuals)."""
+        rp, col, w = self._crs(rp, col, w)
+        n = len(rp) - 1
+        seeds = np.ascontiguousarray(seeds, np.int64)
+        S = len(seeds)
+        g = np.ascontiguousarray(g, np.float64).reshape(n, S)
+        lam = np.empty((n, S))
+        it = np.zeros(S, np.int64)
+        res = np.zeros(S)
+        rc = self.L.alpo_ppr_adjoint(n, _p(rp), _p(col), _p(w), S, _p(seeds), _p(g), alpha, conv,
+                                     max_iter, _p(lam), _p(it), _p(res))
+        assert rc == 0, rc
+        return lam, it, res
+
+    def ppr_grad(self, rp, col, w, x, lam, alpha=0.85):
+        """Same contract as oracle.ppr.grad_weights."""
+        rp, col, w = self._crs(rp, col, w)
+        n = len(rp) - 1
+        x = np.ascontiguousarray(x, np.float64)
+        lam = np.ascontiguousarray(lam, np.float64)
+        S = x.shape[1]
+        grad = np.empty(len(col))
+        rc = self.L.alpo_ppr_grad(n, _p(rp), _p(col), _p(w), S, _p(x), _p(lam), alpha, _p(grad))
+        assert rc == 0, rc
+        return grad
+
 
 class Reference:
     """The unmodified ALP reference (sequential or OpenMP backend)."""
@@ -159,6 +209,7 @@ class Reference:
                                P, P, I32, I32, P]
         L.refw_cg.argtypes = [I64, I64, P, P, P, P, P, I64, D, P, P, P]
         L.refw_pagerank.argtypes = [I64, I64, P, P, P, P, D, D, I64, P, P]
+        L.refw_hpcg.argtypes = [I64, I64, I64, I64, I64, P, P, I64, D, P, P, P, P]
         self.L = L
         self.omp = omp
 
@@ -199,6 +250,20 @@ class Reference:
                                   _p(np.ascontiguousarray(V, np.float64)), _p(pr), alpha, conv,
                                   max_iter, _p(it), _p(ms))
         return rc, pr, int(it[0]), float(ms[0])
+
+    def hpcg(self, nx, levels, colors=27, b=None, max_iter=200, tol=1e-9):
+        """grb::algorithms::hpcg on the nx^3 system; returns (rc, x, iterations,
+        residual, ms of the solve, ms of the system build)."""
+        n = nx ** 3
+        x = np.zeros(n)
+        it = np.zeros(1, np.int64)
+        res = np.zeros(1)
+        ms = np.zeros(1)
+        bms = np.zeros(1)
+        bb = None if b is None else np.ascontiguousarray(b, np.float64)
+        rc = self.L.refw_hpcg(nx, nx, nx, levels, colors, _p(bb), _p(x), max_iter, tol, _p(it),
+                              _p(res), _p(ms), _p(bms))
+        return rc, x, int(it[0]), float(res[0]), float(ms[0]), float(bms[0])
 
 
 def crs_to_coo(rp, col):

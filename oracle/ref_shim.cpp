@@ -18,8 +18,12 @@
 #include <graphblas.hpp>
 #include <graphblas/algorithms/conjugate_gradient.hpp>
 #include <graphblas/algorithms/simple_pagerank.hpp>
+#include <graphblas/algorithms/hpcg/hpcg.hpp>
+#include <graphblas/algorithms/hpcg/system_building_utils.hpp>
 
+#include <array>
 #include <chrono>
+#include <memory>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -250,6 +254,48 @@ __attribute__((visibility("default"))) int refw_pagerank(int64_t n, int64_t nnz,
 	if (ms) *ms = now_ms() - t0;
 	*iterations = int64_t(iters);
 	export_vector<double>(p, n, pr, nullptr);
+	return int(rc);
+}
+
+/* grb::algorithms::hpcg on the system build_hpcg_system makes (27-point
+ * stencil on nx*ny*nz, diagonal 26, off-diagonals -1, max_levels coarser
+ * levels, `colors` static colours, one pre- and one post-smoothing step),
+ * one right-hand side b (NULL: b = A 1), x from zero; *ms times hpcg() alone,
+ * *build_ms the system build. */
+__attribute__((visibility("default"))) int refw_hpcg(int64_t nx, int64_t ny, int64_t nz,
+	int64_t max_levels, int64_t colors, const double *b, double *x, int64_t max_iter, double tol,
+	int64_t *iterations, double *residual, double *ms, double *build_ms) {
+	ensure_init();
+	using namespace grb::algorithms;
+	const std::array< size_t, 3 > sizes = { size_t(nx), size_t(ny), size_t(nz) };
+	hpcg_system_params< 3, double > params { sizes, 1, size_t(colors), 26.0, -1.0, 4,
+		size_t(max_levels), 2 };
+	std::unique_ptr< hpcg_data< double, double, double > > data;
+	const double t0 = now_ms();
+	RC rc = build_hpcg_system< 3, double >( data, params );
+	const size_t n = size_t(nx * ny * nz);
+	Semiring< operators::add< double >, operators::mul< double >, identities::zero,
+		identities::one > ring;
+	if (rc == SUCCESS) {
+		if (b == nullptr) {
+			rc = set(data->x, 1.0);
+			rc = rc ? rc : set(data->b, 0.0);
+			rc = rc ? rc : mxv(data->b, data->A, data->x, ring);
+		} else {
+			rc = build_vector<double>(data->b, int64_t(n), b, nullptr);
+		}
+	}
+	rc = rc ? rc : set(data->x, 0.0);
+	if (build_ms) *build_ms = now_ms() - t0;
+	if (rc != SUCCESS) return int(rc);
+	size_t iters = 0;
+	double res = 0;
+	const double t1 = now_ms();
+	rc = hpcg(*data, true, 1, 1, size_t(max_iter), tol, iters, res);
+	if (ms) *ms = now_ms() - t1;
+	*iterations = int64_t(iters);
+	*residual = res;
+	if (x) export_vector<double>(data->x, int64_t(n), x, nullptr);
 	return int(rc);
 }
 

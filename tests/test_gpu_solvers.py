@@ -130,3 +130,37 @@ def test_pagerank_rmat_matches_restatement(cuda, oracle, scale):
     assert abs(it - it2) <= 1
     np.testing.assert_allclose(pr, pr2, rtol=1e-9, atol=1e-14)
     assert abs(pr.sum() - 1.0) < 1e-8
+
+
+def test_pagerank_planned_equals_plain(cuda):
+    """alpb_pagerank_planned with a caller-held plan of the CCS and scratch
+    gives alpb_pagerank's result bit for bit (same tiles, same grid), on two
+    solves in a row with the same plan; a plan of other offsets is refused."""
+    import torch
+    from alp_b200 import _abi as abi
+    dev = _dev()
+    L = dev.rmat(14, vtype=FP64, seed=8)
+    L.values.fill_(1.0)
+    LT = dev.transpose(L)
+    rc, pr, it, res = pagerank_device(L, LT)
+    assert rc == 0
+    plan = dev.Plan(LT, sched=abi.SCHED_AUTO)
+    work = torch.empty(3 * L.m, dtype=torch.float64, device="cuda")
+    for use_work in (True, False):
+        p2 = torch.zeros(L.m, dtype=torch.float64, device="cuda")
+        it2, res2 = C.c_int64(), C.c_double()
+        rc2 = abi.lib().alpb_pagerank_planned(
+            L.m, dev.ptr(L.offsets), dev.ptr(L.indices), dev.ptr(L.values), dev.ptr(LT.offsets),
+            dev.ptr(LT.indices), dev.ptr(LT.values), dev.ptr(p2), 0, 0.85, 1e-9, 1000,
+            C.byref(it2), C.byref(res2), dev.ptr(work) if use_work else None, plan.h,
+            dev.stream_ptr())
+        torch.cuda.synchronize()
+        assert rc2 == 0 and it2.value == it and res2.value == res
+        np.testing.assert_array_equal(p2.cpu().numpy(), pr)
+    other = dev.Plan(L, sched=abi.SCHED_AUTO)
+    it2, res2 = C.c_int64(), C.c_double()
+    rc3 = abi.lib().alpb_pagerank_planned(
+        L.m, dev.ptr(L.offsets), dev.ptr(L.indices), dev.ptr(L.values), dev.ptr(LT.offsets),
+        dev.ptr(LT.indices), dev.ptr(LT.values), dev.ptr(work), 0, 0.85, 1e-9, 1000,
+        C.byref(it2), C.byref(res2), None, other.h, dev.stream_ptr())
+    assert rc3 == abi.MISMATCH

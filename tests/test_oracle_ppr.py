@@ -64,3 +64,32 @@ def test_gradient_matches_central_differences(oracle):
         wm[k] -= h
         fd = (loss(wp)[0] - loss(wm)[0]) / (2 * h)
         assert abs(fd - g[k]) <= 1e-5 * abs(g[k]) + 1e-7 * np.abs(g).max(), (k, fd, g[k])
+
+
+def test_c_restatement_equals_numpy_restatement(oracle):
+    """ppr_oracle.c (the benchmark-scale checker) against oracle/ppr.py on a
+    weighted R-MAT graph with dangling rows: the same iteration counts, and
+    iterates equal to the last bits (same sums in the same order)."""
+    rp, col, w = oracle.rmat(9, seed=21, vtype=FP64)
+    n = len(rp) - 1
+    rng = np.random.default_rng(7)
+    seeds = rng.integers(0, n, 11)
+    seeds[3] = seeds[7]                      # a repeated seed
+    x, it, res = O.forward(rp, col, w, seeds, conv=1e-10)
+    xc, itc, resc = oracle.ppr_forward(rp, col, w, seeds, conv=1e-10)
+    assert (it == itc).all()
+    np.testing.assert_allclose(xc, x, rtol=1e-14, atol=1e-300)
+    np.testing.assert_allclose(resc, res, rtol=1e-12, atol=1e-300)
+    g = rng.standard_normal((n, len(seeds)))
+    lam, ita, _ = O.adjoint(rp, col, w, seeds, g, conv=1e-10)
+    lamc, itac, _ = oracle.ppr_adjoint(rp, col, w, seeds, g, conv=1e-10)
+    assert (ita == itac).all()
+    np.testing.assert_allclose(lamc, lam, rtol=1e-13, atol=1e-13 * np.abs(lam).max())
+    gr = O.grad_weights(rp, col, w, x, lam)
+    grc = oracle.ppr_grad(rp, col, w, x, lam)
+    np.testing.assert_allclose(grc, gr, rtol=1e-11, atol=1e-13 * np.abs(gr).max())
+    # a warm start and a budget stop
+    x2, it2, _ = O.forward(rp, col, w, seeds, conv=0.0, max_iter=5, x0=x)
+    x2c, it2c, _ = oracle.ppr_forward(rp, col, w, seeds, conv=0.0, max_iter=5, x0=x)
+    assert (it2 == 5).all() and (it2c == 5).all()
+    np.testing.assert_allclose(x2c, x2, rtol=1e-14, atol=1e-300)
