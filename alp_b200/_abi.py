@@ -91,6 +91,7 @@ PROTOS: dict[str, list] = {
     "alpb_hpcg_info": [P, PI64, PI64, PI64, PI],
     "alpb_hpcg_matrix": [P, I64, C.POINTER(P), C.POINTER(P), C.POINTER(P), PI64, PI64],
     "alpb_hpcg_solve": [P, P, P, I32, I64, I64, I64, D, P, P, P],
+    "alpb_hpcg_match_level": [P, I64, I64, I64, P, P, P, P, P, I64, P, P, I64, P, P, P, P, P],
     "alpb_ppr_create": [C.POINTER(P), I64, I64, P, P, P, I32, P],
     "alpb_ppr_destroy": [P],
     "alpb_ppr_set_weights": [P, P, P],

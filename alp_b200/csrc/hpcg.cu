@@ -273,6 +273,66 @@ __global__ void k_hpcg_color_conflicts(const int64_t *offsets, const uint32_t *i
 		}
 }
 
+// ------------------------------------------------- recognising a system --
+// Checks of a caller's level against this handle's (alpb_hpcg_match_level);
+// each sets *bad on the first difference it sees.
+__global__ void k_hg_words_differ(const uint32_t *a, const uint32_t *b, int64_t words,
+	int32_t *bad) {
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < words;
+		 i += int64_t(gridDim.x) * blockDim.x)
+		if (a[i] != b[i]) {
+			*bad = 1;
+			return;
+		}
+}
+
+// every entry assigned and equal to the handle's diagonal value
+__global__ void k_hg_check_diag(const double *d, const uint8_t *flags, int64_t n, double diag,
+	int32_t *bad) {
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+		 i += int64_t(gridDim.x) * blockDim.x)
+		if ((flags && !flags[i]) || d[i] != diag) {
+			*bad = 1;
+			return;
+		}
+}
+
+// colour c of `colors`: assigned (and true) exactly at the rows i = c mod colors
+// (build_static_color_masks, hpcg/matrix_building_utils.hpp:131-165)
+__global__ void k_hg_check_mask(const uint8_t *vals, const uint8_t *flags, int64_t n,
+	int64_t colors, int64_t c, int32_t *bad) {
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+		 i += int64_t(gridDim.x) * blockDim.x) {
+		const bool want = i % colors == c;
+		const bool has = flags ? flags[i] != 0 : true;
+		if (has != want || (has && vals[i] == 0)) {
+			*bad = 1;
+			return;
+		}
+	}
+}
+
+// the injection coarsener of build_ndims_coarsener_matrix: coarse row c holds
+// one 1 at fine column inj(c)
+__global__ void k_hg_check_coarsening(const int64_t *off, const uint32_t *idx, const double *val,
+	int64_t nc, int64_t fine_n, int64_t cnx, int64_t cny, int64_t fnx, int64_t fny,
+	int32_t *bad) {
+	for (int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; c <= nc;
+		 c += int64_t(gridDim.x) * blockDim.x) {
+		if (off[c] != c) {
+			*bad = 1;
+			return;
+		}
+		if (c == nc) continue;
+		const int64_t cx = c % cnx, cy = (c / cnx) % cny, cz = c / (cnx * cny);
+		const int64_t f = 2 * cx + 2 * cy * fnx + 2 * cz * fnx * fny;
+		if (f >= fine_n || int64_t(idx[c]) != f || val[c] != 1.0) {
+			*bad = 1;
+			return;
+		}
+	}
+}
+
 struct HgLevel {
 	int64_t nx = 0, ny = 0, nz = 0, n = 0, nnz = 0;
 	int64_t *offsets = nullptr;
@@ -605,6 +665,56 @@ int alpb_hpcg_solve(alpb_hpcg h, const double *b, double *x, int with_preconditi
 	default: return hg_solve<8>(h, b, x, pc, presmoother_steps, postsmoother_steps,
 		max_iterations, tolerance, iterations, residuals, s);
 	}
+}
+
+int alpb_hpcg_match_level(alpb_hpcg h, int64_t level, int64_t n, int64_t nnz,
+	const int64_t *offsets, const uint32_t *indices, const double *values, const double *diagonal,
+	const uint8_t *diagonal_flags, int64_t colors, const uint8_t *const *mask_values,
+	const uint8_t *const *mask_flags, int64_t coarse_nnz, const int64_t *coarse_offsets,
+	const uint32_t *coarse_indices, const double *coarse_values, int *matches, void *stream) {
+	ALPB_CHECK(h != nullptr && matches != nullptr, ALPB_ILLEGAL,
+		"alpb_hpcg_match_level: null argument");
+	*matches = 0;
+	if (level < 0 || level >= int64_t(h->levels.size())) return ALPB_SUCCESS;
+	const HgLevel &L = h->levels[size_t(level)];
+	if (n != L.n || nnz != L.nnz || colors != h->colors || !offsets || (nnz && (!indices ||
+			!values)) || !diagonal || (colors && (!mask_values || !mask_flags)))
+		return ALPB_SUCCESS;
+	if (level > 0 && (coarse_nnz != L.n || !coarse_offsets || !coarse_indices || !coarse_values))
+		return ALPB_SUCCESS;
+	cudaStream_t s = as_stream(stream);
+	int32_t *bad = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&bad, 4, s));
+	ALPB_CUDA(cudaMemsetAsync(bad, 0, 4, s));
+	const void *const pa[3] = {offsets, indices, values};
+	const void *const pb[3] = {L.offsets, L.indices, L.values};
+	const int64_t nw[3] = {2 * (n + 1), nnz, 2 * nnz};   // 4-byte words
+	for (int k = 0; k < 3; ++k) {
+		if (nw[k] == 0) continue;
+		k_hg_words_differ<<<grid_for(nw[k], 256, 2), 256, 0, s>>>(
+			static_cast<const uint32_t *>(pa[k]), static_cast<const uint32_t *>(pb[k]), nw[k], bad);
+		ALPB_LAUNCHED();
+	}
+	k_hg_check_diag<<<grid_for(n, 256, 2), 256, 0, s>>>(diagonal, diagonal_flags, n, h->diag,
+		bad);
+	ALPB_LAUNCHED();
+	for (int64_t c = 0; c < colors; ++c) {
+		k_hg_check_mask<<<grid_for(n, 256, 2), 256, 0, s>>>(mask_values[c], mask_flags[c], n,
+			colors, c, bad);
+		ALPB_LAUNCHED();
+	}
+	if (level > 0) {
+		const HgLevel &F = h->levels[size_t(level - 1)];
+		k_hg_check_coarsening<<<grid_for(L.n + 1, 256, 2), 256, 0, s>>>(coarse_offsets,
+			coarse_indices, coarse_values, L.n, F.n, L.nx, L.ny, F.nx, F.ny, bad);
+		ALPB_LAUNCHED();
+	}
+	int32_t hb = 1;
+	ALPB_CUDA(cudaMemcpyAsync(&hb, bad, 4, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaFreeAsync(bad, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	*matches = hb == 0 ? 1 : 0;
+	return ALPB_SUCCESS;
 }
 
 }  // extern "C"

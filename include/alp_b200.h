@@ -469,6 +469,23 @@ ALPB_API int alpb_hpcg_matrix(alpb_hpcg h, int64_t level, const int64_t **offset
 ALPB_API int alpb_hpcg_solve(alpb_hpcg h, const double *b, double *x, int with_preconditioning,
 	int64_t presmoother_steps, int64_t postsmoother_steps, int64_t max_iterations,
 	double tolerance, int64_t *iterations, double *residuals, void *stream);
+/* Whether a caller's multigrid level equals level `level` of this handle, so
+ * that the caller's own HPCG data can be solved by this handle (the b200
+ * overload of grb::algorithms::hpcg recognises build_hpcg_system's systems
+ * this way; no counterpart in the reference).  Compared on the device: the
+ * system matrix (n, nnz and the CRS arrays word for word), the diagonal
+ * vector (every entry assigned and equal to `diag`; diagonal_flags NULL =
+ * dense), the `colors` colour masks (host arrays of device pointers: mask c
+ * assigned and true exactly at the rows i = c mod colors; a NULL flags entry =
+ * dense) and, for level > 0, the coarsening matrix from the finer level
+ * (coarse_nnz entries; row c holds one 1 at the injected fine row).
+ * *matches = 1 when everything agrees, else 0. */
+ALPB_API int alpb_hpcg_match_level(alpb_hpcg h, int64_t level, int64_t n, int64_t nnz,
+	const int64_t *offsets, const uint32_t *indices, const double *values,
+	const double *diagonal, const uint8_t *diagonal_flags, int64_t colors,
+	const uint8_t *const *mask_values, const uint8_t *const *mask_flags, int64_t coarse_nnz,
+	const int64_t *coarse_offsets, const uint32_t *coarse_indices,
+	const double *coarse_values, int *matches, void *stream);
 
 /* ======================================================================
  * Adjoint gradients of a CG solve (implicit function theorem; no iterate is

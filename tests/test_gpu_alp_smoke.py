@@ -17,11 +17,16 @@ ROOT = Path(__file__).resolve().parent.parent
 
 
 def run(name, *args, backend="b200"):
+    """Runs one smoke program; on b200 with ALPB_TRACE set, so that the output
+    shows which solves took the fused device path."""
+    import os
     exe = (ROOT / "_build" / "cpp" / f"smoke_{name}_b200" if backend == "b200"
            else ROOT / "oracle" / "_ref" / "cpp" / f"smoke_{name}_ref")
     if not exe.exists():
         pytest.fail(f"{exe} is not built (build() compiles it where the ALP sources exist)")
-    r = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=900)
+    env = dict(os.environ, ALPB_TRACE="1")
+    r = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=900,
+                       env=env)
     out = r.stdout + r.stderr
     assert r.returncode == 0, out[-3000:]
     assert "Test OK" in out, out[-3000:]
@@ -125,6 +130,8 @@ def test_simple_pagerank_matches_reference(cuda, inputs):
     g, _, _ = inputs
     out = run("simple_pagerank", g, "direct", 1, 1, 1000)
     outr = run("simple_pagerank", g, "direct", 1, 1, 1000, backend="ref")
+    # the unchanged program's simple_pagerank call ran the fused device solver
+    assert "grb::b200: fused simple_pagerank" in out, out[-2000:]
     assert solver_result(out)[0] == solver_result(outr)[0]
     assert first_ten(out) == pytest.approx(first_ten(outr), rel=1e-5)
 
@@ -158,6 +165,7 @@ def test_conjugate_gradient_smoke_matches_reference(cuda, inputs):
     _, _, s = inputs
     out = run("conjugate_gradient", s, "direct", 1, 1, 1000, "false")
     outr = run("conjugate_gradient", s, "direct", 1, 1, 1000, "false", backend="ref")
+    assert "grb::b200: fused conjugate_gradient" in out, out[-2000:]
     it, res = solver_result(out)
     itr, resr = solver_result(outr)
     assert abs(it - itr) <= 1 and res < 1e-8 and resr < 1e-8

@@ -36,10 +36,10 @@ UNIT = ["masked_mxv", "sparse_mxv", "masked_vxm", "dot", "set", "eWiseMul", "mul
         "eWiseMatrix"]
 
 
-def _run(exe: Path, *args, timeout=300):
+def _run(exe: Path, *args, timeout=300, env=None):
     if not exe.exists():
         pytest.fail(f"{exe} is not built (build() compiles it where the ALP sources exist)")
-    env = dict(os.environ, OMP_NUM_THREADS="1")
+    env = dict(os.environ, OMP_NUM_THREADS="1", **(env or {}))
     return subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True,
                           timeout=timeout, env=env)
 
@@ -268,6 +268,34 @@ def _hpcg_result(out: str):
     return int(it.group(1)), float(it.group(2)), float(norm.group(1))
 
 
+def test_driver_solvers_take_the_fused_path(cuda, oracle):
+    """ALP's conjugate_gradient and simple_pagerank, called unchanged on b200
+    containers, run the fused device solvers (one launch per solve), as the
+    ALPB_TRACE line shows; the results were compared above."""
+    from oracle.oracle import crs_to_coo
+    I, J, V = oracle.stencil_coo((10, 10, 10), 26.0, -1.0)
+    m = 1000
+    rp, col, vals = oracle.coo_to_crs(m, I, J, V, 3)
+    b = np.zeros(m)
+    oracle.mxv(0, 0, 2, m, m, rp, col, vals, 3, b, v=np.ones(m))
+    rp2, col2, _ = oracle.rmat(9, edge_factor=8, seed=78, vtype=3)
+    I2, J2 = crs_to_coo(rp2, col2)
+    n2 = len(rp2) - 1
+    env = dict(os.environ, ALPB_TRACE="1")
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "cg.bin"
+        write_case(f, 2, 0, 0, m, m, I, J, V, (np.zeros(m), np.ones(m, np.uint8)),
+                   (b, np.ones(m, np.uint8)))
+        r = subprocess.run([str(B200_BIN / "alp_driver_b200"), str(f)], capture_output=True,
+                           text=True, timeout=300, env=env)
+        assert r.returncode == 0 and "grb::b200: fused conjugate_gradient" in r.stderr, r.stderr
+        f2 = Path(d) / "pr.bin"
+        write_case(f2, 3, 0, 0, n2, n2, I2, J2, np.ones(len(I2)))
+        r = subprocess.run([str(B200_BIN / "alp_driver_b200"), str(f2)], capture_output=True,
+                           text=True, timeout=300, env=env)
+        assert r.returncode == 0 and "grb::b200: fused simple_pagerank" in r.stderr, r.stderr
+
+
 def test_hpcg_smoke_matches_reference(cuda):
     """ALP's HPCG smoke test (tests/smoke/hpcg.cpp: 16^3, multigrid V-cycle with
     red-black Gauss-Seidel smoothing, CG outer loop), compiled unchanged on
@@ -282,3 +310,6 @@ def test_hpcg_smoke_matches_reference(cuda):
     ib, _, nb = _hpcg_result(b.stdout)
     assert abs(ia - ib) <= 1, (ia, ib)
     assert nb < 4e-14, nb
+    # the unchanged program's hpcg call ran the fused device solver
+    b = _run(B200_BIN / "smoke_hpcg_b200", *args, env={"ALPB_TRACE": "1"})
+    assert "grb::b200: fused hpcg" in b.stderr, b.stderr[-2000:]

@@ -159,3 +159,36 @@ def test_hpcg_without_preconditioning(cuda):
     ir, rr, xr = reference(16, 1, 27, 1, 1, 300, 1e-9, False, b)
     assert it[0] == ir
     np.testing.assert_allclose(x[:, 0], xr, rtol=1e-9, atol=1e-9 * np.abs(xr).max())
+
+
+B200_DRIVER = ROOT / "_build" / "cpp" / "hpcg_driver_b200"
+
+
+@pytest.mark.parametrize("nx,levels,colors", [(16, 1, 27), (32, 2, 27), (16, 1, 16)])
+def test_alp_hpcg_call_takes_the_fused_path(cuda, nx, levels, colors):
+    """grb::algorithms::hpcg called unchanged on a b200 system that
+    build_hpcg_system made (tests/cpp/hpcg_driver.cpp compiled for b200): the
+    overload recognises the system on the device and runs the fused device
+    HPCG (ALPB_TRACE line), with the reference build's iteration count and x
+    within 1e-9 relative; 16 colours exercise the two-pass colour step."""
+    import os
+    if not B200_DRIVER.exists():
+        pytest.fail(f"{B200_DRIVER} is not built")
+    rng = np.random.default_rng(100 + nx)
+    b = rng.standard_normal(nx ** 3)
+    with tempfile.TemporaryDirectory() as d:
+        rhs = str(Path(d) / "b.bin")
+        b.tofile(rhs)
+        xo = Path(d) / "x.bin"
+        r = subprocess.run([str(B200_DRIVER), *map(str, (nx, nx, nx, levels, colors, 1, 1, 200,
+                                                         1e-9, 1)), rhs, str(xo)],
+                           capture_output=True, text=True, timeout=600,
+                           env=dict(os.environ, ALPB_TRACE="1"))
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert "grb::b200: fused hpcg" in r.stderr, r.stderr
+        out = dict(line.split() for line in r.stdout.splitlines() if len(line.split()) == 2)
+        x = np.fromfile(xo)
+    ir, rr, xr = reference(nx, levels, colors, 1, 1, 200, 1e-9, True, b)
+    assert int(out["iterations"]) == ir
+    np.testing.assert_allclose(x, xr, rtol=1e-9, atol=1e-9 * np.abs(xr).max())
+    assert abs(float(out["residual"]) - rr) <= 1e-6 * rr
