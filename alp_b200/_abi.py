@@ -108,6 +108,10 @@ PROTOS: dict[str, list] = {
     "alpb_reduce_f64": [PD, I32, I64, P, P, P],
     "alpb_vec_op": [I32, I32, I32, D, I32, U32, I64, P, I32, P, P, P, P, I32, I32,
                     P, I32, P, D, P, I32, P, D, P],
+    "alpb_vec_op_dom": [I32, I32, I32, U64, I32, U32, I32, I64, P, I32, P, P, P, P, I32, I32,
+                        P, I32, P, U64, P, I32, P, U64, P],
+    "alpb_vec_reduce_dom": [P, I32, U64, I32, U32, I32, I64, P, I32, P, P, I32, P, P, P, I32,
+                            I32, P],
     "alpb_count_assigned": [P, I64, PI64, P],
     "alpb_vec_reduce": [PD, I32, D, I32, U32, I64, P, I32, P, P, I32, P, P, P, I32, I32, P],
     "alpb_cg_solve": [I64, P, P, P, P, P, I64, D, PI64, PD, P, P, P],

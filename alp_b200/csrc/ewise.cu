@@ -4,69 +4,120 @@
 // (reference/blas1.hpp, reference/io.hpp).
 //
 // Every operand is (values, assigned flags) with flags == nullptr meaning
-// dense, or a scalar.  Values are read into double and the result is cast
-// back to the output type (the ALP operator domains seen by the kernels are
-// double, int32, int64 and bool; integers up to 2^53 round-trip exactly).
+// dense, or a scalar.  Values are read into the operator's domain -- double,
+// int64_t or uint64_t, chosen by the caller from the ALP operator's type --
+// computed there and cast to the output type, as the reference's operators
+// cast their operands (graphblas/ops.hpp): integer operators compute exactly,
+// with two's-complement wrap-around.
 #include "common.cuh"
 
-#include <vector>
+#include <cstring>
+#include <type_traits>
 
 namespace alpb {
 
-__device__ __forceinline__ double ld_val(const void *p, int type, int64_t i) {
+// ------------------------------------------------------------ domains --
+// An ALP operator computes in its own domain: double, or a 64-bit integer
+// (int and size_t operators).  Integer domains compute in int64_t or
+// uint64_t with two's-complement wrap-around; storing into a narrower type
+// truncates, so int32 sums and products wrap exactly as 32-bit ones do.
+template <class T>
+__device__ __forceinline__ T ld_as(const void *p, int type, int64_t i) {
 	switch (type) {
-	case ALPB_FP64: return reinterpret_cast<const double *>(p)[i];
-	case ALPB_INT32: return double(reinterpret_cast<const int32_t *>(p)[i]);
-	case ALPB_BOOL: return reinterpret_cast<const uint8_t *>(p)[i] ? 1.0 : 0.0;
-	case ALPB_INT64: return double(reinterpret_cast<const int64_t *>(p)[i]);
-	case ALPB_UINT32: return double(reinterpret_cast<const uint32_t *>(p)[i]);
-	case ALPB_UINT8: return double(reinterpret_cast<const uint8_t *>(p)[i]);
-	case ALPB_INT8: return double(reinterpret_cast<const int8_t *>(p)[i]);
+	case ALPB_FP64: return T(reinterpret_cast<const double *>(p)[i]);
+	case ALPB_INT32: return T(int64_t(reinterpret_cast<const int32_t *>(p)[i]));
+	case ALPB_BOOL: return reinterpret_cast<const uint8_t *>(p)[i] ? T(1) : T(0);
+	case ALPB_INT64: return T(reinterpret_cast<const int64_t *>(p)[i]);
+	case ALPB_UINT32: return T(reinterpret_cast<const uint32_t *>(p)[i]);
+	case ALPB_UINT8: return T(reinterpret_cast<const uint8_t *>(p)[i]);
+	case ALPB_INT8: return T(int64_t(reinterpret_cast<const int8_t *>(p)[i]));
+	case ALPB_UINT64: return T(reinterpret_cast<const uint64_t *>(p)[i]);
 	}
-	return 0.0;
+	return T(0);
 }
-__device__ __forceinline__ void st_val(void *p, int type, int64_t i, double v) {
+template <>
+__device__ __forceinline__ uint64_t ld_as<uint64_t>(const void *p, int type, int64_t i) {
 	switch (type) {
-	case ALPB_FP64: reinterpret_cast<double *>(p)[i] = v; break;
-	case ALPB_INT32: reinterpret_cast<int32_t *>(p)[i] = int32_t(int64_t(v)); break;
-	case ALPB_BOOL: reinterpret_cast<uint8_t *>(p)[i] = v != 0.0 ? 1 : 0; break;
-	case ALPB_INT64: reinterpret_cast<int64_t *>(p)[i] = int64_t(v); break;
-	case ALPB_UINT32: reinterpret_cast<uint32_t *>(p)[i] = uint32_t(int64_t(v)); break;
-	case ALPB_UINT8: reinterpret_cast<uint8_t *>(p)[i] = uint8_t(int64_t(v)); break;
-	case ALPB_INT8: reinterpret_cast<int8_t *>(p)[i] = int8_t(int64_t(v)); break;
+	case ALPB_FP64: return uint64_t(reinterpret_cast<const double *>(p)[i]);
+	case ALPB_INT64:
+	case ALPB_UINT64: return reinterpret_cast<const uint64_t *>(p)[i];   // size_t storage
+	default: return uint64_t(ld_as<int64_t>(p, type, i));
 	}
-}
-__device__ __forceinline__ double opd(int op, double a, double b) {
-	switch (op) {
-	case ALPB_OP_ADD: return a + b;
-	case ALPB_OP_SUB: return a - b;
-	case ALPB_OP_MUL: return a * b;
-	case ALPB_OP_DIV: return a / b;
-	case ALPB_OP_MIN: return a < b ? a : b;
-	case ALPB_OP_MAX: return a > b ? a : b;
-	case ALPB_OP_ABS_DIFF: return a > b ? a - b : b - a;
-	case ALPB_OP_LEFT_ASSIGN: return a;
-	case ALPB_OP_RIGHT_ASSIGN: return b;
-	case ALPB_OP_LOR: return (a != 0.0 || b != 0.0) ? 1.0 : 0.0;
-	case ALPB_OP_LAND: return (a != 0.0 && b != 0.0) ? 1.0 : 0.0;
-	case ALPB_OP_LEFT_ASSIGN_IF: return a;  // callers test opd_skips first
-	case ALPB_OP_EQUAL: return a == b ? 1.0 : 0.0;
-	case ALPB_OP_NOT_EQUAL: return a != b ? 1.0 : 0.0;
-	case ALPB_OP_LESS: return a < b ? 1.0 : 0.0;
-	case ALPB_OP_LEQ: return a <= b ? 1.0 : 0.0;
-	case ALPB_OP_GREATER: return a > b ? 1.0 : 0.0;
-	case ALPB_OP_GEQ: return a >= b ? 1.0 : 0.0;
-	}
-	return 0.0;
-}
-// True where op leaves its output unchanged (left_assign_if with b false).
-__device__ __forceinline__ bool opd_skips(int op, double b) {
-	return op == ALPB_OP_LEFT_ASSIGN_IF && b == 0.0;
 }
 
+template <class T>
+__device__ __forceinline__ void st_as(void *p, int type, int64_t i, T v) {
+	switch (type) {
+	case ALPB_FP64: reinterpret_cast<double *>(p)[i] = double(v); break;
+	case ALPB_INT32: reinterpret_cast<int32_t *>(p)[i] = int32_t(uint32_t(uint64_t(int64_t(v)))); break;
+	case ALPB_BOOL: reinterpret_cast<uint8_t *>(p)[i] = v != T(0) ? 1 : 0; break;
+	case ALPB_INT64: reinterpret_cast<int64_t *>(p)[i] = int64_t(v); break;
+	case ALPB_UINT32: reinterpret_cast<uint32_t *>(p)[i] = uint32_t(uint64_t(int64_t(v))); break;
+	case ALPB_UINT8: reinterpret_cast<uint8_t *>(p)[i] = uint8_t(uint64_t(int64_t(v))); break;
+	case ALPB_INT8: reinterpret_cast<int8_t *>(p)[i] = int8_t(uint8_t(uint64_t(int64_t(v)))); break;
+	case ALPB_UINT64: reinterpret_cast<uint64_t *>(p)[i] = uint64_t(int64_t(v)); break;
+	}
+}
+template <>
+__device__ __forceinline__ void st_as<uint64_t>(void *p, int type, int64_t i, uint64_t v) {
+	switch (type) {
+	case ALPB_FP64: reinterpret_cast<double *>(p)[i] = double(v); break;
+	case ALPB_INT64:
+	case ALPB_UINT64: reinterpret_cast<uint64_t *>(p)[i] = v; break;
+	default: st_as<int64_t>(p, type, i, int64_t(v)); break;
+	}
+}
+
+// wrapping + - * for the integer domains (no signed-overflow UB)
+template <class T> __device__ __forceinline__ T wrap_add(T a, T b) { return a + b; }
+template <class T> __device__ __forceinline__ T wrap_sub(T a, T b) { return a - b; }
+template <class T> __device__ __forceinline__ T wrap_mul(T a, T b) { return a * b; }
+template <> __device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t b) {
+	return int64_t(uint64_t(a) + uint64_t(b));
+}
+template <> __device__ __forceinline__ int64_t wrap_sub(int64_t a, int64_t b) {
+	return int64_t(uint64_t(a) - uint64_t(b));
+}
+template <> __device__ __forceinline__ int64_t wrap_mul(int64_t a, int64_t b) {
+	return int64_t(uint64_t(a) * uint64_t(b));
+}
+
+template <class T>
+__device__ __forceinline__ T opv(int op, T a, T b) {
+	switch (op) {
+	case ALPB_OP_ADD: return wrap_add(a, b);
+	case ALPB_OP_SUB: return wrap_sub(a, b);
+	case ALPB_OP_MUL: return wrap_mul(a, b);
+	case ALPB_OP_DIV:
+		if constexpr (std::is_floating_point<T>::value) return a / b;
+		else return b == T(0) ? T(0) : a / b;   // the host's division by zero is undefined
+	case ALPB_OP_MIN: return a < b ? a : b;
+	case ALPB_OP_MAX: return a > b ? a : b;
+	case ALPB_OP_ABS_DIFF: return a > b ? wrap_sub(a, b) : wrap_sub(b, a);
+	case ALPB_OP_LEFT_ASSIGN: return a;
+	case ALPB_OP_RIGHT_ASSIGN: return b;
+	case ALPB_OP_LOR: return (a != T(0) || b != T(0)) ? T(1) : T(0);
+	case ALPB_OP_LAND: return (a != T(0) && b != T(0)) ? T(1) : T(0);
+	case ALPB_OP_LEFT_ASSIGN_IF: return a;  // callers test opv_skips first
+	case ALPB_OP_EQUAL: return a == b ? T(1) : T(0);
+	case ALPB_OP_NOT_EQUAL: return a != b ? T(1) : T(0);
+	case ALPB_OP_LESS: return a < b ? T(1) : T(0);
+	case ALPB_OP_LEQ: return a <= b ? T(1) : T(0);
+	case ALPB_OP_GREATER: return a > b ? T(1) : T(0);
+	case ALPB_OP_GEQ: return a >= b ? T(1) : T(0);
+	}
+	return T(0);
+}
+// True where op leaves its output unchanged (left_assign_if with b false).
+template <class T>
+__device__ __forceinline__ bool opv_skips(int op, T b) {
+	return op == ALPB_OP_LEFT_ASSIGN_IF && b == T(0);
+}
+
+template <class T>
 struct VecArgs {
 	int kind, op, monoid;
-	double identity;
+	T identity;
 	uint32_t descr;
 	int64_t n;
 	void *z;
@@ -80,15 +131,16 @@ struct VecArgs {
 	const void *x;
 	int xt;
 	const uint8_t *xa;
-	double alpha;
+	T alpha;
 	const void *y;
 	int yt;
 	const uint8_t *ya;
-	double beta;
+	T beta;
 	int mul_op;
 };
 
-__global__ void k_vec(VecArgs a) {
+template <class T>
+__global__ void k_vec(VecArgs<T> a) {
 	int64_t newly = 0;
 	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < a.n;
 		 i += int64_t(gridDim.x) * blockDim.x) {
@@ -96,14 +148,14 @@ __global__ void k_vec(VecArgs a) {
 		const bool zh = a.za == nullptr || a.za[i] != 0;
 		const bool xh = a.x == nullptr || a.xa == nullptr || a.xa[i] != 0;
 		const bool yh = a.y == nullptr || a.ya == nullptr || a.ya[i] != 0;
-		const double xv = a.x ? (xh ? ld_val(a.x, a.xt, i) : 0.0) : a.alpha;
-		const double yv = a.y ? (yh ? ld_val(a.y, a.yt, i) : 0.0) : a.beta;
+		const T xv = a.x ? (xh ? ld_as<T>(a.x, a.xt, i) : T(0)) : a.alpha;
+		const T yv = a.y ? (yh ? ld_as<T>(a.y, a.yt, i) : T(0)) : a.beta;
 		bool write = false, assign = false;
-		double out = 0.0;
+		T out = T(0);
 		switch (a.kind) {
 		case ALPB_VEC_SET:  // z_i = x_i (or i under use_index) where x is present
 			if (xh) {
-				out = (a.descr & ALPB_DESC_USE_INDEX) ? double(i) : xv;
+				out = (a.descr & ALPB_DESC_USE_INDEX) ? T(i) : xv;
 				write = true;
 				assign = true;
 			}
@@ -112,41 +164,41 @@ __global__ void k_vec(VecArgs a) {
 		case ALPB_VEC_FOLDR:  // z_i = x_i op z_i
 			if (!xh) break;
 			if (zh) {
-				const double zv = ld_val(a.z, a.zt, i);
-				if (opd_skips(a.op, a.kind == ALPB_VEC_FOLDL ? xv : zv)) break;
-				out = a.kind == ALPB_VEC_FOLDL ? opd(a.op, zv, xv) : opd(a.op, xv, zv);
+				const T zv = ld_as<T>(a.z, a.zt, i);
+				if (opv_skips(a.op, a.kind == ALPB_VEC_FOLDL ? xv : zv)) break;
+				out = a.kind == ALPB_VEC_FOLDL ? opv(a.op, zv, xv) : opv(a.op, xv, zv);
 				write = true;
 			} else if (a.monoid) {
 				// monoid fold into an absent entry: identity op x_i (a scalar x
 				// reaches every absent entry, reference/blas1.hpp:957-981)
-				out = a.kind == ALPB_VEC_FOLDL ? opd(a.op, a.identity, xv) : opd(a.op, xv, a.identity);
+				out = a.kind == ALPB_VEC_FOLDL ? opv(a.op, a.identity, xv) : opv(a.op, xv, a.identity);
 				write = true;
 				assign = true;
 			}
 			break;
 		case ALPB_VEC_APPLY:  // z_i = x_i op y_i: operator = intersection, monoid = union
 			if (xh && yh) {
-				if (opd_skips(a.op, yv)) break;
-				out = opd(a.op, xv, yv);
+				if (opv_skips(a.op, yv)) break;
+				out = opv(a.op, xv, yv);
 				write = true;
 				assign = true;
 			}
 			else if (a.monoid && (xh || yh)) {
-				out = xh ? opd(a.op, xv, a.identity) : opd(a.op, a.identity, yv);
+				out = xh ? opv(a.op, xv, a.identity) : opv(a.op, a.identity, yv);
 				write = true;
 				assign = true;
 			}
 			break;
 		case ALPB_VEC_MULADD: {  // z_i = z_i (+) (x_i (*) y_i) over the ring
-			if (!(xh && yh) || opd_skips(a.mul_op, yv)) break;
-			const double prod = opd(a.mul_op, xv, yv);
-			if (zh) out = opd(a.op, ld_val(a.z, a.zt, i), prod);
+			if (!(xh && yh) || opv_skips(a.mul_op, yv)) break;
+			const T prod = opv(a.mul_op, xv, yv);
+			if (zh) out = opv(a.op, ld_as<T>(a.z, a.zt, i), prod);
 			else { out = prod; assign = true; }
 			write = true;
 			break;
 		}
 		}
-		if (write) st_val(a.z, a.zt, i, out);
+		if (write) st_as<T>(a.z, a.zt, i, out);
 		if (assign && a.za && !a.za[i]) {
 			a.za[i] = 1;
 			++newly;
@@ -176,106 +228,97 @@ __global__ void k_count_assigned(const uint8_t *a, int64_t n, int64_t *cnt) {
 	if ((threadIdx.x & 31) == 0 && c) atomicAdd((unsigned long long *) cnt, (unsigned long long) c);
 }
 
+template <class T>
+__device__ __forceinline__ T shfl_down_t(T v, int o) { return __shfl_down_sync(0xffffffffu, v, o); }
+
 // Typed reduction: partial[b] = (+)_i x_i (*) y_i over i where x, y (and the
 // mask) are present; y == nullptr means "no second operand" (plain fold).
-__global__ void k_vec_dot(int add_op, double ident, int mul_op, int64_t n, const void *x, int xt,
+template <class T>
+__global__ void k_vec_dot(int add_op, T ident, int mul_op, int64_t n, const void *x, int xt,
 	const uint8_t *xa, const void *y, int yt, const uint8_t *ya, const void *m,
-	const uint8_t *ma, int mt, int masked, uint32_t descr, double *partials) {
-	__shared__ double sm[32];
-	double acc = ident;
+	const uint8_t *ma, int mt, int masked, uint32_t descr, T *partials) {
+	__shared__ T sm[32];
+	T acc = ident;
 	bool any = false;
 	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
 		 i += int64_t(gridDim.x) * blockDim.x) {
 		if (xa && !xa[i]) continue;
 		if (y && ya && !ya[i]) continue;
 		if (masked && !eval_mask(m, ma, mt, descr, i)) continue;
-		const double xv = ld_val(x, xt, i);
-		const double yv = y ? ld_val(y, yt, i) : 0.0;
-		if (y && opd_skips(mul_op, yv)) continue;
-		const double t = y ? opd(mul_op, xv, yv) : xv;
-		acc = any ? opd(add_op, acc, t) : opd(add_op, ident, t);
+		const T xv = ld_as<T>(x, xt, i);
+		const T yv = y ? ld_as<T>(y, yt, i) : T(0);
+		if (y && opv_skips(mul_op, yv)) continue;
+		const T t = y ? opv(mul_op, xv, yv) : xv;
+		acc = any ? opv(add_op, acc, t) : opv(add_op, ident, t);
 		any = true;
 	}
 	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-	for (int o = 16; o > 0; o >>= 1) acc = opd(add_op, acc, __shfl_down_sync(0xffffffffu, acc, o));
+	for (int o = 16; o > 0; o >>= 1) acc = opv(add_op, acc, shfl_down_t(acc, o));
 	if (lane == 0) sm[wid] = acc;
 	__syncthreads();
 	if (wid == 0) {
-		double w = lane < int(blockDim.x >> 5) ? sm[lane] : ident;
-		for (int o = 16; o > 0; o >>= 1) w = opd(add_op, w, __shfl_down_sync(0xffffffffu, w, o));
+		T w = lane < int(blockDim.x >> 5) ? sm[lane] : ident;
+		for (int o = 16; o > 0; o >>= 1) w = opv(add_op, w, shfl_down_t(w, o));
 		if (lane == 0) partials[blockIdx.x] = w;
 	}
 }
 
-} // namespace alpb
+// *result = *result (+) partial[0] (+) ... (+) partial[g-1], in block order,
+// by one thread (the reference folds into the given scalar).
+template <class T>
+__global__ void k_vec_dot_finish(int add_op, const T *partials, int g, T *result) {
+	if (blockIdx.x != 0 || threadIdx.x != 0) return;
+	T acc = *result;
+	for (int b = 0; b < g; ++b) acc = opv(add_op, acc, partials[b]);
+	*result = acc;
+}
 
-using namespace alpb;
+template <class T>
+static T from_bits(uint64_t bits) {
+	T v;
+	memcpy(&v, &bits, sizeof(T));
+	return v;
+}
 
-extern "C" {
-
-int alpb_vec_reduce(double *result, int add_op, double identity, int mul_op, uint32_t descr,
-	int64_t n, const void *x, int x_type, const uint8_t *x_assigned, const void *y, int y_type,
-	const uint8_t *y_assigned, const void *mask, const uint8_t *mask_assigned, int mask_type,
-	int masked, void *stream) {
-	ALPB_CHECK(result != nullptr, ALPB_ILLEGAL, "alpb_vec_reduce: null result");
-	ALPB_CHECK(add_op >= ALPB_OP_ADD && add_op <= ALPB_OP_LAND && mul_op >= ALPB_OP_ADD &&
-		mul_op <= ALPB_OP_GEQ, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op,
-		mul_op);
-	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
-	cudaStream_t s = as_stream(stream);
+template <class T>
+static int vec_reduce_run(void *result, int add_op, uint64_t identity, int mul_op,
+	uint32_t descr, int64_t n, const void *x, int x_type, const uint8_t *x_assigned,
+	const void *y, int y_type, const uint8_t *y_assigned, const void *mask,
+	const uint8_t *mask_assigned, int mask_type, int masked, cudaStream_t s) {
 	int64_t g64 = (n + 256 * 8 - 1) / (256 * 8);
 	if (g64 > int64_t(sm_count()) * 4) g64 = int64_t(sm_count()) * 4;
 	const int g = int(g64 < 1 ? 1 : g64);
-	double *part = nullptr;
-	ALPB_CUDA(cudaMallocAsync(&part, size_t(g) * 8, s));
-	k_vec_dot<<<g, 256, 0, s>>>(add_op, identity, mul_op, n, x, x_type, x_assigned, y, y_type,
-		y_assigned, mask, mask_assigned, mask == nullptr ? ALPB_VOID : mask_type, masked, descr, part);
+	T *part = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&part, size_t(g + 1) * sizeof(T), s));
+	k_vec_dot<T><<<g, 256, 0, s>>>(add_op, from_bits<T>(identity), mul_op, n, x, x_type,
+		x_assigned, y, y_type, y_assigned, mask, mask_assigned,
+		mask == nullptr ? ALPB_VOID : mask_type, masked, descr, part);
 	ALPB_LAUNCHED();
-	std::vector<double> h(static_cast<size_t>(g));
-	ALPB_CUDA(cudaMemcpyAsync(h.data(), part, size_t(g) * 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaMemcpyAsync(part + g, result, sizeof(T), cudaMemcpyHostToDevice, s));
+	k_vec_dot_finish<T><<<1, 32, 0, s>>>(add_op, part, g, part + g);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cudaMemcpyAsync(result, part + g, sizeof(T), cudaMemcpyDeviceToHost, s));
 	ALPB_CUDA(cudaFreeAsync(part, s));
 	ALPB_CUDA(cudaStreamSynchronize(s));
-	double acc = *result;  // the reference folds into the given scalar
-	for (int b = 0; b < g; ++b) {
-		const double v = h[size_t(b)];
-		switch (add_op) {
-		case ALPB_OP_ADD: acc = acc + v; break;
-		case ALPB_OP_MUL: acc = acc * v; break;
-		case ALPB_OP_MIN: acc = acc < v ? acc : v; break;
-		case ALPB_OP_MAX: acc = acc > v ? acc : v; break;
-		case ALPB_OP_LOR: acc = (acc != 0 || v != 0) ? 1 : 0; break;
-		case ALPB_OP_LAND: acc = (acc != 0 && v != 0) ? 1 : 0; break;
-		default: acc = v; break;
-		}
-	}
-	*result = acc;
 	return ALPB_SUCCESS;
 }
 
-int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_op, uint32_t descr,
-	int64_t n, void *z, int z_type, uint8_t *z_assigned, int64_t *z_nnz,
+template <class T>
+static int vec_op_run(int kind, int op, int monoid, uint64_t identity, int mul_op,
+	uint32_t descr, int64_t n, void *z, int z_type, uint8_t *z_assigned, int64_t *z_nnz,
 	const void *mask, const uint8_t *mask_assigned, int mask_type, int masked,
-	const void *x, int x_type, const uint8_t *x_assigned, double alpha,
-	const void *y, int y_type, const uint8_t *y_assigned, double beta, void *stream) {
-	ALPB_CHECK(kind >= ALPB_VEC_SET && kind <= ALPB_VEC_MULADD, ALPB_ILLEGAL,
-		"alpb_vec_op: kind %d", kind);
-	ALPB_CHECK(op >= ALPB_OP_ADD && op <= ALPB_OP_GEQ, ALPB_UNSUPPORTED,
-		"alpb_vec_op: op %d", op);
-	ALPB_CHECK(type_size(z_type) > 0, ALPB_UNSUPPORTED, "alpb_vec_op: output type %d", z_type);
-	ALPB_CHECK(z_assigned == nullptr || z_nnz != nullptr, ALPB_ILLEGAL,
-		"alpb_vec_op: sparse output needs its nnz counter");
-	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
-	cudaStream_t s = as_stream(stream);
+	const void *x, int x_type, const uint8_t *x_assigned, uint64_t alpha,
+	const void *y, int y_type, const uint8_t *y_assigned, uint64_t beta, cudaStream_t s) {
 	if (kind == ALPB_VEC_APPLY && z_assigned) {
 		k_vec_clear_flags<<<grid_for(n, 256), 256, 0, s>>>(z_assigned, n);
 		ALPB_LAUNCHED();
 		ALPB_CUDA(cudaMemsetAsync(z_nnz, 0, 8, s));
 	}
-	VecArgs a;
+	VecArgs<T> a;
 	a.kind = kind;
 	a.op = op;
 	a.monoid = monoid;
-	a.identity = identity;
+	a.identity = from_bits<T>(identity);
 	a.descr = descr;
 	a.n = n;
 	a.z = z;
@@ -289,15 +332,102 @@ int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_op, uint3
 	a.x = x;
 	a.xt = x_type;
 	a.xa = x_assigned;
-	a.alpha = alpha;
+	a.alpha = from_bits<T>(alpha);
 	a.y = y;
 	a.yt = y_type;
 	a.ya = y_assigned;
-	a.beta = beta;
+	a.beta = from_bits<T>(beta);
 	a.mul_op = mul_op;
-	k_vec<<<grid_for(n, 256), 256, 0, s>>>(a);
+	k_vec<T><<<grid_for(n, 256), 256, 0, s>>>(a);
 	ALPB_LAUNCHED();
 	return ALPB_SUCCESS;
+}
+
+static uint64_t bits_of(double v) {
+	uint64_t b;
+	memcpy(&b, &v, 8);
+	return b;
+}
+
+} // namespace alpb
+
+using namespace alpb;
+
+extern "C" {
+
+int alpb_vec_reduce_dom(void *result, int add_op, uint64_t identity, int mul_op,
+	uint32_t descr, int domain, int64_t n, const void *x, int x_type, const uint8_t *x_assigned,
+	const void *y, int y_type, const uint8_t *y_assigned, const void *mask,
+	const uint8_t *mask_assigned, int mask_type, int masked, void *stream) {
+	ALPB_CHECK(result != nullptr, ALPB_ILLEGAL, "alpb_vec_reduce: null result");
+	ALPB_CHECK(add_op >= ALPB_OP_ADD && add_op <= ALPB_OP_LAND && mul_op >= ALPB_OP_ADD &&
+		mul_op <= ALPB_OP_GEQ, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op,
+		mul_op);
+	ALPB_CHECK(domain == ALPB_FP64 || domain == ALPB_INT64 || domain == ALPB_UINT64,
+		ALPB_UNSUPPORTED, "alpb_vec_reduce: domain %d", domain);
+	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
+	cudaStream_t s = as_stream(stream);
+	switch (domain) {
+	case ALPB_FP64:
+		return vec_reduce_run<double>(result, add_op, identity, mul_op, descr, n, x, x_type,
+			x_assigned, y, y_type, y_assigned, mask, mask_assigned, mask_type, masked, s);
+	case ALPB_INT64:
+		return vec_reduce_run<int64_t>(result, add_op, identity, mul_op, descr, n, x, x_type,
+			x_assigned, y, y_type, y_assigned, mask, mask_assigned, mask_type, masked, s);
+	default:
+		return vec_reduce_run<uint64_t>(result, add_op, identity, mul_op, descr, n, x, x_type,
+			x_assigned, y, y_type, y_assigned, mask, mask_assigned, mask_type, masked, s);
+	}
+}
+
+int alpb_vec_reduce(double *result, int add_op, double identity, int mul_op, uint32_t descr,
+	int64_t n, const void *x, int x_type, const uint8_t *x_assigned, const void *y, int y_type,
+	const uint8_t *y_assigned, const void *mask, const uint8_t *mask_assigned, int mask_type,
+	int masked, void *stream) {
+	return alpb_vec_reduce_dom(result, add_op, bits_of(identity), mul_op, descr, ALPB_FP64, n, x,
+		x_type, x_assigned, y, y_type, y_assigned, mask, mask_assigned, mask_type, masked, stream);
+}
+
+int alpb_vec_op_dom(int kind, int op, int monoid, uint64_t identity, int mul_op, uint32_t descr,
+	int domain, int64_t n, void *z, int z_type, uint8_t *z_assigned, int64_t *z_nnz,
+	const void *mask, const uint8_t *mask_assigned, int mask_type, int masked,
+	const void *x, int x_type, const uint8_t *x_assigned, uint64_t alpha,
+	const void *y, int y_type, const uint8_t *y_assigned, uint64_t beta, void *stream) {
+	ALPB_CHECK(kind >= ALPB_VEC_SET && kind <= ALPB_VEC_MULADD, ALPB_ILLEGAL,
+		"alpb_vec_op: kind %d", kind);
+	ALPB_CHECK(op >= ALPB_OP_ADD && op <= ALPB_OP_GEQ, ALPB_UNSUPPORTED,
+		"alpb_vec_op: op %d", op);
+	ALPB_CHECK(type_size(z_type) > 0, ALPB_UNSUPPORTED, "alpb_vec_op: output type %d", z_type);
+	ALPB_CHECK(z_assigned == nullptr || z_nnz != nullptr, ALPB_ILLEGAL,
+		"alpb_vec_op: sparse output needs its nnz counter");
+	ALPB_CHECK(domain == ALPB_FP64 || domain == ALPB_INT64 || domain == ALPB_UINT64,
+		ALPB_UNSUPPORTED, "alpb_vec_op: domain %d", domain);
+	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
+	cudaStream_t s = as_stream(stream);
+	switch (domain) {
+	case ALPB_FP64:
+		return vec_op_run<double>(kind, op, monoid, identity, mul_op, descr, n, z, z_type,
+			z_assigned, z_nnz, mask, mask_assigned, mask_type, masked, x, x_type, x_assigned, alpha,
+			y, y_type, y_assigned, beta, s);
+	case ALPB_INT64:
+		return vec_op_run<int64_t>(kind, op, monoid, identity, mul_op, descr, n, z, z_type,
+			z_assigned, z_nnz, mask, mask_assigned, mask_type, masked, x, x_type, x_assigned, alpha,
+			y, y_type, y_assigned, beta, s);
+	default:
+		return vec_op_run<uint64_t>(kind, op, monoid, identity, mul_op, descr, n, z, z_type,
+			z_assigned, z_nnz, mask, mask_assigned, mask_type, masked, x, x_type, x_assigned, alpha,
+			y, y_type, y_assigned, beta, s);
+	}
+}
+
+int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_op, uint32_t descr,
+	int64_t n, void *z, int z_type, uint8_t *z_assigned, int64_t *z_nnz,
+	const void *mask, const uint8_t *mask_assigned, int mask_type, int masked,
+	const void *x, int x_type, const uint8_t *x_assigned, double alpha,
+	const void *y, int y_type, const uint8_t *y_assigned, double beta, void *stream) {
+	return alpb_vec_op_dom(kind, op, monoid, bits_of(identity), mul_op, descr, ALPB_FP64, n, z,
+		z_type, z_assigned, z_nnz, mask, mask_assigned, mask_type, masked, x, x_type, x_assigned,
+		bits_of(alpha), y, y_type, y_assigned, bits_of(beta), stream);
 }
 
 int alpb_count_assigned(const uint8_t *assigned, int64_t n, int64_t *count, void *stream) {

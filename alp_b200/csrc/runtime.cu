@@ -41,6 +41,7 @@ size_t type_size(int type) {
 	case ALPB_INT64: return 8;
 	case ALPB_UINT8: return 1;
 	case ALPB_INT8: return 1;
+	case ALPB_UINT64: return 8;
 	}
 	return 0;
 }

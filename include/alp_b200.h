@@ -77,7 +77,9 @@ enum alpb_type {
 	ALPB_UINT32 = 4,
 	ALPB_INT64 = 5,
 	ALPB_UINT8 = 6,  /* unsigned char                                */
-	ALPB_INT8 = 7    /* char / signed char                           */
+	ALPB_INT8 = 7,   /* char / signed char                           */
+	ALPB_UINT64 = 8  /* size_t; also the unsigned 64-bit compute domain of
+	                    alpb_vec_op_dom / alpb_vec_reduce_dom            */
 };
 
 /*
@@ -385,11 +387,31 @@ ALPB_API int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_
 /* *result = *result (+) [(+)_i x_i (*) y_i] over the indices where x, y (y may
  * be NULL: a plain fold of x) and the mask are present; values of any type
  * code, computed in double; identity is the additive monoid's.  Covers
- * grb::dot and the vector-to-scalar grb::foldl / foldr (masked or not). */
+ * grb::dot and the vector-to-scalar grb::foldl / foldr (masked or not).
+ * (alpb_vec_op and alpb_vec_reduce compute in double: the FP64 domain of the
+ * two _dom forms below.) */
 ALPB_API int alpb_vec_reduce(double *result, int add_op, double identity, int mul_op,
 	uint32_t descr, int64_t n, const void *x, int x_type, const uint8_t *x_assigned,
 	const void *y, int y_type, const uint8_t *y_assigned, const void *mask,
 	const uint8_t *mask_assigned, int mask_type, int masked, void *stream);
+/* The same two primitives computing in the operator's own domain: `domain` is
+ * ALPB_FP64 (double), ALPB_INT64 (int64_t) or ALPB_UINT64 (uint64_t); the C++
+ * backend passes the domain of the ALP operator (its D3 type), as the
+ * reference's operators cast their operands to it.  Integer domains compute
+ * exactly with two's-complement wrap-around, and a narrower output type
+ * truncates (int32 results wrap as 32-bit arithmetic does).  identity, alpha
+ * and beta are the bits of a value of the domain type (memcpy of a double,
+ * int64_t or uint64_t); *result of the reduction is a value of the domain type
+ * (in: the scalar folded into; out: the result), folded on the device. */
+ALPB_API int alpb_vec_op_dom(int kind, int op, int monoid, uint64_t identity, int mul_op,
+	uint32_t descr, int domain, int64_t n, void *z, int z_type, uint8_t *z_assigned,
+	int64_t *z_nnz, const void *mask, const uint8_t *mask_assigned, int mask_type, int masked,
+	const void *x, int x_type, const uint8_t *x_assigned, uint64_t alpha,
+	const void *y, int y_type, const uint8_t *y_assigned, uint64_t beta, void *stream);
+ALPB_API int alpb_vec_reduce_dom(void *result, int add_op, uint64_t identity, int mul_op,
+	uint32_t descr, int domain, int64_t n, const void *x, int x_type,
+	const uint8_t *x_assigned, const void *y, int y_type, const uint8_t *y_assigned,
+	const void *mask, const uint8_t *mask_assigned, int mask_type, int masked, void *stream);
 /* number of assigned entries (synchronises). */
 ALPB_API int alpb_count_assigned(const uint8_t *assigned, int64_t n, int64_t *count,
 	void *stream);

@@ -1,8 +1,10 @@
 /*
  * Level-1 primitives of the b200 backend (reference: graphblas/reference/
- * blas1.hpp).  Every primitive runs on the device through alpb_vec_op /
- * alpb_vec_reduce with ALP's sparse semantics and returns once the result is
- * in place (blocking execution).  Operators and monoids are those of
+ * blas1.hpp).  Every primitive runs on the device through alpb_vec_op_dom /
+ * alpb_vec_reduce_dom with ALP's sparse semantics and returns once the result
+ * is in place (blocking execution).  Values are computed in the operands'
+ * domain (internal::b200rt::domain_of): double, or exact 64-bit integers with
+ * wrap-around, so integer primitives give the reference's bits.  Operators and monoids are those of
  * graphblas/ops.hpp that have a device code (internal::b200rt::op_code); any
  * other operator, or a domain without a device type, gives UNSUPPORTED.
  *
@@ -31,19 +33,21 @@ namespace grb {
 			template< class Monoid >
 			struct monoid_code {
 				static constexpr int value = op_code< typename Monoid::Operator >::value;
-				static double identity() {
-					return static_cast< double >( Monoid().template getIdentity< double >() );
+				/** The identity in the monoid's own domain (exact as a scalar_t). */
+				static scalar_t identity() {
+					return static_cast< scalar_t >(
+						Monoid().template getIdentity< typename Monoid::D3 >() );
 				}
 			};
 
-			/** z <- kind(z, x, y) through alpb_vec_op; x / y may be scalars. */
+			/** z <- kind(z, x, y) through alpb_vec_op_dom; x / y may be scalars. */
 			template< Descriptor descr, typename Z, typename X, typename Y, typename M,
 				typename Coords >
-			RC vec_op( const int kind, const int op, const bool monoid, const double identity,
+			RC vec_op( const int kind, const int op, const bool monoid, const scalar_t identity,
 				const int mul_op, Vector< Z, grb::b200, Coords > &z,
 				const Vector< M, grb::b200, typename nd< Coords >::type > * const mask,
-				const Vector< X, grb::b200, typename nd< Coords >::type > * const x, const double alpha,
-				const Vector< Y, grb::b200, typename nd< Coords >::type > * const y, const double beta
+				const Vector< X, grb::b200, typename nd< Coords >::type > * const x, const scalar_t alpha,
+				const Vector< Y, grb::b200, typename nd< Coords >::type > * const y, const scalar_t beta
 			) {
 				const size_t n = z.b200_size();
 				if( mask && size( *mask ) > 0 && size( *mask ) != n ) { return MISMATCH; }
@@ -66,24 +70,28 @@ namespace grb {
 				if( masked ) { mask->b200_device_ready(); }
 				// a dense output stays dense unless eWiseApply may drop entries
 				const bool out_sparse = !z.b200_dense() || kind == ALPB_VEC_APPLY;
-				const RC rc = check( alpb_vec_op( kind, op, monoid ? 1 : 0, identity, mul_op, descr, n,
+				// the operands' domain: integer operators compute exactly on the device
+				constexpr int dom = domain_of< Z, X, Y >::value;
+				const RC rc = check( alpb_vec_op_dom( kind, op, monoid ? 1 : 0,
+					domain_bits( identity, dom ), mul_op, descr, dom, n,
 					z.b200_values(), zt, out_sparse ? z.b200_flags() : nullptr,
 					out_sparse ? z.b200_counter() : nullptr,
 					masked ? mask->b200_values() : nullptr,
 					masked ? mask->b200_flags_or_dense() : nullptr, mt, masked ? 1 : 0,
-					x ? x->b200_values() : nullptr, xt, x ? x->b200_flags_or_dense() : nullptr, alpha,
-					y ? y->b200_values() : nullptr, yt, y ? y->b200_flags_or_dense() : nullptr, beta,
-					stream() ), "blas1" );
+					x ? x->b200_values() : nullptr, xt, x ? x->b200_flags_or_dense() : nullptr,
+					domain_bits( alpha, dom ),
+					y ? y->b200_values() : nullptr, yt, y ? y->b200_flags_or_dense() : nullptr,
+					domain_bits( beta, dom ), stream() ), "blas1" );
 				(void) alpb_stream_sync( stream() );
 				if( kind == ALPB_VEC_APPLY ) { z.b200_mark_sparse(); }
 				z.b200_refresh();
 				return rc;
 			}
 
-			/** *out (+)= reduce( x (*) y ) through alpb_vec_reduce. */
+			/** *out (+)= reduce( x (*) y ) through alpb_vec_reduce_dom. */
 			template< Descriptor descr, typename OutT, typename X, typename Y, typename M,
 				typename Coords >
-			RC vec_reduce( OutT &out, const int add_op, const double identity, const int mul_op,
+			RC vec_reduce( OutT &out, const int add_op, const scalar_t identity, const int mul_op,
 				const Vector< X, grb::b200, Coords > &x,
 				const Vector< Y, grb::b200, typename nd< Coords >::type > * const y,
 				const Vector< M, grb::b200, typename nd< Coords >::type > * const mask
@@ -103,13 +111,15 @@ namespace grb {
 				x.b200_device_ready();
 				if( y ) { y->b200_device_ready(); }
 				if( masked ) { mask->b200_device_ready(); }
-				double r = static_cast< double >( out );
-				const RC rc = check( alpb_vec_reduce( &r, add_op, identity, mul_op, descr, n,
-					x.b200_values(), xt, x.b200_flags_or_dense(),
+				// folded on the device in the operands' domain, exactly for integers
+				constexpr int dom = domain_of< OutT, X, Y >::value;
+				uint64_t r = domain_bits( static_cast< scalar_t >( out ), dom );
+				const RC rc = check( alpb_vec_reduce_dom( &r, add_op, domain_bits( identity, dom ),
+					mul_op, descr, dom, n, x.b200_values(), xt, x.b200_flags_or_dense(),
 					y ? y->b200_values() : nullptr, yt, y ? y->b200_flags_or_dense() : nullptr,
 					masked ? mask->b200_values() : nullptr, masked ? mask->b200_flags_or_dense() : nullptr,
 					mt, masked ? 1 : 0, stream() ), "reduce" );
-				if( rc == SUCCESS ) { out = static_cast< OutT >( r ); }
+				if( rc == SUCCESS ) { out = from_domain_bits< OutT >( r, dom ); }
 				return rc;
 			}
 
@@ -207,7 +217,7 @@ namespace grb {
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDL,
 			internal::b200rt::op_code< Op >::value, false, 0.0, 0, x, nullptr, nullptr,
-			static_cast< double >( beta ), nullptr, 0.0 );
+			static_cast< internal::b200rt::scalar_t >( beta ), nullptr, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
@@ -224,7 +234,7 @@ namespace grb {
 		// absent entries take beta (reference/blas1.hpp:957-981)
 		return vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDL,
 			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, x, nullptr,
-			nullptr, static_cast< double >( beta ), nullptr, 0.0 );
+			nullptr, static_cast< internal::b200rt::scalar_t >( beta ), nullptr, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Op, typename IOType,
@@ -239,7 +249,7 @@ namespace grb {
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, IOType, IOType, IOType, MaskType >( ALPB_VEC_FOLDL,
 			internal::b200rt::op_code< Op >::value, false, 0.0, 0, x, &m, nullptr,
-			static_cast< double >( beta ), nullptr, 0.0 );
+			static_cast< internal::b200rt::scalar_t >( beta ), nullptr, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
@@ -257,7 +267,7 @@ namespace grb {
 		using namespace internal::b200rt;
 		return vec_op< descr, IOType, IOType, IOType, MaskType >( ALPB_VEC_FOLDL,
 			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, x, &m, nullptr,
-			static_cast< double >( beta ), nullptr, 0.0 );
+			static_cast< internal::b200rt::scalar_t >( beta ), nullptr, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Monoid, typename IOType,
@@ -273,7 +283,7 @@ namespace grb {
 		using namespace internal::b200rt;
 		return vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDR,
 			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, y, nullptr,
-			nullptr, static_cast< double >( alpha ), nullptr, 0.0 );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), nullptr, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class OP, typename IOType,
@@ -288,7 +298,7 @@ namespace grb {
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, IOType, IOType, IOType, bool >( ALPB_VEC_FOLDR,
 			internal::b200rt::op_code< OP >::value, false, 0.0, 0, y, nullptr, nullptr,
-			static_cast< double >( alpha ), nullptr, 0.0 );
+			static_cast< internal::b200rt::scalar_t >( alpha ), nullptr, 0.0 );
 	}
 
 	// ------------------------------------------------- vector -> vector fold --
@@ -444,7 +454,7 @@ namespace grb {
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, OutputType, InputType1, InputType1, bool >(
 			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, nullptr, &x, 0.0,
-			nullptr, static_cast< double >( beta ) );
+			nullptr, static_cast< internal::b200rt::scalar_t >( beta ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
@@ -464,7 +474,7 @@ namespace grb {
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, OutputType, InputType2, InputType2, bool >(
 			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, nullptr, nullptr,
-			static_cast< double >( alpha ), &y, 0.0 );
+			static_cast< internal::b200rt::scalar_t >( alpha ), &y, 0.0 );
 	}
 
 	// two scalars: z is set to alpha (.) beta, everywhere or under the mask
@@ -545,7 +555,7 @@ namespace grb {
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, OutputType, InputType1, InputType1, MaskType >(
 			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, &mask, &x, 0.0,
-			nullptr, static_cast< double >( beta ) );
+			nullptr, static_cast< internal::b200rt::scalar_t >( beta ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
@@ -564,7 +574,7 @@ namespace grb {
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::vec_op< descr, OutputType, InputType2, InputType2, MaskType >(
 			ALPB_VEC_APPLY, internal::b200rt::op_code< OP >::value, false, 0.0, 0, z, &mask, nullptr,
-			static_cast< double >( alpha ), &y, 0.0 );
+			static_cast< internal::b200rt::scalar_t >( alpha ), &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class OP, typename OutputType,
@@ -623,7 +633,7 @@ namespace grb {
 		using namespace internal::b200rt;
 		return vec_op< descr, OutputType, InputType1, InputType1, bool >( ALPB_VEC_APPLY,
 			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, nullptr, &x,
-			0.0, nullptr, static_cast< double >( beta ) );
+			0.0, nullptr, static_cast< internal::b200rt::scalar_t >( beta ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
@@ -640,7 +650,7 @@ namespace grb {
 		using namespace internal::b200rt;
 		return vec_op< descr, OutputType, InputType2, InputType2, bool >( ALPB_VEC_APPLY,
 			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, nullptr,
-			nullptr, static_cast< double >( alpha ), &y, 0.0 );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
@@ -659,7 +669,7 @@ namespace grb {
 		using namespace internal::b200rt;
 		return vec_op< descr, OutputType, InputType1, InputType1, MaskType >( ALPB_VEC_APPLY,
 			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, &mask, &x,
-			0.0, nullptr, static_cast< double >( beta ) );
+			0.0, nullptr, static_cast< internal::b200rt::scalar_t >( beta ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Monoid, typename OutputType,
@@ -679,7 +689,7 @@ namespace grb {
 		using namespace internal::b200rt;
 		return vec_op< descr, OutputType, InputType2, InputType2, MaskType >( ALPB_VEC_APPLY,
 			monoid_code< Monoid >::value, true, monoid_code< Monoid >::identity(), 0, z, &mask,
-			nullptr, static_cast< double >( alpha ), &y, 0.0 );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), &y, 0.0 );
 	}
 
 	// ------------------------------------------------------------- eWiseMul --
@@ -699,7 +709,7 @@ namespace grb {
 		return vec_op< descr, OutputType, InputType2, InputType2, bool >( ALPB_VEC_MULADD,
 			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
 			op_code< typename Ring::MultiplicativeOperator >::value, z, nullptr, nullptr,
-			static_cast< double >( alpha ), &y, 0.0 );
+			static_cast< internal::b200rt::scalar_t >( alpha ), &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
@@ -734,7 +744,7 @@ namespace grb {
 		return vec_op< descr, OutputType, InputType1, InputType1, bool >( ALPB_VEC_MULADD,
 			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
 			op_code< typename Ring::MultiplicativeOperator >::value, z, nullptr, &x, 0.0, nullptr,
-			static_cast< double >( beta ) );
+			static_cast< internal::b200rt::scalar_t >( beta ) );
 	}
 
 	/** z = z (+) (alpha (*) beta): nothing when either is the ring's zero, else
@@ -800,7 +810,7 @@ namespace grb {
 		return vec_op< descr, OutputType, InputType2, InputType2, MaskType >( ALPB_VEC_MULADD,
 			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
 			op_code< typename Ring::MultiplicativeOperator >::value, z, &m, nullptr,
-			static_cast< double >( alpha ), &y, 0.0 );
+			static_cast< internal::b200rt::scalar_t >( alpha ), &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
@@ -824,7 +834,7 @@ namespace grb {
 		return vec_op< descr, OutputType, InputType1, InputType1, MaskType >( ALPB_VEC_MULADD,
 			op_code< typename Ring::AdditiveOperator >::value, false, 0.0,
 			op_code< typename Ring::MultiplicativeOperator >::value, z, &m, &x, 0.0, nullptr,
-			static_cast< double >( beta ) );
+			static_cast< internal::b200rt::scalar_t >( beta ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename InputType1,
@@ -858,23 +868,31 @@ namespace grb {
 				typename M, typename Coords >
 			RC muladd( Vector< Z, grb::b200, Coords > &z,
 				const Vector< M, grb::b200, typename nd< Coords >::type > * const mask,
-				const Vector< A, grb::b200, typename nd< Coords >::type > * const a, const double alpha,
-				const Vector< X, grb::b200, typename nd< Coords >::type > * const x, const double chi,
-				const Vector< Y, grb::b200, typename nd< Coords >::type > * const y, const double gamma
+				const Vector< A, grb::b200, typename nd< Coords >::type > * const a, const scalar_t alpha,
+				const Vector< X, grb::b200, typename nd< Coords >::type > * const x, const scalar_t chi,
+				const Vector< Y, grb::b200, typename nd< Coords >::type > * const y, const scalar_t gamma
 			) {
 				const int add = op_code< typename Ring::AdditiveOperator >::value;
 				const int mul = op_code< typename Ring::MultiplicativeOperator >::value;
-				const double zero = static_cast< double >( Ring().template getZero< Z >() );
+				const scalar_t zero = static_cast< scalar_t >( Ring().template getZero< Z >() );
 				RC rc;
 				if( !a && !x ) {
 					// both scalars: fold the constant product into every entry
 					rc = vec_op< descr, Z, Z, Z, M >( ALPB_VEC_FOLDL, add, false, zero, 0, z, mask,
 						nullptr, 0.0, nullptr, 0.0 );
-					const double p = 0.0;
-					(void) p;
 					if( rc == SUCCESS ) {
+						// the constant product, formed in Z as the ring's operator would
+						Z prod;
+						if( std::is_floating_point< Z >::value ) {
+							prod = static_cast< Z >( static_cast< double >( alpha ) *
+								static_cast< double >( chi ) );
+						} else {
+							const uint64_t pa = domain_bits( alpha, ALPB_UINT64 ),
+								pc = domain_bits( chi, ALPB_UINT64 );
+							prod = static_cast< Z >( pa * pc );   // wraps, as integer products do
+						}
 						Vector< Z, grb::b200, Coords > c( z.b200_size() );
-						rc = set< descriptors::no_operation >( c, static_cast< Z >( alpha * chi ) );
+						rc = set< descriptors::no_operation >( c, prod );
 						if( rc == SUCCESS ) {
 							rc = vec_op< descr, Z, Z, Z, M >( ALPB_VEC_FOLDL, add, true, zero, 0, z, mask,
 								&c, 0.0, nullptr, 0.0 );
@@ -914,7 +932,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, OutputType, OutputType, bool >( z, nullptr,
-			nullptr, static_cast< double >( alpha ), nullptr, static_cast< double >( chi ), nullptr, static_cast< double >( gamma ) );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), nullptr, static_cast< internal::b200rt::scalar_t >( chi ), nullptr, static_cast< internal::b200rt::scalar_t >( gamma ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -932,7 +950,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, OutputType, InputType3, bool >( z, nullptr,
-			nullptr, static_cast< double >( alpha ), nullptr, static_cast< double >( chi ), &y, 0.0 );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), nullptr, static_cast< internal::b200rt::scalar_t >( chi ), &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -950,7 +968,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, InputType2, OutputType, bool >( z, nullptr,
-			nullptr, static_cast< double >( alpha ), &x, 0.0, nullptr, static_cast< double >( gamma ) );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), &x, 0.0, nullptr, static_cast< internal::b200rt::scalar_t >( gamma ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -967,7 +985,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, InputType2, InputType3, bool >( z, nullptr,
-			nullptr, static_cast< double >( alpha ), &x, 0.0, &y, 0.0 );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), &x, 0.0, &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -985,7 +1003,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, OutputType, OutputType, bool >( z, nullptr,
-			&a, 0.0, nullptr, static_cast< double >( chi ), nullptr, static_cast< double >( gamma ) );
+			&a, 0.0, nullptr, static_cast< internal::b200rt::scalar_t >( chi ), nullptr, static_cast< internal::b200rt::scalar_t >( gamma ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1002,7 +1020,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, OutputType, InputType3, bool >( z, nullptr,
-			&a, 0.0, nullptr, static_cast< double >( chi ), &y, 0.0 );
+			&a, 0.0, nullptr, static_cast< internal::b200rt::scalar_t >( chi ), &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1019,7 +1037,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, InputType2, OutputType, bool >( z, nullptr,
-			&a, 0.0, &x, 0.0, nullptr, static_cast< double >( gamma ) );
+			&a, 0.0, &x, 0.0, nullptr, static_cast< internal::b200rt::scalar_t >( gamma ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1056,7 +1074,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, OutputType, OutputType, MaskType >( z, &m,
-			nullptr, static_cast< double >( alpha ), nullptr, static_cast< double >( chi ), nullptr, static_cast< double >( gamma ) );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), nullptr, static_cast< internal::b200rt::scalar_t >( chi ), nullptr, static_cast< internal::b200rt::scalar_t >( gamma ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1076,7 +1094,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, OutputType, InputType3, MaskType >( z, &m,
-			nullptr, static_cast< double >( alpha ), nullptr, static_cast< double >( chi ), &y, 0.0 );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), nullptr, static_cast< internal::b200rt::scalar_t >( chi ), &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1096,7 +1114,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, InputType2, OutputType, MaskType >( z, &m,
-			nullptr, static_cast< double >( alpha ), &x, 0.0, nullptr, static_cast< double >( gamma ) );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), &x, 0.0, nullptr, static_cast< internal::b200rt::scalar_t >( gamma ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1115,7 +1133,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, OutputType, InputType2, InputType3, MaskType >( z, &m,
-			nullptr, static_cast< double >( alpha ), &x, 0.0, &y, 0.0 );
+			nullptr, static_cast< internal::b200rt::scalar_t >( alpha ), &x, 0.0, &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1135,7 +1153,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, OutputType, OutputType, MaskType >( z, &m,
-			&a, 0.0, nullptr, static_cast< double >( chi ), nullptr, static_cast< double >( gamma ) );
+			&a, 0.0, nullptr, static_cast< internal::b200rt::scalar_t >( chi ), nullptr, static_cast< internal::b200rt::scalar_t >( gamma ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1154,7 +1172,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, OutputType, InputType3, MaskType >( z, &m,
-			&a, 0.0, nullptr, static_cast< double >( chi ), &y, 0.0 );
+			&a, 0.0, nullptr, static_cast< internal::b200rt::scalar_t >( chi ), &y, 0.0 );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >
@@ -1173,7 +1191,7 @@ namespace grb {
 		(void) ring;
 		if( phase == RESIZE ) { return SUCCESS; }
 		return internal::b200rt::muladd< descr, Ring, OutputType, InputType1, InputType2, OutputType, MaskType >( z, &m,
-			&a, 0.0, &x, 0.0, nullptr, static_cast< double >( gamma ) );
+			&a, 0.0, &x, 0.0, nullptr, static_cast< internal::b200rt::scalar_t >( gamma ) );
 	}
 
 	template< Descriptor descr = descriptors::no_operation, class Ring, typename OutputType, typename MaskType, typename InputType1, typename InputType2, typename InputType3, typename Coords >

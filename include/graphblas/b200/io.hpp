@@ -117,7 +117,8 @@ namespace grb {
 	namespace internal {
 		namespace b200rt {
 
-			/** z = value over `mask` (or everywhere) through alpb_vec_op. */
+			/** z = value over `mask` (or everywhere) through alpb_vec_op_dom (or
+			 *  alpb_set_scalar for values a double holds exactly). */
 			template< Descriptor descr, typename DataType, typename MaskType, typename T,
 				typename Coords >
 			RC set_scalar( Vector< DataType, grb::b200, Coords > &x,
@@ -142,18 +143,22 @@ namespace grb {
 					const RC crc = clear( x );
 					if( crc != SUCCESS ) { return crc; }
 				}
-				if( !mask && !( descr & descriptors::use_index ) ) {
+				// a 64-bit integer value does not fit a double: it takes the typed path
+				constexpr int dom = domain_of< DataType, T >::value;
+				if( !mask && !( descr & descriptors::use_index ) &&
+					!( std::is_integral< DataType >::value && sizeof( DataType ) == 8 )
+				) {
 					const RC rc = check( alpb_set_scalar( x.b200_values(), zt, n, static_cast< double >( val ),
 						x.b200_flags(), x.b200_counter(), stream() ), "set" );
 					if( rc == SUCCESS ) { x.b200_mark_dense(); }
 					return rc;
 				}
-				const RC rc = check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0,
-					descr, n, x.b200_values(), zt, x.b200_flags(), x.b200_counter(),
+				const RC rc = check( alpb_vec_op_dom( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0, 0,
+					descr, dom, n, x.b200_values(), zt, x.b200_flags(), x.b200_counter(),
 					mask ? mask->b200_values() : nullptr,
 					mask ? mask->b200_flags_or_dense() : nullptr, mt, mask ? 1 : 0,
-					nullptr, zt, nullptr, static_cast< double >( val ),
-					nullptr, zt, nullptr, 0.0, stream() ), "set" );
+					nullptr, zt, nullptr, domain_bits( static_cast< scalar_t >( val ), dom ),
+					nullptr, zt, nullptr, 0, stream() ), "set" );
 				x.b200_refresh();
 				return rc;
 			}
@@ -226,9 +231,10 @@ namespace grb {
 		y.b200_device_ready();
 		RC rc = clear( x );
 		if( rc != SUCCESS ) { return rc; }
-		rc = check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0, descr, n,
+		rc = check( alpb_vec_op_dom( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0, 0, descr,
+			domain_of< OutputType, InputType >::value, n,
 			x.b200_values(), zt, x.b200_flags(), x.b200_counter(), nullptr, nullptr, ALPB_VOID, 0,
-			y.b200_values(), yt, y.b200_flags_or_dense(), 0.0, nullptr, zt, nullptr, 0.0, stream() ),
+			y.b200_values(), yt, y.b200_flags_or_dense(), 0, nullptr, zt, nullptr, 0, stream() ),
 			"set (vector)" );
 		x.b200_refresh();
 		return rc;
@@ -267,10 +273,11 @@ namespace grb {
 			const RC crc = clear( x );
 			if( crc != SUCCESS ) { return crc; }
 		}
-		const RC rc = check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0, descr, n,
+		const RC rc = check( alpb_vec_op_dom( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0, 0, descr,
+			domain_of< OutputType, InputType >::value, n,
 			x.b200_values(), zt, x.b200_flags(), x.b200_counter(), mask.b200_values(),
-			mask.b200_flags_or_dense(), mt, 1, y.b200_values(), yt, y.b200_flags_or_dense(), 0.0,
-			nullptr, zt, nullptr, 0.0, stream() ), "set (masked vector)" );
+			mask.b200_flags_or_dense(), mt, 1, y.b200_values(), yt, y.b200_flags_or_dense(), 0,
+			nullptr, zt, nullptr, 0, stream() ), "set (masked vector)" );
 		x.b200_refresh();
 		return rc;
 	}

@@ -273,10 +273,10 @@ namespace grb {
 						"set (matrix indices)" ) );
 					if( dt == ALPB_VOID ) { return; }
 					dst.values = alloc< storage_type >( nz );
-					keep( check( alpb_vec_op( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0.0, 0, 0,
-						static_cast< int64_t >( nz ), dst.values, dt, nullptr, nullptr, nullptr, nullptr,
-						ALPB_VOID, 0, src.values, st, nullptr, 0.0, nullptr, st, nullptr, 0.0, stream() ),
-						"set (matrix values)" ) );
+					keep( check( alpb_vec_op_dom( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0, 0, 0,
+						domain_of< D, D2 >::value, static_cast< int64_t >( nz ), dst.values, dt, nullptr,
+						nullptr, nullptr, nullptr, ALPB_VOID, 0, src.values, st, nullptr, 0, nullptr, st,
+						nullptr, 0, stream() ), "set (matrix values)" ) );
 				};
 				one( _crs, A.b200_crs(), m );
 				one( _ccs, A.b200_ccs(), n );

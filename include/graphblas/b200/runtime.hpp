@@ -168,6 +168,68 @@ namespace grb {
 				static constexpr int value = ALPB_RING_TIMES_PLUS_F64;
 			};
 
+			/** Host scalar that holds every double and every 64-bit integer
+			 *  exactly (a 64-bit or wider significand), so that scalars reach the
+			 *  device unrounded in whichever domain the primitive computes. */
+			typedef long double scalar_t;
+			static_assert( std::numeric_limits< long double >::digits >= 64,
+				"the b200 backend needs a long double with a 64-bit significand" );
+
+			/** Compute domain of an element-wise primitive over operands of these
+			 *  C++ types, as the reference's operators cast to their domain:
+			 *  ALPB_FP64 when any is floating point, else ALPB_UINT64 when any is
+			 *  an unsigned 64-bit integer, else ALPB_INT64 (exact for bool and
+			 *  every narrower integer). */
+			template< typename... T >
+			struct domain_of {
+				static constexpr bool fp = false, u64 = false;
+				static constexpr int value = ALPB_INT64;
+			};
+			template< typename H, typename... T >
+			struct domain_of< H, T... > {
+				static constexpr bool fp = std::is_floating_point< H >::value || domain_of< T... >::fp;
+				static constexpr bool u64 = ( std::is_integral< H >::value &&
+					std::is_unsigned< H >::value && sizeof( H ) == 8 ) || domain_of< T... >::u64;
+				static constexpr int value = fp ? ALPB_FP64 : ( u64 ? ALPB_UINT64 : ALPB_INT64 );
+			};
+
+			/** The bits of v as a value of domain `dom`.  Integer domains clamp to
+			 *  their range: an infinite identity (of min or max) becomes the
+			 *  domain's extreme, which is that identity there. */
+			inline uint64_t domain_bits( const scalar_t v, const int dom ) {
+				uint64_t b = 0;
+				if( dom == ALPB_FP64 ) {
+					const double d = static_cast< double >( v );
+					std::memcpy( &b, &d, 8 );
+				} else if( dom == ALPB_INT64 ) {
+					const scalar_t lo = static_cast< scalar_t >( std::numeric_limits< int64_t >::min() );
+					const scalar_t hi = static_cast< scalar_t >( std::numeric_limits< int64_t >::max() );
+					const int64_t i = v != v ? 0 : v <= lo ? std::numeric_limits< int64_t >::min() :
+						v >= hi ? std::numeric_limits< int64_t >::max() : static_cast< int64_t >( v );
+					std::memcpy( &b, &i, 8 );
+				} else {
+					const scalar_t hi = static_cast< scalar_t >( std::numeric_limits< uint64_t >::max() );
+					// a negative scalar wraps, as its conversion to an unsigned type does
+					b = v != v ? 0 : v >= hi ? std::numeric_limits< uint64_t >::max() :
+						v < 0 ? static_cast< uint64_t >( static_cast< int64_t >( v ) ) :
+						static_cast< uint64_t >( v );
+				}
+				return b;
+			}
+
+			/** A value of domain `dom` (its bits) as T, converted the way C++
+			 *  converts from the domain's type (integers wrap). */
+			template< typename T >
+			T from_domain_bits( const uint64_t b, const int dom ) {
+				if( dom == ALPB_FP64 ) {
+					double d;
+					std::memcpy( &d, &b, 8 );
+					return static_cast< T >( d );
+				}
+				if( dom == ALPB_INT64 ) { return static_cast< T >( static_cast< int64_t >( b ) ); }
+				return static_cast< T >( b );
+			}
+
 			/** Device allocation that reports OUTOFMEM through the C-ABI. */
 			template< typename T >
 			T * alloc( const size_t n ) {

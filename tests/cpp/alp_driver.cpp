@@ -15,6 +15,10 @@
  *   op 4: BLAS1 script on u, v (dot, folds, eWiseApply, eWiseMul, eWiseMulAdd, set)
  *   op 5: matrix-to-matrix set and ALP's capacity contract (default capacity,
  *         too small a capacity, the RESIZE phase, an empty source)
+ *   op 6: integer BLAS1 on m entries with values from a seeded hash (size_t
+ *         values above 2^53, int values near the ends of their range): dot,
+ *         folds, eWiseApply, eWiseMul(Add) and set over size_t and int, printed
+ *         as hexadecimal so that both builds are compared bit for bit
  *   ring 0: plus-times double, 1: lor-land bool, 2: min-plus int
  */
 #include <cstdint>
@@ -263,6 +267,93 @@ static RC run_matrix_set( const Case &c ) {
 	return SUCCESS;
 }
 
+static uint64_t mix64( uint64_t z ) {   // splitmix64 finaliser
+	z += 0x9e3779b97f4a7c15ull;
+	z = ( z ^ ( z >> 30 ) ) * 0xbf58476d1ce4e5b9ull;
+	z = ( z ^ ( z >> 27 ) ) * 0x94d049bb133111ebull;
+	return z ^ ( z >> 31 );
+}
+
+template< typename T >
+static void print_hex( const char *tag, const T v ) {
+	std::printf( "%s 0x%016llx\n", tag, static_cast< unsigned long long >(
+		static_cast< uint64_t >( v ) ) );
+}
+
+template< typename T >
+static void print_hex_vector( const char *tag, const Vector< T > &x ) {
+	std::vector< std::pair< size_t, T > > e;
+	for( const auto &p : x ) { e.push_back( p ); }
+	std::sort( e.begin(), e.end() );
+	std::printf( "%s_nnz %zu\n", tag, e.size() );
+	for( const auto &p : e ) {
+		std::printf( "%s_%zu 0x%016llx\n", tag, p.first, static_cast< unsigned long long >(
+			static_cast< uint64_t >( p.second ) ) );
+	}
+}
+
+static RC run_integer_blas1( const Case &c ) {
+	const size_t n = static_cast< size_t >( c.m );
+	Vector< size_t > u( n ), v( n ), z( n );
+	Vector< int > a( n ), b( n ), w( n );
+	RC rc = SUCCESS;
+	for( size_t i = 0; rc == SUCCESS && i < n; ++i ) {
+		// size_t values well above 2^53; ints within 1000 of INT_MAX / INT_MIN
+		rc = setElement( u, mix64( 3 * i + 1 ) | ( size_t( 1 ) << 60 ), i );
+		rc = rc ? rc : setElement( v, mix64( 3 * i + 2 ), i );
+		const int64_t r = static_cast< int64_t >( mix64( 3 * i + 3 ) % 2000 );
+		rc = rc ? rc : setElement( a, static_cast< int >( i % 2 ? 2147483647 - r : -2147483647 + r ), i );
+		rc = rc ? rc : setElement( b, static_cast< int >( r - 1000 ), i );
+	}
+	std::printf( "rc_load %d\n", int( rc ) );
+	Semiring< operators::add< size_t >, operators::mul< size_t >, identities::zero,
+		identities::one > ringU;
+	Semiring< operators::add< int >, operators::mul< int >, identities::zero,
+		identities::one > ringI;
+	Semiring< operators::min< int >, operators::add< int >, identities::infinity,
+		identities::zero > minPlus;
+	Monoid< operators::add< size_t >, identities::zero > addU;
+	Monoid< operators::max< size_t >, identities::negative_infinity > maxU;
+	Monoid< operators::min< size_t >, identities::infinity > minU;
+	Monoid< operators::add< int >, identities::zero > addI;
+	size_t du = 7;
+	std::printf( "rc_dot_u64 %d\n", int( dot( du, u, v, ringU ) ) );
+	print_hex( "dot_u64", du );
+	size_t su = 0, mu = 0, nu = 0;
+	std::printf( "rc_fold_u64 %d\n", int( foldl( su, u, addU ) ) );
+	print_hex( "fold_add_u64", su );
+	std::printf( "rc_fold_max_u64 %d\n", int( foldl( mu, v, maxU ) ) );
+	print_hex( "fold_max_u64", mu );
+	nu = ~size_t( 0 );
+	std::printf( "rc_fold_min_u64 %d\n", int( foldl( nu, v, minU ) ) );
+	print_hex( "fold_min_u64", nu );
+	int di = 0, si = 0;
+	std::printf( "rc_dot_i32 %d\n", int( dot( di, a, b, ringI ) ) );
+	print_hex( "dot_i32", di );
+	std::printf( "rc_fold_i32 %d\n", int( foldl( si, a, addI ) ) );
+	print_hex( "fold_add_i32", si );
+	rc = eWiseApply( z, u, v, operators::add< size_t >() );
+	std::printf( "rc_apply_u64 %d\n", int( rc ) );
+	print_hex_vector( "apply_u64", z );
+	rc = set( z, u ) ? FAILED : foldl( z, v, operators::mul< size_t >() );
+	std::printf( "rc_foldl_u64 %d\n", int( rc ) );
+	print_hex_vector( "foldl_u64", z );
+	rc = set( z, ~size_t( 0 ) - 5 );
+	std::printf( "rc_set_u64 %d\n", int( rc ) );
+	print_hex_vector( "set_u64", z );
+	rc = set( z, u ) ? FAILED : eWiseMul( z, v, u, ringU );
+	std::printf( "rc_mul_u64 %d\n", int( rc ) );
+	print_hex_vector( "mul_u64", z );
+	rc = eWiseApply( w, a, b, operators::add< int >() );
+	std::printf( "rc_apply_i32 %d\n", int( rc ) );
+	print_hex_vector( "apply_i32", w );
+	Vector< int > c3( n );
+	rc = set( w, a ) ? FAILED : ( set( c3, b ) ? FAILED : eWiseMulAdd( w, a, b, c3, minPlus ) );
+	std::printf( "rc_minplus_i32 %d\n", int( rc ) );
+	print_hex_vector( "minplus_i32", w );
+	return SUCCESS;
+}
+
 int main( int argc, char **argv ) {
 	if( argc != 2 ) {
 		std::cerr << "usage: " << argv[ 0 ] << " <case file>\n";
@@ -292,6 +383,8 @@ int main( int argc, char **argv ) {
 		rc = run_pagerank( c );
 	} else if( c.op == 5 ) {
 		rc = run_matrix_set( c );
+	} else if( c.op == 6 ) {
+		rc = run_integer_blas1( c );
 	} else {
 		rc = run_blas1( c );
 	}

@@ -268,6 +268,20 @@ def _hpcg_result(out: str):
     return int(it.group(1)), float(it.group(2)), float(norm.group(1))
 
 
+@pytest.mark.parametrize("n", [50, 5000])
+def test_driver_integer_blas1_bit_exact(cuda, n):
+    """Integer level-1 primitives against the reference build, bit for bit:
+    size_t values above 2^53 (dot over the (+, *) ring, folds under add, max
+    and min, eWiseApply, foldl, eWiseMul, set of a value near 2^64) and int
+    values near the ends of their range, whose sums and products overflow and
+    must wrap as the reference's 32-bit arithmetic does (dot, fold,
+    eWiseApply, eWiseMulAdd over the min-plus ring)."""
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "case.bin"
+        write_case(f, 6, 0, 0, n, 0, [], [], [])
+        compare(f, 0.0)
+
+
 def test_driver_solvers_take_the_fused_path(cuda, oracle):
     """ALP's conjugate_gradient and simple_pagerank, called unchanged on b200
     containers, run the fused device solvers (one launch per solve), as the

@@ -345,3 +345,98 @@ def test_elementwise(cuda):
     torch.testing.assert_close(z, a + 0.25 * b - b, rtol=1e-15, atol=0)
     abi.call("alpb_set_scalar", dev.ptr(z), FP64, n, 7.0, None, None, dev.stream_ptr())
     assert bool((z == 7.0).all())
+
+
+@pytest.mark.parametrize("case", ["rmat18", "stencil64"])
+def test_autotuner_picks_a_schedule_and_keeps_parity(cuda, oracle, case):
+    """The schedule rule and the autotuner (alpb_spmv_autotune).  The rule
+    (ALPB_SCHED_AUTO without timing): skewed rows (R-MAT scale 18) take the
+    merge path; regular rows (27-point 64^3) take the vector schedule with
+    about mean/6 lanes per row (4 for 27 nonzeroes).  The autotuner then times
+    the candidates on the device: on R-MAT the vector schedules are several
+    times slower, so it must keep the merge path; on the stencil either may
+    win.  Whatever it keeps, the product through the tuned plan matches the
+    restatement (1e-12 relative) on two calls in a row."""
+    import torch
+    from alp_b200 import _abi as abi
+    dev = _dev()
+    if case == "rmat18":
+        A = dev.rmat(18, vtype=FP64, seed=61)
+    else:
+        A = dev.stencil((64, 64, 64), 26.0, -1.0)
+    x = dev.gen_values(A.n, FP64, seed=62)
+    u0 = dev.gen_values(A.m, FP64, seed=63)
+    plan = dev.Plan(A, sched=abi.SCHED_AUTO)
+    sched, vw, _ = plan.info()
+    if case == "rmat18":
+        assert sched == abi.SCHED_MERGE_PATH
+    else:
+        assert sched == abi.SCHED_VECTOR and vw == 4, (sched, vw)
+    scratch = torch.empty_like(u0)
+    plan.autotune(0, x, scratch)
+    sched2, vw2, _ = plan.info()
+    if case == "rmat18":
+        assert sched2 == abi.SCHED_MERGE_PATH
+    else:
+        assert sched2 in (abi.SCHED_MERGE_PATH, abi.SCHED_VECTOR)
+    o, i, v = A.to_host()
+    want = _np(u0).copy()
+    rc, _ = oracle.mxv(0, 0, 2, A.m, A.n, o, i, v, FP64, want, v=_np(x))
+    assert rc == 0
+    for _ in range(2):
+        u = u0.clone()
+        dev.mxv(0, A, u, x, plan=plan)
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(_np(u), want, rtol=1e-12, atol=1e-300)
+
+
+def test_vec_engine_integer_domains(cuda):
+    """alpb_vec_op_dom / alpb_vec_reduce_dom in the integer domains: int32
+    products and sums wrap as 32-bit arithmetic, uint64 values above 2^53 keep
+    every bit (numpy's wrapping arithmetic is the checker), and the folded
+    result includes the scalar it starts from."""
+    import ctypes as C
+    import torch
+    from alp_b200 import _abi as abi
+    dev = _dev()
+    rng = np.random.default_rng(17)
+    n = 100_003
+    a = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)
+    b = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)
+    u = rng.integers(0, 2**63, n, dtype=np.int64).astype(np.uint64) * np.uint64(2) + np.uint64(1)
+    v = rng.integers(0, 2**63, n, dtype=np.int64).astype(np.uint64)
+    ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    tu, tv = torch.from_numpy(u.view(np.int64)).cuda(), torch.from_numpy(v.view(np.int64)).cuda()
+    INT32, INT64, UINT64 = abi.INT32, 5, 8
+    ADD, MUL, MAX = 0, 2, 5
+    # z = a * b in int32 (wraps), computed in the signed 64-bit domain
+    z = torch.empty_like(ta)
+    abi.call("alpb_vec_op_dom", 3, MUL, 0, 0, 0, 0, INT64, n, dev.ptr(z), INT32, None, None,
+             None, None, 0, 0, dev.ptr(ta), INT32, None, 0, dev.ptr(tb), INT32, None, 0,
+             dev.stream_ptr())
+    with np.errstate(over="ignore"):
+        np.testing.assert_array_equal(z.cpu().numpy(), a * b)
+    # dot over int32 with 32-bit wrap: fold into 5 in int64, truncate
+    r = C.c_uint64(5)
+    abi.call("alpb_vec_reduce_dom", C.byref(r), ADD, 0, MUL, 0, INT64, n, dev.ptr(ta), INT32, None,
+             dev.ptr(tb), INT32, None, None, None, 0, 0, dev.stream_ptr())
+    want = (5 + (a.astype(np.int64) * b.astype(np.int64)).sum()) & 0xffffffff
+    assert (r.value & 0xffffffff) == int(want)
+    # uint64: z = u + v (wraps mod 2^64), dot and max fold, every bit kept
+    z64 = torch.empty_like(tu)
+    abi.call("alpb_vec_op_dom", 3, ADD, 0, 0, 0, 0, UINT64, n, dev.ptr(z64), INT64, None, None,
+             None, None, 0, 0, dev.ptr(tu), INT64, None, 0, dev.ptr(tv), INT64, None, 0,
+             dev.stream_ptr())
+    with np.errstate(over="ignore"):
+        np.testing.assert_array_equal(z64.cpu().numpy().view(np.uint64), u + v)
+    r = C.c_uint64(3)
+    abi.call("alpb_vec_reduce_dom", C.byref(r), ADD, 0, MUL, 0, UINT64, n, dev.ptr(tu), INT64,
+             None, dev.ptr(tv), INT64, None, None, None, 0, 0, dev.stream_ptr())
+    want = 3
+    for x, y in zip(u.tolist(), v.tolist()):
+        want = (want + x * y) & (2**64 - 1)
+    assert r.value == want
+    r = C.c_uint64(0)
+    abi.call("alpb_vec_reduce_dom", C.byref(r), MAX, 0, MUL, 0, UINT64, n, dev.ptr(tu), INT64,
+             None, None, INT64, None, None, None, 0, 0, dev.stream_ptr())
+    assert r.value == int(u.max())
