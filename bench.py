@@ -329,6 +329,7 @@ def extra_workloads(args, A, plan, cpu: bool) -> dict:
     from alp_b200 import device as dev
     stream = torch.cuda.current_stream()
     out = {}
+    later = []     # host reference runs, after the device timings
     # boolean lor/land, value mask with 50% true, dense: the reference reads a
     # non-inverted mask on its CRS gather by structure, so every row runs
     Ab = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices, None, abi.VOID)
@@ -352,7 +353,35 @@ def extra_workloads(args, A, plan, cpu: bool) -> dict:
     nb = algorithmic_bytes(A.m, A.n, A.nnz, 4, 4)
     out["mxv_min_plus_i32"] = {"ms": round(ms, 4), "GB/s": round(nb / ms / 1e6, 1), "bytes": nb}
     del Ai, xi, ui
-    # simple_pagerank, unit weights (column-stochastic after the out-degree scaling)
+    out["pagerank_rmat22"] = pagerank_workload(stream, A, cpu, later)
+    out["cg_27pt_32"] = cg_workload(stream, 32, cpu, later)
+    out["batched_cg"] = batched_cg_workload(stream, cpu=cpu, later=later)
+    out["hpcg_256"] = hpcg_workload(stream, cpu=cpu, later=later)
+    out["adjoint_cg"] = adjoint_workload(stream)
+    out["ppr_rmat24"] = ppr_workload(stream)
+    # the host's reference runs come after every device timing: reference_omp's
+    # threads keep spinning for a while after a parallel region and would
+    # delay the launching thread of a device solve timed next
+    for job in later:
+        job()
+    # each rate next to its fraction of the measured HBM copy bandwidth
+    peak = measured_peaks()["hbm_gbs"]
+    for v in out.values():
+        for k in [k for k in v if k.endswith("GB/s") and isinstance(v[k], (int, float))]:
+            v[k.replace("GB/s", "frac_of_measured_hbm")] = round(v[k] / peak, 4)
+    return out
+
+
+def pagerank_workload(stream, A, cpu: bool = False, later: list | None = None) -> dict:
+    """simple_pagerank on the pattern of A with unit weights (column-stochastic
+    after the out-degree scaling), alpha 0.85, conv 1e-9: one alpb_pagerank
+    call with its set-up, and the solve alone (alpb_pagerank_planned with the
+    CCS plan and scratch made beforehand)."""
+    import ctypes as C
+    import torch
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+    out = {}
     L = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices,
                 torch.ones(A.nnz, dtype=torch.float64, device="cuda"), abi.FP64)
     LT = dev.transpose(L)
@@ -379,18 +408,33 @@ def extra_workloads(args, A, plan, cpu: bool) -> dict:
             C.byref(it), C.byref(res), dev.ptr(pwork), pplan.h, dev.stream_ptr())
     ms = timed(pagerank_planned, 3, stream)
     per_iter = (A.nnz * 12 + (A.n + 1) * 8 + 6 * A.n * 8)
-    out["pagerank_rmat22"] = {"rc": prc[0], "iterations": it.value, "residual": res.value,
-                              "ms_per_solve": round(ms, 3),
-                              "ms_per_iter": round(ms / max(it.value, 1), 4),
-                              "ms_per_call_with_setup": round(ms_call, 3),
-                              "GB/s": round(per_iter * it.value / ms / 1e6, 1),
-                              "bytes_per_iteration": per_iter}
+    out.update({"rc": prc[0], "iterations": it.value, "residual": res.value,
+                "ms_per_solve": round(ms, 3), "ms_per_iter": round(ms / max(it.value, 1), 4),
+                "ms_per_call_with_setup": round(ms_call, 3),
+                "GB/s": round(per_iter * it.value / ms / 1e6, 1),
+                "bytes_per_iteration": per_iter})
     if cpu:
-        out["pagerank_rmat22"]["cpu_reference_omp"] = cpu_pagerank(L, ms)
-    del pplan, pwork
-    del L, LT, pr
-    # plain CG, 27-point 32^3 (the reference's CPU-runnable configuration)
-    S = dev.stencil((32, 32, 32), 26.0, -1.0)
+        job = (lambda n=L.m, h=L.to_host(), t=ms:
+               out.__setitem__("cpu_reference_omp", cpu_pagerank(n, h, t)))
+        if later is not None:
+            later.append(job)
+        else:
+            job()
+    del pplan, pwork, L, LT, pr
+    return out
+
+
+def cg_workload(stream, side: int = 32, cpu: bool = False, later: list | None = None) -> dict:
+    """Plain CG on the 27-point side^3 grid (diagonal 26, off-diagonals -1),
+    b = A 1, x0 = 0, tol 1e-10, max 500: the reference's CPU-runnable
+    configuration at 32^3, one fused alpb_cg_solve launch per solve."""
+    import ctypes as C
+    import torch
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+    out = {}
+    it, res = C.c_int64(), C.c_double()
+    S = dev.stencil((side, side, side), 26.0, -1.0)
     ones = torch.ones(S.n, dtype=torch.float64, device="cuda")
     b = torch.zeros_like(ones)
     dev.mxv(abi.RING_PLUS_TIMES_F64, S, b, ones)
@@ -404,26 +448,22 @@ def extra_workloads(args, A, plan, cpu: bool) -> dict:
                  dev.ptr(b), dev.ptr(x), 500, 1e-10, C.byref(it), C.byref(res), dev.ptr(work),
                  ps.h, dev.stream_ptr())
     ms = timed(cg, 5, stream)
-    out["cg_27pt_32"] = {"iterations": it.value, "residual": res.value,
-                         "ms_per_solve": round(ms, 4),
-                         "us_per_iteration": round(1e3 * ms / max(it.value, 1), 2),
-                         "err_vs_ones_inf": float((x - 1).abs().max().item())}
+    out.update({"iterations": it.value, "residual": res.value, "ms_per_solve": round(ms, 4),
+                "us_per_iteration": round(1e3 * ms / max(it.value, 1), 2),
+                "err_vs_ones_inf": float((x - 1).abs().max().item())})
     if cpu:
-        out["cg_27pt_32"]["cpu_reference_omp"] = cpu_cg(S, b, ms)
+        job = (lambda n=S.m, h=S.to_host(), hb=b.cpu().numpy(), t=ms:
+               out.__setitem__("cpu_reference_omp", cpu_cg(n, h, hb, t)))
+        if later is not None:
+            later.append(job)
+        else:
+            job()
     del S, ps, work
-    out["batched_cg"] = batched_cg_workload(stream, cpu=cpu)
-    out["hpcg_256"] = hpcg_workload(stream, cpu=cpu)
-    out["adjoint_cg"] = adjoint_workload(stream)
-    out["ppr_rmat24"] = ppr_workload(stream)
-    # each rate next to its fraction of the measured HBM copy bandwidth
-    peak = measured_peaks()["hbm_gbs"]
-    for v in out.values():
-        for k in [k for k in v if k.endswith("GB/s") and isinstance(v[k], (int, float))]:
-            v[k.replace("GB/s", "frac_of_measured_hbm")] = round(v[k] / peak, 4)
     return out
 
 
-def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024, cpu: bool = False) -> dict:
+def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024, cpu: bool = False,
+                        later: list | None = None) -> dict:
     """256 shifted 2-D 5-point Poisson systems, sides log-uniform in [32, 512],
     shift U(0.01, 1), b ~ N(0, 1), relative tolerance 1e-8, FP64: one
     graph-captured persistent launch against one alpb_cg_solve launch per
@@ -500,17 +540,28 @@ def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024, cpu: bool = F
     # temp and writes x, r)
     per_iter = 12 * nnzs + 8 * (rows + 1) + 80 * rows
     moved = float((it * per_iter).sum())
-    cpu_res = None
+    out = {"systems": nseg, "rows": n, "nnz": nnz, "tol": tol, "rc": rc,
+           "all_converged": bool(conv.all()), "iterations_max": int(it.max()),
+           "iterations_sum": int(it.sum()), "plain_iterations_sum": int(itp.sum()),
+           "batched_ms": round(ms_b, 3), "plain_ms": round(ms_p, 3),
+           "batched_solves_per_s": round(nseg / (ms_b * 1e-3), 1),
+           "plain_solves_per_s": round(nseg / (ms_p * 1e-3), 1),
+           "speedup": round(ms_p / ms_b, 2),
+           "batched_GB/s": round(moved / ms_b / 1e6, 1),
+           "plain_GB/s": round(moved / ms_p / 1e6, 1),
+           "max_rel_diff_batched_vs_plain": diff}
     if cpu:
-        # reference_omp solving the 256 systems one after the other (the same
-        # matrices and right-hand sides, copied from the device)
-        from oracle.oracle import crs_to_coo
-        ref = reference_omp()
-        if ref is None:
-            cpu_res = _cpu_unavailable()
-        else:
-            hrp, hci, hva = rp.cpu().numpy(), ci.cpu().numpy().view(np.uint32), va.cpu().numpy()
-            hb = b.cpu().numpy()
+        hrp, hci, hva = rp.cpu().numpy(), ci.cpu().numpy().view(np.uint32), va.cpu().numpy()
+        hb = b.cpu().numpy()
+
+        def cpu_batched():
+            # reference_omp solving the 256 systems one after the other (the
+            # same matrices and right-hand sides, copied from the device)
+            from oracle.oracle import crs_to_coo
+            ref = reference_omp()
+            if ref is None:
+                out["cpu_reference_omp"] = _cpu_unavailable()
+                return
             tot, its = 0.0, 0
             for k in range(nseg):
                 r0, r1 = int(seg_rows[k]), int(seg_rows[k + 1])
@@ -521,22 +572,17 @@ def batched_cg_workload(stream, nseg: int = 256, seed: int = 2024, cpu: bool = F
                                               np.zeros(r1 - r0), max_iter, tol)
                 tot += ms_k
                 its += itk
-            cpu_res = {"ms": round(tot, 1), "iterations_sum": its, "threads": ref.threads(),
-                       "solves_per_s": round(nseg / (tot * 1e-3), 1),
-                       "gpu_batched_speedup": round(tot / ms_b, 1),
-                       "sample": "the whole workload: conjugate_gradient on each of the 256 "
-                                 "systems in turn, solves alone timed"}
-    return {"systems": nseg, "rows": n, "nnz": nnz, "tol": tol, "rc": rc,
-            "all_converged": bool(conv.all()), "iterations_max": int(it.max()),
-            "iterations_sum": int(it.sum()), "plain_iterations_sum": int(itp.sum()),
-            "batched_ms": round(ms_b, 3), "plain_ms": round(ms_p, 3),
-            "batched_solves_per_s": round(nseg / (ms_b * 1e-3), 1),
-            "plain_solves_per_s": round(nseg / (ms_p * 1e-3), 1),
-            "speedup": round(ms_p / ms_b, 2),
-            "batched_GB/s": round(moved / ms_b / 1e6, 1),
-            "plain_GB/s": round(moved / ms_p / 1e6, 1),
-            "max_rel_diff_batched_vs_plain": diff,
-            **({"cpu_reference_omp": cpu_res} if cpu_res else {})}
+            out["cpu_reference_omp"] = {
+                "ms": round(tot, 1), "iterations_sum": its, "threads": ref.threads(),
+                "solves_per_s": round(nseg / (tot * 1e-3), 1),
+                "gpu_batched_speedup": round(tot / ms_b, 1),
+                "sample": "the whole workload: conjugate_gradient on each of the 256 "
+                          "systems in turn, solves alone timed"}
+        if later is not None:
+            later.append(cpu_batched)
+        else:
+            cpu_batched()
+    return out
 
 
 def _hpcg_gpu(stream, side, coarse_levels, nrhs, seed):
@@ -567,7 +613,7 @@ def _hpcg_gpu(stream, side, coarse_levels, nrhs, seed):
 
 
 def hpcg_workload(stream, side: int = 256, coarse_levels: int = 3, nrhs: int = 8,
-                  cpu: bool = False) -> dict:
+                  cpu: bool = False, later: list | None = None) -> dict:
     """HPCG on the 27-point 256^3 system (diagonal 26, off-diagonals -1) with
     three coarser levels (128^3, 64^3, 32^3), 27 static colours, one pre- and
     one post-smoothing step, 8 right-hand sides ~ N(0, 1) solved together,
@@ -599,11 +645,13 @@ def hpcg_workload(stream, side: int = 256, coarse_levels: int = 3, nrhs: int = 8
            "bytes_per_iteration": int(per_iter),
            "gathered_GB/s": round(gathered * iters / ms / 1e6, 1)}
     if cpu:
-        ref = reference_omp()
-        if ref is None:
-            out["cpu_reference_omp"] = _cpu_unavailable()
-        else:
-            ms64, it64, _, _, _, _, _ = _hpcg_gpu(stream, 64, 3, 8, 32)
+        ms64, it64, _, _, _, _, _ = _hpcg_gpu(stream, 64, 3, 8, 32)
+
+        def cpu_hpcg():
+            ref = reference_omp()
+            if ref is None:
+                out["cpu_reference_omp"] = _cpu_unavailable()
+                return
             b = np.random.default_rng(64).standard_normal(64 ** 3)
             rc, _, itc, _, msc, _ = ref.hpcg(64, 3, 27, b, 500, 1e-9)
             out["cpu_reference_omp"] = {
@@ -613,6 +661,10 @@ def hpcg_workload(stream, side: int = 256, coarse_levels: int = 3, nrhs: int = 8
                 "gpu_speedup_64": round(msc / (ms64 / 8), 1),
                 "sample": "grb::algorithms::hpcg on 64^3 with 3 coarser levels, one right-hand "
                           "side (the device at 64^3 solves 8 together; ms per right-hand side)"}
+        if later is not None:
+            later.append(cpu_hpcg)
+        else:
+            cpu_hpcg()
     return out
 
 
@@ -782,34 +834,33 @@ def _cpu_unavailable():
     return {"ms": None, "sample": "unavailable: oracle/_ref/libalp_ref_omp.so not built"}
 
 
-def cpu_pagerank(L, gpu_ms) -> dict:
+def cpu_pagerank(n, host_crs, gpu_ms) -> dict:
     """grb::algorithms::simple_pagerank on reference_omp, same graph and
     parameters (alpha 0.85, conv 1e-9); the solve alone is timed."""
     from oracle.oracle import crs_to_coo
     ref = reference_omp()
     if ref is None:
         return _cpu_unavailable()
-    o, i, v = L.to_host()
+    o, i, v = host_crs
     I, J = crs_to_coo(o, i)
-    rc, pr, it, ms = ref.pagerank(L.m, I, J, v, alpha=0.85, conv=1e-9, max_iter=1000)
+    rc, pr, it, ms = ref.pagerank(n, I, J, v, alpha=0.85, conv=1e-9, max_iter=1000)
     return {"rc": rc, "iterations": it, "ms": round(ms, 1), "threads": ref.threads(),
             "gpu_speedup": round(ms / gpu_ms, 1),
             "sample": "the whole workload: simple_pagerank on the same scale-22 graph, one solve"}
 
 
-def cpu_cg(S, b, gpu_ms) -> dict:
+def cpu_cg(n, host_crs, hb, gpu_ms) -> dict:
     """grb::algorithms::conjugate_gradient on reference_omp, same system and
     parameters (x0 = 0, tol 1e-10, max 500); mean of 5 solves."""
     from oracle.oracle import crs_to_coo
     ref = reference_omp()
     if ref is None:
         return _cpu_unavailable()
-    o, i, v = S.to_host()
+    o, i, v = host_crs
     I, J = crs_to_coo(o, i)
-    hb = b.cpu().numpy()
     tot, it = 0.0, 0
     for _ in range(5):
-        rc, _, it, _, ms = ref.cg(S.m, I, J, v, hb, np.zeros(S.m), 500, 1e-10)
+        rc, _, it, _, ms = ref.cg(n, I, J, v, hb, np.zeros(n), 500, 1e-10)
         tot += ms
     return {"rc": rc, "iterations": it, "ms": round(tot / 5, 3), "threads": ref.threads(),
             "gpu_speedup": round(tot / 5 / gpu_ms, 1),
@@ -850,12 +901,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale (22 is the benchmark; smaller for profiling captures)")
-    ap.add_argument("--only", choices=["batched_cg", "hpcg", "adjoint_cg", "ppr"],
+    ap.add_argument("--only", choices=["batched_cg", "hpcg", "adjoint_cg", "ppr", "pagerank", "cg"],
                     help="run one secondary workload alone and print its line (profiling)")
     ap.add_argument("--hpcg-side", type=int, default=256)
     ap.add_argument("--hpcg-levels", type=int, default=3)
     ap.add_argument("--ppr-scale", type=int, default=24)
     ap.add_argument("--ppr-seeds", type=int, default=64)
+    ap.add_argument("--cg-side", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -870,13 +922,17 @@ def main():
     if args.only:
         import torch
         from alp_b200 import _abi as abi
+        from alp_b200 import device as dev
         torch.cuda.set_device(local_rank)
         abi.call("alpb_init", local_rank)
         stream = torch.cuda.current_stream()
         run = {"batched_cg": lambda: batched_cg_workload(stream),
                "hpcg": lambda: hpcg_workload(stream, args.hpcg_side, args.hpcg_levels),
                "adjoint_cg": lambda: adjoint_workload(stream),
-               "ppr": lambda: ppr_workload(stream, args.ppr_scale, args.ppr_seeds)}[args.only]
+               "ppr": lambda: ppr_workload(stream, args.ppr_scale, args.ppr_seeds),
+               "pagerank": lambda: pagerank_workload(
+                   stream, dev.rmat(args.scale, EDGE_FACTOR, seed=SEED, vtype=abi.FP64)),
+               "cg": lambda: cg_workload(stream, args.cg_side)}[args.only]
         if rank == 0:
             print(json.dumps({"workload": args.only, **run()}), flush=True)
         return
