@@ -77,6 +77,8 @@ PROTOS: dict[str, list] = {
     "alpb_gen_sym_dd_values": [P, P, I64, U64, D, D, D, P, P],
     "alpb_spmv_plan_create": [C.POINTER(P), I64, I64, P, I32, I32, P],
     "alpb_spmv_plan_destroy": [P],
+    "alpb_spmv_plan_hot": [P, I32, I64, P, I64, P],
+    "alpb_spmv_plan_hot_info": [P, PI64, PD],
     "alpb_spmv_autotune": [P, I32, I64, P, P, I32, P, P, P],
     "alpb_spmv_plan_info": [P, PI, PI, PI64],
     "alpb_mxv": [I32, U32, I32, I64, I64, I64, P, P, P, I32,

@@ -17,10 +17,11 @@
 namespace alpb {
 
 // ------------------------------------------------------------ domains --
-// An ALP operator computes in its own domain: double, or a 64-bit integer
-// (int and size_t operators).  Integer domains compute in int64_t or
-// uint64_t with two's-complement wrap-around; storing into a narrower type
-// truncates, so int32 sums and products wrap exactly as 32-bit ones do.
+// An ALP operator computes in its own domain: double, or an integer type of
+// 32 or 64 bits (int, size_t, ... operators).  Integer domains compute with
+// two's-complement wrap-around at their own width, so an int operator's
+// overflowing sum wraps before a later min or comparison sees it, exactly as
+// the reference's int arithmetic does.
 template <class T>
 __device__ __forceinline__ T ld_as(const void *p, int type, int64_t i) {
 	switch (type) {
@@ -68,6 +69,29 @@ __device__ __forceinline__ void st_as<uint64_t>(void *p, int type, int64_t i, ui
 	}
 }
 
+// 32-bit integer domains: loaded through the 64-bit ones, narrowed with
+// wrap-around (a double converts directly, as C++ converts it)
+template <>
+__device__ __forceinline__ int32_t ld_as<int32_t>(const void *p, int type, int64_t i) {
+	if (type == ALPB_FP64) return int32_t(reinterpret_cast<const double *>(p)[i]);
+	return int32_t(uint32_t(uint64_t(ld_as<int64_t>(p, type, i))));
+}
+template <>
+__device__ __forceinline__ uint32_t ld_as<uint32_t>(const void *p, int type, int64_t i) {
+	if (type == ALPB_FP64) return uint32_t(reinterpret_cast<const double *>(p)[i]);
+	return uint32_t(ld_as<uint64_t>(p, type, i));
+}
+template <>
+__device__ __forceinline__ void st_as<int32_t>(void *p, int type, int64_t i, int32_t v) {
+	if (type == ALPB_FP64) reinterpret_cast<double *>(p)[i] = double(v);
+	else st_as<int64_t>(p, type, i, int64_t(v));   // sign-extends into 64-bit outputs
+}
+template <>
+__device__ __forceinline__ void st_as<uint32_t>(void *p, int type, int64_t i, uint32_t v) {
+	if (type == ALPB_FP64) reinterpret_cast<double *>(p)[i] = double(v);
+	else st_as<int64_t>(p, type, i, int64_t(v));   // zero-extends into 64-bit outputs
+}
+
 // wrapping + - * for the integer domains (no signed-overflow UB)
 template <class T> __device__ __forceinline__ T wrap_add(T a, T b) { return a + b; }
 template <class T> __device__ __forceinline__ T wrap_sub(T a, T b) { return a - b; }
@@ -80,6 +104,15 @@ template <> __device__ __forceinline__ int64_t wrap_sub(int64_t a, int64_t b) {
 }
 template <> __device__ __forceinline__ int64_t wrap_mul(int64_t a, int64_t b) {
 	return int64_t(uint64_t(a) * uint64_t(b));
+}
+template <> __device__ __forceinline__ int32_t wrap_add(int32_t a, int32_t b) {
+	return int32_t(uint32_t(a) + uint32_t(b));
+}
+template <> __device__ __forceinline__ int32_t wrap_sub(int32_t a, int32_t b) {
+	return int32_t(uint32_t(a) - uint32_t(b));
+}
+template <> __device__ __forceinline__ int32_t wrap_mul(int32_t a, int32_t b) {
+	return int32_t(uint32_t(a) * uint32_t(b));
 }
 
 template <class T>
@@ -363,8 +396,9 @@ int alpb_vec_reduce_dom(void *result, int add_op, uint64_t identity, int mul_op,
 	ALPB_CHECK(add_op >= ALPB_OP_ADD && add_op <= ALPB_OP_LAND && mul_op >= ALPB_OP_ADD &&
 		mul_op <= ALPB_OP_GEQ, ALPB_UNSUPPORTED, "alpb_vec_reduce: ops %d %d", add_op,
 		mul_op);
-	ALPB_CHECK(domain == ALPB_FP64 || domain == ALPB_INT64 || domain == ALPB_UINT64,
-		ALPB_UNSUPPORTED, "alpb_vec_reduce: domain %d", domain);
+	ALPB_CHECK(domain == ALPB_FP64 || domain == ALPB_INT64 || domain == ALPB_UINT64 ||
+		domain == ALPB_INT32 || domain == ALPB_UINT32, ALPB_UNSUPPORTED,
+		"alpb_vec_reduce: domain %d", domain);
 	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
 	cudaStream_t s = as_stream(stream);
 	switch (domain) {
@@ -373,6 +407,12 @@ int alpb_vec_reduce_dom(void *result, int add_op, uint64_t identity, int mul_op,
 			x_assigned, y, y_type, y_assigned, mask, mask_assigned, mask_type, masked, s);
 	case ALPB_INT64:
 		return vec_reduce_run<int64_t>(result, add_op, identity, mul_op, descr, n, x, x_type,
+			x_assigned, y, y_type, y_assigned, mask, mask_assigned, mask_type, masked, s);
+	case ALPB_INT32:
+		return vec_reduce_run<int32_t>(result, add_op, identity, mul_op, descr, n, x, x_type,
+			x_assigned, y, y_type, y_assigned, mask, mask_assigned, mask_type, masked, s);
+	case ALPB_UINT32:
+		return vec_reduce_run<uint32_t>(result, add_op, identity, mul_op, descr, n, x, x_type,
 			x_assigned, y, y_type, y_assigned, mask, mask_assigned, mask_type, masked, s);
 	default:
 		return vec_reduce_run<uint64_t>(result, add_op, identity, mul_op, descr, n, x, x_type,
@@ -400,11 +440,20 @@ int alpb_vec_op_dom(int kind, int op, int monoid, uint64_t identity, int mul_op,
 	ALPB_CHECK(type_size(z_type) > 0, ALPB_UNSUPPORTED, "alpb_vec_op: output type %d", z_type);
 	ALPB_CHECK(z_assigned == nullptr || z_nnz != nullptr, ALPB_ILLEGAL,
 		"alpb_vec_op: sparse output needs its nnz counter");
-	ALPB_CHECK(domain == ALPB_FP64 || domain == ALPB_INT64 || domain == ALPB_UINT64,
-		ALPB_UNSUPPORTED, "alpb_vec_op: domain %d", domain);
+	ALPB_CHECK(domain == ALPB_FP64 || domain == ALPB_INT64 || domain == ALPB_UINT64 ||
+		domain == ALPB_INT32 || domain == ALPB_UINT32, ALPB_UNSUPPORTED,
+		"alpb_vec_op: domain %d", domain);
 	if (n <= 0) return n == 0 ? ALPB_SUCCESS : ALPB_ILLEGAL;
 	cudaStream_t s = as_stream(stream);
 	switch (domain) {
+	case ALPB_INT32:
+		return vec_op_run<int32_t>(kind, op, monoid, identity, mul_op, descr, n, z, z_type,
+			z_assigned, z_nnz, mask, mask_assigned, mask_type, masked, x, x_type, x_assigned, alpha,
+			y, y_type, y_assigned, beta, s);
+	case ALPB_UINT32:
+		return vec_op_run<uint32_t>(kind, op, monoid, identity, mul_op, descr, n, z, z_type,
+			z_assigned, z_nnz, mask, mask_assigned, mask_type, masked, x, x_type, x_assigned, alpha,
+			y, y_type, y_assigned, beta, s);
 	case ALPB_FP64:
 		return vec_op_run<double>(kind, op, monoid, identity, mul_op, descr, n, z, z_type,
 			z_assigned, z_nnz, mask, mask_assigned, mask_type, masked, x, x_type, x_assigned, alpha,

@@ -20,6 +20,7 @@
 #include "wmerge.cuh"
 
 #include <algorithm>
+#include <vector>
 
 namespace alpb {
 
@@ -236,6 +237,88 @@ k_spmv_wmerge(MergeTables mt, const int64_t *__restrict__ offsets,
 	}
 }
 
+// ------------------------------------------------- hot-column cache path --
+// The same warp tiles as k_spmv_wmerge, on a plan whose hot_idx marks the
+// nonzeroes of its hot columns: one block per SM copies the hot columns'
+// x values (gathered once per product into hot_x) into shared memory, and
+// the staging loop reads a marked column from there instead of from global
+// memory.  Products and sums are those of k_spmv_wmerge, bit for bit.
+constexpr uint32_t kHotBit = 0x80000000u;
+#ifndef ALPB_HOT_WARPS
+#define ALPB_HOT_WARPS 16
+#endif
+constexpr int HOT_WARPS = ALPB_HOT_WARPS;   // one block of these per SM
+
+template <class T>
+struct HotX {
+	const T *xs;
+	const T *__restrict__ x;
+	__device__ __forceinline__ T operator()(uint32_t c) const {
+		return (c & kHotBit) ? xs[c ^ kHotBit] : __ldg(x + c);
+	}
+};
+
+template <class R>
+struct HotSmem {
+	static constexpr size_t warp_bytes = (sizeof(WarpSmem<R>) + 15) / 16 * 16;
+	static constexpr size_t y_off = warp_bytes * HOT_WARPS;
+	static constexpr size_t x_off = y_off + size_t(HOT_WARPS) * WM_TILE * sizeof(typename R::T);
+	static size_t bytes(int64_t hot_k) { return x_off + size_t(hot_k) * sizeof(typename R::T); }
+};
+
+__global__ void k_col_counts(const uint32_t *__restrict__ idx, int64_t nnz, uint32_t *cnt) {
+	for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < nnz;
+		 k += int64_t(gridDim.x) * blockDim.x)
+		atomicAdd(cnt + idx[k], 1u);
+}
+
+__global__ void k_hot_remap(const uint32_t *__restrict__ idx, int64_t nnz,
+	const int32_t *__restrict__ slot, uint32_t *out) {
+	for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < nnz;
+		 k += int64_t(gridDim.x) * blockDim.x) {
+		const uint32_t c = idx[k];
+		const int32_t sl = slot[c];
+		out[k] = sl >= 0 ? (kHotBit | uint32_t(sl)) : c;
+	}
+}
+
+template <class T>
+__global__ void k_hot_gather(const uint32_t *__restrict__ cols, const T *__restrict__ x,
+	T *__restrict__ hx, int64_t k) {
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < k;
+		 i += int64_t(gridDim.x) * blockDim.x)
+		hx[i] = x[cols[i]];
+}
+
+template <class R>
+__global__ void __launch_bounds__(32 * HOT_WARPS, 1)
+k_spmv_wmerge_hot(MergeTables mt, const int64_t *__restrict__ offsets,
+	const uint32_t *__restrict__ hot_idx, const typename R::T *__restrict__ values,
+	const typename R::T *__restrict__ x, const typename R::T *__restrict__ hx, int64_t hot_k,
+	typename R::T *__restrict__ y, int left) {
+	using T = typename R::T;
+	extern __shared__ __align__(16) unsigned char hot_smem[];
+	WarpSmem<R> *sm = reinterpret_cast<WarpSmem<R> *>(hot_smem);
+	T *ybuf = reinterpret_cast<T *>(hot_smem + HotSmem<R>::y_off);
+	T *xs = reinterpret_cast<T *>(hot_smem + HotSmem<R>::x_off);
+	for (int64_t i = threadIdx.x; i < hot_k; i += blockDim.x) xs[i] = hx[i];
+	__syncthreads();
+	const int w = threadIdx.x >> 5;
+	HotX<T> xl{xs, x};
+	WarpAccumulateY<R> epi{y, ybuf + size_t(w) * WM_TILE};
+	WarpSmem<R> &mine = *reinterpret_cast<WarpSmem<R> *>(hot_smem + HotSmem<R>::warp_bytes * w);
+	(void) sm;
+	const int64_t nw = int64_t(gridDim.x) * HOT_WARPS;
+	int64_t t = int64_t(blockIdx.x) * HOT_WARPS + w;
+	WmMeta g = wm_meta(mt, t);
+	while (t < mt.ntiles) {
+		const WmMeta next = wm_meta(mt, t + nw);
+		warp_tile<R>(t, g, mt, offsets, hot_idx, values, xl, epi, left, mine);
+		t += nw;
+		g = next;
+	}
+}
+
 // ------------------------------------------------------ vector schedules --
 // Rows are handed out per warp (32/W rows at a time) so that every lane of a
 // warp runs the same number of outer iterations and the width-W shuffles
@@ -379,7 +462,28 @@ template <class R>
 int launch_merge(const SpmvArgs &a, const alpb_spmv_plan_s &p, cudaStream_t s) {
 	using T = typename R::T;
 	if (p.ntiles == 0) return ALPB_SUCCESS;
-	if (p.tile == WM_TILE) {
+	if (p.tile == WM_TILE && p.hot_on && p.hot_k > 0 && a.indices == p.hot_src) {
+		const size_t smem = HotSmem<R>::bytes(p.hot_k);
+		static size_t smem_set = 0;
+		if (smem > smem_set) {
+			ALPB_CUDA(cudaFuncSetAttribute(k_spmv_wmerge_hot<R>,
+				cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+			smem_set = smem;
+		}
+		T *hx = reinterpret_cast<T *>(p.hot_x);
+		k_hot_gather<T><<<grid_for(p.hot_k, 256), 256, 0, s>>>(p.hot_cols,
+			reinterpret_cast<const T *>(a.v), hx, p.hot_k);
+		ALPB_LAUNCHED();
+		int64_t grid = (p.ntiles + HOT_WARPS - 1) / HOT_WARPS;
+		if (grid > sm_count()) grid = sm_count();
+		const MergeTables mt = merge_tables(p);
+		k_spmv_wmerge_hot<R><<<unsigned(grid), 32 * HOT_WARPS, smem, s>>>(mt, a.offsets,
+			p.hot_idx, reinterpret_cast<const T *>(a.values), reinterpret_cast<const T *>(a.v), hx,
+			p.hot_k, reinterpret_cast<T *>(a.u), a.left);
+		ALPB_LAUNCHED();
+		k_wm_fixup<R><<<grid_for((p.ntiles + 31) / 32 * 32, 256), 256, 0, s>>>(mt,
+			AccumulateY<R>{reinterpret_cast<T *>(a.u)});
+	} else if (p.tile == WM_TILE) {
 		static int blocks_per_sm = 0;
 		if (!blocks_per_sm) {
 			ALPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
@@ -634,6 +738,9 @@ int alpb_spmv_plan_destroy(alpb_spmv_plan p) {
 	cudaFree(p->tail_has);
 	cudaFree(p->ready);
 	cudaFree(p->tile_d);
+	cudaFree(p->hot_idx);
+	cudaFree(p->hot_cols);
+	cudaFree(p->hot_x);
 	delete p;
 	return ALPB_SUCCESS;
 }
@@ -643,6 +750,126 @@ int alpb_spmv_plan_info(alpb_spmv_plan p, int *sched, int *vw, int64_t *tiles) {
 	if (sched) *sched = p->sched;
 	if (vw) *vw = p->vw;
 	if (tiles) *tiles = p->ntiles;
+	return ALPB_SUCCESS;
+}
+
+} // extern "C"
+
+namespace alpb {
+
+// Hot-column slots that fit the shared memory of one block (227 KB) next to
+// the warps' tiles, for the value type of `ring`.
+template <class R>
+static int64_t hot_slots_for() {
+	const size_t cap = 227 * 1024;
+	return HotSmem<R>::x_off >= cap ? 0
+		: int64_t((cap - HotSmem<R>::x_off) / sizeof(typename R::T)) / 1024 * 1024;
+}
+static int64_t hot_slots_max(int ring) {
+	switch (ring) {
+	case ALPB_RING_PLUS_TIMES_F64: return hot_slots_for<RingPlusTimesF64>();
+	case ALPB_RING_LOR_LAND_BOOL: return hot_slots_for<RingLorLandBool>();
+	case ALPB_RING_MIN_PLUS_I32: return hot_slots_for<RingMinPlusI32>();
+	case ALPB_RING_PLUS_PATTERN_F64: return hot_slots_for<RingPlusPatternF64>();
+	case ALPB_RING_PLUS_TIMES_I32: return hot_slots_for<RingPlusTimesI32>();
+	case ALPB_RING_PLUS_RIGHT_IF_U64: return hot_slots_for<RingPlusRightIfU64>();
+	case ALPB_RING_MAX_LEFT_IF_U64: return hot_slots_for<RingMaxLeftIfU64>();
+	case ALPB_RING_TIMES_PLUS_F64: return hot_slots_for<RingTimesPlusF64>();
+	}
+	return 0;
+}
+
+static void hot_release(alpb_spmv_plan_s *p) {
+	cudaFree(p->hot_idx);
+	cudaFree(p->hot_cols);
+	cudaFree(p->hot_x);
+	p->hot_idx = nullptr;
+	p->hot_cols = nullptr;
+	p->hot_x = nullptr;
+	p->hot_k = 0;
+	p->hot_on = 0;
+	p->hot_src = nullptr;
+	p->hot_cover = 0;
+}
+
+// Hot-column cache of K slots for the index array `indices` (n columns): the
+// K most frequent columns (ties to the smaller column) get the slots in order
+// of decreasing frequency.  Column counts are taken on the device; the
+// selection runs on the host (n counts) once per plan.
+static int hot_build(alpb_spmv_plan_s *p, const uint32_t *indices, int64_t n, int64_t K,
+	cudaStream_t s) {
+	hot_release(p);
+	if (K <= 0 || n <= K || n >= (int64_t(1) << 31) || p->nnz == 0) return ALPB_SUCCESS;
+	uint32_t *cnt = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&cnt, size_t(n) * 4, s));
+	ALPB_CUDA(cudaMemsetAsync(cnt, 0, size_t(n) * 4, s));
+	k_col_counts<<<grid_for(p->nnz, 256, 4), 256, 0, s>>>(indices, p->nnz, cnt);
+	ALPB_LAUNCHED();
+	std::vector<uint32_t> h(static_cast<size_t>(n));
+	ALPB_CUDA(cudaMemcpyAsync(h.data(), cnt, size_t(n) * 4, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaFreeAsync(cnt, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	std::vector<uint32_t> order(static_cast<size_t>(n));
+	for (int64_t j = 0; j < n; ++j) order[size_t(j)] = uint32_t(j);
+	const auto more = [&h](uint32_t a, uint32_t b) { return h[a] != h[b] ? h[a] > h[b] : a < b; };
+	std::partial_sort(order.begin(), order.begin() + K, order.end(), more);
+	std::vector<int32_t> slot(static_cast<size_t>(n), -1);
+	uint64_t covered = 0;
+	for (int64_t k = 0; k < K; ++k) {
+		slot[order[size_t(k)]] = int32_t(k);
+		covered += h[order[size_t(k)]];
+	}
+	int32_t *dslot = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&dslot, size_t(n) * 4, s));
+	ALPB_CUDA(cudaMemcpyAsync(dslot, slot.data(), size_t(n) * 4, cudaMemcpyHostToDevice, s));
+	if (cudaMalloc(&p->hot_idx, size_t(p->nnz) * 4) != cudaSuccess ||
+		cudaMalloc(&p->hot_cols, size_t(K) * 4) != cudaSuccess ||
+		cudaMalloc(&p->hot_x, size_t(K) * 8) != cudaSuccess) {
+		cudaGetLastError();
+		cudaFreeAsync(dslot, s);
+		cudaStreamSynchronize(s);
+		hot_release(p);
+		set_error("alpb_spmv_autotune: out of device memory for the hot-column cache");
+		return ALPB_OUTOFMEM;
+	}
+	ALPB_CUDA(cudaMemcpyAsync(p->hot_cols, order.data(), size_t(K) * 4, cudaMemcpyHostToDevice, s));
+	k_hot_remap<<<grid_for(p->nnz, 256, 4), 256, 0, s>>>(indices, p->nnz, dslot, p->hot_idx);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cudaFreeAsync(dslot, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	p->hot_k = K;
+	p->hot_src = indices;
+	p->hot_cover = double(covered) / double(p->nnz);
+	return ALPB_SUCCESS;
+}
+
+} // namespace alpb
+
+extern "C" {
+
+int alpb_spmv_plan_hot(alpb_spmv_plan p, int ring, int64_t n, const uint32_t *indices,
+	int64_t slots, void *stream) {
+	ALPB_CHECK(p != nullptr, ALPB_ILLEGAL, "alpb_spmv_plan_hot: null plan");
+	ALPB_CHECK(ring_value_type(ring) >= 0, ALPB_UNSUPPORTED,
+		"alpb_spmv_plan_hot: semiring %d is not instantiated on the device", ring);
+	ALPB_CHECK(slots >= 0 && slots <= hot_slots_max(ring), ALPB_ILLEGAL,
+		"alpb_spmv_plan_hot: %lld slots (at most %lld for semiring %d)", (long long) slots,
+		(long long) hot_slots_max(ring), ring);
+	ALPB_CHECK(slots == 0 || (indices != nullptr && n > 0), ALPB_ILLEGAL,
+		"alpb_spmv_plan_hot: null indices");
+	ALPB_CHECK(slots == 0 || p->tile == WM_TILE, ALPB_UNSUPPORTED,
+		"alpb_spmv_plan_hot: the plan has no warp tiles");
+	cudaStream_t s = as_stream(stream);
+	const int rc = hot_build(p, indices, n, slots, s);
+	if (rc != ALPB_SUCCESS) return rc;
+	p->hot_on = p->hot_k > 0 ? 1 : 0;
+	return ALPB_SUCCESS;
+}
+
+int alpb_spmv_plan_hot_info(alpb_spmv_plan p, int64_t *slots, double *cover) {
+	ALPB_CHECK(p != nullptr, ALPB_ILLEGAL, "alpb_spmv_plan_hot_info: null plan");
+	if (slots) *slots = p->hot_on ? p->hot_k : 0;
+	if (cover) *cover = p->hot_on ? p->hot_cover : 0.0;
 	return ALPB_SUCCESS;
 }
 
@@ -689,10 +916,49 @@ int alpb_spmv_autotune(alpb_spmv_plan p, int ring, int64_t n, const uint32_t *in
 		}
 		if (total < best) { best = total; best_i = c; }
 	}
-	ALPB_CUDA(cudaEventDestroy(e0));
-	ALPB_CUDA(cudaEventDestroy(e1));
 	p->sched = cands[best_i].sched;
 	p->vw = cands[best_i].sched == ALPB_SCHED_VECTOR ? cands[best_i].w : saved_vw;
+	// skewed rows on the merge path: try the hot-column cache at two sizes
+	// (its shared memory bounds the slots for the ring's type)
+	hot_release(p);
+	if (p->sched == ALPB_SCHED_MERGE_PATH && p->tile == WM_TILE && n >= (int64_t(1) << 16) &&
+		p->nnz >= (int64_t(1) << 20)) {
+		const int64_t slots_max = hot_slots_max(ring);
+		int64_t best_k = 0;
+		for (const int64_t K : {slots_max / 2, slots_max}) {
+			int rc = hot_build(p, indices, n, K, s);
+			if (rc != ALPB_SUCCESS) {
+				ALPB_CUDA(cudaEventDestroy(e0));
+				ALPB_CUDA(cudaEventDestroy(e1));
+				return rc;
+			}
+			if (p->hot_k == 0) break;
+			p->hot_on = 1;
+			float total = 0;
+			for (int rep = 0; rep < 4; ++rep) {
+				ALPB_CUDA(cudaEventRecord(e0, s));
+				rc = dispatch_spmv(ring, a, p, ALPB_SCHED_MERGE_PATH, s);
+				if (rc != ALPB_SUCCESS) { hot_release(p); return rc; }
+				ALPB_CUDA(cudaEventRecord(e1, s));
+				ALPB_CUDA(cudaEventSynchronize(e1));
+				float ms = 0;
+				ALPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+				if (rep > 0) total += ms;
+			}
+			if (total < 0.98f * best) {
+				best = total;
+				best_k = K;
+			}
+		}
+		if (best_k == 0) hot_release(p);
+		else if (best_k != p->hot_k) {
+			const int rc = hot_build(p, indices, n, best_k, s);
+			if (rc != ALPB_SUCCESS) return rc;
+		}
+		p->hot_on = p->hot_k > 0 ? 1 : 0;
+	}
+	ALPB_CUDA(cudaEventDestroy(e0));
+	ALPB_CUDA(cudaEventDestroy(e1));
 	p->tuned_ms = best / 3.0f;
 	return ALPB_SUCCESS;
 }

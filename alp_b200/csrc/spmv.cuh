@@ -28,6 +28,19 @@ struct alpb_spmv_plan_s {
 	int64_t *tile_d = nullptr;
 	double mean = 0, maxlen = 0, cv = 0;
 	float tuned_ms = 0;
+	// Hot-column cache of the merge path, for skewed (power-law) matrices;
+	// made by the autotuner when it wins.  The hot_k most frequent columns of
+	// the index array `hot_src` get shared-memory slots: hot_idx is that
+	// array with every hot column replaced by (slot | 1 << 31), and each
+	// product gathers x at hot_cols into hot_x, which every block copies into
+	// shared memory, so the gathers of those nonzeroes never leave the SM.
+	int64_t hot_k = 0;
+	int hot_on = 0;
+	double hot_cover = 0;               // share of the nonzeroes in hot columns
+	const uint32_t *hot_src = nullptr;  // the column indices hot_idx was made from
+	uint32_t *hot_idx = nullptr;        // nnz
+	uint32_t *hot_cols = nullptr;       // hot_k
+	uint64_t *hot_x = nullptr;          // hot_k values (8 bytes hold any ring's type)
 };
 
 namespace alpb {

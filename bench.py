@@ -169,6 +169,9 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
     plan = dev.Plan(A, sched=abi.SCHED_AUTO)
     plan.autotune(abi.RING_PLUS_TIMES_F64, x, u)
     sched, vw, tiles = plan.info()
+    hot_slots, hot_cover = C.c_int64(), C.c_double()
+    abi.call("alpb_spmv_plan_hot_info", plan.h, C.byref(hot_slots), C.byref(hot_cover))
+    hot = hot_slots.value > 0
     nbytes = algorithmic_bytes(A.m, A.n, A.nnz)
 
     def step():
@@ -257,8 +260,9 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
     e2e_value = replica_rate(nbytes, e2e_ms, world)
 
     peaks = measured_peaks()
-    kernel_tag = (f"spmv_wmerge_rmat{args.scale}" if sched == abi.SCHED_MERGE_PATH
-                  else f"spmv_vector_rmat{args.scale}")
+    kernel_tag = (f"spmv_vector_rmat{args.scale}" if sched != abi.SCHED_MERGE_PATH
+                  else f"spmv_wmerge_hot_rmat{args.scale}" if hot
+                  else f"spmv_wmerge_rmat{args.scale}")
     traffic = profiled_traffic(kernel_tag)
     achieved = nbytes / (ms * 1e-3) / 1e9
     extra = {}
@@ -280,6 +284,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
                    "nnz": A.nnz, "edge_factor": EDGE_FACTOR, "rmat_abcd": [0.57, 0.19, 0.19, 0.05],
                    "seed": SEED, "schedule": {1: "merge_path", 2: "vector"}[sched],
                    "vector_width": vw, "tiles": tiles, "bytes_per_step": nbytes,
+                   "hot_columns": hot_slots.value, "hot_cover": round(hot_cover.value, 4),
                    "l2": "inputs larger than L2 (matrix 0.8 GB); no flush",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
@@ -287,8 +292,10 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
                      "frac": round(achieved / peaks["hbm_gbs"], 4),
                      "peak_source": peaks["source"],
                      "traffic": traffic,
-                     "kernel": "k_spmv_wmerge<RingPlusTimesF64> + k_wm_fixup" if sched == 1
-                     else f"k_spmv_vector_dense<RingPlusTimesF64,{vw}>"},
+                     "kernel": (f"k_spmv_vector_dense<RingPlusTimesF64,{vw}>" if sched != 1
+                                else "k_hot_gather + k_spmv_wmerge_hot<RingPlusTimesF64> + "
+                                     "k_wm_fixup" if hot
+                                else "k_spmv_wmerge<RingPlusTimesF64> + k_wm_fixup")},
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": A.n * 8,
                 "d2h_bytes_per_step": A.m * 8, "ms_per_step": round(e2e_ms, 5),
                 "pipelined": "copy-in of step k+1 and copy-out of step k overlap the products"},
@@ -303,10 +310,16 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
 
 
 def timed(fn, reps: int, stream):
+    """Device time of one call of fn (CUDA events on `stream`), mean of reps,
+    after a warm-up of at least two calls and half a second: a GPU that sat
+    idle (say, while the host ran a reference) takes that long to bring its
+    clocks back up, and a short solve timed earlier reads up to 20x slow."""
     import torch
-    for _ in range(2):
+    t0, k = time.time(), 0
+    while k < 2 or (time.time() - t0 < 0.5 and k < 200):
         fn()
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        k += 1
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(reps):

@@ -239,10 +239,26 @@ ALPB_API int alpb_gen_normal(double *out, int64_t count, uint64_t seed, uint64_t
 ALPB_API int alpb_spmv_plan_create(alpb_spmv_plan *plan, int64_t m, int64_t nnz,
 	const int64_t *offsets, int sched, int vector_width, void *stream);
 ALPB_API int alpb_spmv_plan_destroy(alpb_spmv_plan plan);
-/* Time the candidate schedules on this matrix/ring and keep the fastest. */
+/* Time the candidate schedules on this matrix/ring and keep the fastest; on
+ * the merge path of a large skewed matrix also try the hot-column cache at
+ * two sizes (alpb_spmv_plan_hot) and keep it when it is faster. */
 ALPB_API int alpb_spmv_autotune(alpb_spmv_plan plan, int ring, int64_t n,
 	const uint32_t *indices, const void *values, int value_type, const void *x,
 	void *y_scratch, void *stream);
+/* The hot-column cache of the merge path, for power-law matrices (the
+ * autotuner sets it up when it pays; this call sets it up by hand, or removes
+ * it with slots = 0).  The `slots` most frequent columns of `indices` (the
+ * storage's column indices, n columns, n < 2^31) get shared-memory slots:
+ * each dense product then gathers x at those columns once, every block copies
+ * them into shared memory, and their nonzeroes read x from there.  Results
+ * are bit-identical to the merge path without it.  The plan keeps a marked
+ * copy of `indices` (4 bytes per nonzero) and uses the cache only for products
+ * given that same index array.  slots <= a per-ring maximum (shared memory:
+ * 18,432 for 8-byte types); ALPB_ILLEGAL beyond it. */
+ALPB_API int alpb_spmv_plan_hot(alpb_spmv_plan plan, int ring, int64_t n,
+	const uint32_t *indices, int64_t slots, void *stream);
+/* slots in use (0: no cache) and the share of the nonzeroes they cover. */
+ALPB_API int alpb_spmv_plan_hot_info(alpb_spmv_plan plan, int64_t *slots, double *cover);
 /* chosen schedule and vector width (for reporting). */
 ALPB_API int alpb_spmv_plan_info(alpb_spmv_plan plan, int *sched, int *vector_width,
 	int64_t *tiles);
@@ -395,14 +411,15 @@ ALPB_API int alpb_vec_reduce(double *result, int add_op, double identity, int mu
 	const void *y, int y_type, const uint8_t *y_assigned, const void *mask,
 	const uint8_t *mask_assigned, int mask_type, int masked, void *stream);
 /* The same two primitives computing in the operator's own domain: `domain` is
- * ALPB_FP64 (double), ALPB_INT64 (int64_t) or ALPB_UINT64 (uint64_t); the C++
- * backend passes the domain of the ALP operator (its D3 type), as the
- * reference's operators cast their operands to it.  Integer domains compute
- * exactly with two's-complement wrap-around, and a narrower output type
- * truncates (int32 results wrap as 32-bit arithmetic does).  identity, alpha
- * and beta are the bits of a value of the domain type (memcpy of a double,
- * int64_t or uint64_t); *result of the reduction is a value of the domain type
- * (in: the scalar folded into; out: the result), folded on the device. */
+ * ALPB_FP64 (double), ALPB_INT64 (int64_t), ALPB_UINT64 (uint64_t), ALPB_INT32
+ * (int32_t) or ALPB_UINT32 (uint32_t); the C++ backend passes the domain of
+ * the operands' C++ types, as the reference's operators cast their operands
+ * to theirs.  Integer domains compute exactly with two's-complement
+ * wrap-around at their own width.  identity, alpha and beta hold the bits of
+ * a value of the domain type in their low bytes (memcpy of a double, int64_t,
+ * uint64_t, int32_t or uint32_t); *result of the reduction is a value of the
+ * domain type (in: the scalar folded into; out: the result), folded on the
+ * device. */
 ALPB_API int alpb_vec_op_dom(int kind, int op, int monoid, uint64_t identity, int mul_op,
 	uint32_t descr, int domain, int64_t n, void *z, int z_type, uint8_t *z_assigned,
 	int64_t *z_nnz, const void *mask, const uint8_t *mask_assigned, int mask_type, int masked,

@@ -177,20 +177,26 @@ namespace grb {
 
 			/** Compute domain of an element-wise primitive over operands of these
 			 *  C++ types, as the reference's operators cast to their domain:
-			 *  ALPB_FP64 when any is floating point, else ALPB_UINT64 when any is
-			 *  an unsigned 64-bit integer, else ALPB_INT64 (exact for bool and
-			 *  every narrower integer). */
+			 *  ALPB_FP64 when any is floating point; else the widest integer
+			 *  width among them (64 or 32 bits, bool and narrower types count as
+			 *  32), unsigned when an operand of that width is unsigned. */
 			template< typename... T >
 			struct domain_of {
-				static constexpr bool fp = false, u64 = false;
-				static constexpr int value = ALPB_INT64;
+				static constexpr bool fp = false, wide = false, u64 = false, u32 = false;
+				static constexpr int value = ALPB_INT32;
 			};
 			template< typename H, typename... T >
 			struct domain_of< H, T... > {
-				static constexpr bool fp = std::is_floating_point< H >::value || domain_of< T... >::fp;
-				static constexpr bool u64 = ( std::is_integral< H >::value &&
-					std::is_unsigned< H >::value && sizeof( H ) == 8 ) || domain_of< T... >::u64;
-				static constexpr int value = fp ? ALPB_FP64 : ( u64 ? ALPB_UINT64 : ALPB_INT64 );
+				typedef domain_of< T... > rest;
+				static constexpr bool is_int = std::is_integral< H >::value;
+				static constexpr bool fp = std::is_floating_point< H >::value || rest::fp;
+				static constexpr bool wide = ( is_int && sizeof( H ) == 8 ) || rest::wide;
+				static constexpr bool u64 = ( is_int && std::is_unsigned< H >::value &&
+					sizeof( H ) == 8 ) || rest::u64;
+				static constexpr bool u32 = ( is_int && std::is_unsigned< H >::value &&
+					sizeof( H ) == 4 ) || rest::u32;
+				static constexpr int value = fp ? ALPB_FP64 : wide ? ( u64 ? ALPB_UINT64 : ALPB_INT64 ) :
+					( u32 ? ALPB_UINT32 : ALPB_INT32 );
 			};
 
 			/** The bits of v as a value of domain `dom`.  Integer domains clamp to
@@ -207,6 +213,17 @@ namespace grb {
 					const int64_t i = v != v ? 0 : v <= lo ? std::numeric_limits< int64_t >::min() :
 						v >= hi ? std::numeric_limits< int64_t >::max() : static_cast< int64_t >( v );
 					std::memcpy( &b, &i, 8 );
+				} else if( dom == ALPB_INT32 ) {
+					const int32_t i = v != v ? 0 : v <= -2147483648.0L ? std::numeric_limits< int32_t >::min() :
+						v >= 2147483647.0L ? std::numeric_limits< int32_t >::max() :
+						static_cast< int32_t >( v );
+					std::memcpy( &b, &i, 4 );
+				} else if( dom == ALPB_UINT32 ) {
+					// a negative scalar wraps, as its conversion to an unsigned type does
+					const uint32_t u = v != v ? 0 : v >= 4294967295.0L ? 4294967295u :
+						v < 0 ? static_cast< uint32_t >( static_cast< int64_t >( v ) ) :
+						static_cast< uint32_t >( v );
+					std::memcpy( &b, &u, 4 );
 				} else {
 					const scalar_t hi = static_cast< scalar_t >( std::numeric_limits< uint64_t >::max() );
 					// a negative scalar wraps, as its conversion to an unsigned type does
@@ -227,6 +244,12 @@ namespace grb {
 					return static_cast< T >( d );
 				}
 				if( dom == ALPB_INT64 ) { return static_cast< T >( static_cast< int64_t >( b ) ); }
+				if( dom == ALPB_INT32 ) {
+					int32_t i;
+					std::memcpy( &i, &b, 4 );
+					return static_cast< T >( i );
+				}
+				if( dom == ALPB_UINT32 ) { return static_cast< T >( static_cast< uint32_t >( b ) ); }
 				return static_cast< T >( b );
 			}
 
