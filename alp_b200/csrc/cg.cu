@@ -12,10 +12,14 @@
 //   B: alpha = sigma / beta; x += alpha u_new; r -= alpha temp; r . r.
 //
 // The u update of the reference (u = r + (r.r / sigma) u, :455-468) is thus
-// folded into the next SpMV's gather, with u double-buffered so that no
-// block overwrites an entry another block still gathers.  Convergence is
-// tested exactly as the reference does (sqrt(r.r) < tol * ||b||, :437), and
-// the returned residual is r.r.
+// folded into the next SpMV's gather.  r and u are stored side by side, one
+// 16-byte pair per row, so that the gather of a nonzero is ONE load (one L1
+// wavefront) that brings both; phase A writes u_new to its own array, which
+// phase B folds back into the pairs, so no block overwrites a pair that
+// another block still gathers.  Convergence is tested exactly as the
+// reference does (sqrt(r.r) < tol * ||b||, :437), and the returned residual
+// is r.r.  Work space: pairs (2n doubles), u_new (n), temp (n); on return
+// its first n doubles hold the final residual vector r.
 #include "common.cuh"
 #include "merge.cuh"
 #include "wmerge.cuh"
@@ -42,7 +46,10 @@ struct CgArgs {
 	const uint32_t *indices;
 	const double *values;
 	const double *b;
-	double *x, *r, *u0, *u1, *temp;
+	double *x;
+	double2 *pr;   // (r_i, u_i)
+	double *u_new, *temp;
+	double *r_out; // the first n doubles of the work space: r on return
 	double *blk;  // [4][grid] block partials: prelude r.r, prelude b.b, beta, r.r
 	int64_t n, max_iter;
 	double tol;
@@ -72,43 +79,42 @@ struct PreludeEpi {
 		const double t = has ? 0.0 + v : 0.0;      // temp = 0; temp += A x
 		const double bi = sm->p0[i - base];
 		const double ri = (0.0 + bi) - t;           // r = 0; r += b; r -= temp
-		a->r[i] = ri;
-		a->u0[i] = 0.0;
+		a->pr[i] = make_double2(ri, 0.0);            // u = 0: gamma = 0 takes u = r
 		acc_rr += ri * ri;
 		acc_bb += bi * bi;
 	}
 };
 
 struct GatherU {
-	const double *r, *u_old;
+	const double2 *pr;
 	double gamma;
-	// r and u_old were written by other blocks before the last barrier: read
+	// the pairs were written by other blocks before the last barrier: read
 	// them through L2 (ld.global.cg) so no stale L1 line can be hit
 	__device__ __forceinline__ double operator()(uint32_t j) const {
-		return __ldcg(r + j) + gamma * __ldcg(u_old + j);
+		const double2 p = __ldcg(pr + j);
+		return p.x + gamma * p.y;
 	}
 };
 
 struct IterEpi {
 	const CgArgs *a;
 	CgWarpSmem *sm;
-	const double *u_old;
-	double *u_new;
 	double gamma;
 	int64_t base = 0;
 	double acc = 0.0;
 	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
 		base = i0;
 		for (int k = lane; k < nrows; k += 32) {
-			sm->p0[k] = __ldcg(a->r + i0 + k);
-			sm->p1[k] = __ldcg(u_old + i0 + k);
+			const double2 p = __ldcg(a->pr + i0 + k);
+			sm->p0[k] = p.x;
+			sm->p1[k] = p.y;
 		}
 	}
 	__device__ __forceinline__ void row(int64_t i, double v, bool has) {
 		const double t = has ? 0.0 + v : 0.0;      // temp = 0; temp += A u
 		a->temp[i] = t;
 		const double un = sm->p0[i - base] + gamma * sm->p1[i - base];
-		u_new[i] = un;
+		a->u_new[i] = un;
 		acc += t * un;
 	}
 };
@@ -167,13 +173,12 @@ __global__ void __launch_bounds__(32 * CG_WARPS, 6) k_cg(CgArgs a) {
 	double gamma = 0.0;
 	double rr = 0.0;
 	int64_t iter = 0;
-	double *u_old = a.u0, *u_new = a.u1;
 	for (;;) {
 		++iter;
 		// phase A: temp = A u_new, u_new = r + gamma u_old, beta terms
 		{
-			IterEpi epi{&a, &sm[w], u_old, u_new, gamma};
-			GatherU xl{a.r, u_old, gamma};
+			IterEpi epi{&a, &sm[w], gamma};
+			GatherU xl{a.pr, gamma};
 			++epoch;
 			int64_t t = gw;
 			WmMeta g = wm_meta(a.mt, t);
@@ -194,10 +199,10 @@ __global__ void __launch_bounds__(32 * CG_WARPS, 6) k_cg(CgArgs a) {
 		const double alpha = sigma / beta;
 		double part = 0.0;
 		for (int64_t i = rb + threadIdx.x; i < re; i += blockDim.x) {
-			const double un = __ldcg(u_new + i);
+			const double un = __ldcg(a.u_new + i);
 			a.x[i] = a.x[i] + alpha * un;
-			const double ri = __ldcg(a.r + i) - alpha * __ldcg(a.temp + i);
-			a.r[i] = ri;
+			const double ri = __ldcg(a.pr + i).x - alpha * __ldcg(a.temp + i);
+			a.pr[i] = make_double2(ri, un);
 			part += ri * ri;
 		}
 		part = block_sum(part, red);
@@ -207,10 +212,12 @@ __global__ void __launch_bounds__(32 * CG_WARPS, 6) k_cg(CgArgs a) {
 		if (sqrt(rr) < tol_abs || iter >= a.max_iter) break;
 		gamma = rr / sigma;  // alpha = beta / sigma in the reference's naming
 		sigma = rr;
-		double *tmp = u_old;
-		u_old = u_new;
-		u_new = tmp;
 	}
+	// r out to the first n doubles of the work space, which the pairs occupy:
+	// through temp, with a barrier between reading the pairs and overwriting them
+	for (int64_t i = rb + threadIdx.x; i < re; i += blockDim.x) a.temp[i] = __ldcg(a.pr + i).x;
+	if (!grid_sync(&st->gs)) return;
+	for (int64_t i = rb + threadIdx.x; i < re; i += blockDim.x) a.r_out[i] = __ldcg(a.temp + i);
 	if (blockIdx.x == 0 && threadIdx.x == 0) {
 		st->iterations = iter;
 		st->residual = rr;
@@ -248,7 +255,10 @@ extern "C" int alpb_cg_solve(int64_t n, const int64_t *row_ptr, const uint32_t *
 	}
 	const int grid = solver_grid(k_cg, 32 * CG_WARPS, plan->ntiles, CG_WARPS);
 	ALPB_CHECK(grid > 0, ALPB_PANIC, "alpb_cg_solve: no cooperative occupancy");
-	double *wk = work, *own_work = nullptr, *scratch = nullptr;
+	// the (r, u) pairs take 16-byte loads: a work space that is not 16-byte
+	// aligned is replaced by an internal one
+	double *wk = (reinterpret_cast<uintptr_t>(work) & 15) ? nullptr : work;
+	double *own_work = nullptr, *scratch = nullptr;
 	CgState *st = nullptr;
 	if (!wk) {
 		ALPB_CUDA(cudaMallocAsync(&own_work, size_t(4 * n) * 8, s));
@@ -264,10 +274,10 @@ extern "C" int alpb_cg_solve(int64_t n, const int64_t *row_ptr, const uint32_t *
 	a.values = values;
 	a.b = b;
 	a.x = x;
-	a.r = wk;
-	a.u0 = wk + n;
-	a.u1 = wk + 2 * n;
+	a.pr = reinterpret_cast<double2 *>(wk);
+	a.u_new = wk + 2 * n;
 	a.temp = wk + 3 * n;
+	a.r_out = wk;
 	a.blk = scratch;
 	a.n = n;
 	a.max_iter = max_iter;

@@ -170,6 +170,260 @@ __global__ void __launch_bounds__(32 * PR_WARPS, 6) k_pagerank(PrArgs a) {
 	}
 }
 
+// ------------------------------------------------ large graphs: per-step --
+// For large graphs one cooperative kernel is the wrong shape: its columns
+// that cross warp tiles wait on each other in tile order, and its grid is
+// capped at what stays co-resident.  There every iteration is instead three
+// ordinary launches -- the product over the CCS with the same row epilogue
+// (k_pr_step; a column that crosses tiles leaves per-tile partials), the
+// crossing columns' epilogue (k_pr_fix), and one block that sums the block
+// partials in a fixed order and decides whether to stop (k_pr_finish).
+// Iterations are queued in chunks; once the stop is decided every queued
+// kernel returns at once, and the host reads the state once per chunk.
+constexpr int PRS_WARPS = 4;
+constexpr int PRS_CHUNK = 8;
+
+struct PrStepState {
+	int64_t iterations;
+	double residual, d;
+	int done;
+};
+
+struct PrStepArgs {
+	MergeTables mt;                // over the CCS
+	const int64_t *ccs_ptr;
+	const uint32_t *ccs_row;
+	const double *ccs_val;
+	const int64_t *crs_ptr;
+	const double *crs_val;
+	double *pr, *rs, *next0, *next1;
+	double *blk;                   // [2][grid]: residual, dangling of k_pr_step
+	double *fix;                   // [2][fix_grid]: the same of k_pr_fix
+	int grid, fix_grid;
+	int64_t n, max_iter;
+	double alpha, conv;
+	int init_given;
+	PrStepState *st;
+};
+
+// the row epilogue of both kernels (old pr and the row scale read directly)
+struct PrStepEpi {
+	const PrStepArgs *a;
+	PrWarpSmem *sm;                // null: no per-tile prefetch (the crossing columns)
+	double *next_out;
+	double d;
+	int64_t base = 0;
+	double acc_res = 0.0, acc_dang = 0.0;
+	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
+		base = i0;
+		for (int k = lane; k < nrows; k += 32) {
+			sm->old_pr[k] = a->pr[i0 + k];
+			sm->rs[k] = __ldg(a->rs + i0 + k);
+		}
+	}
+	__device__ __forceinline__ void row(int64_t j, double v, bool has) {
+		const double nn = has ? 0.0 + v : 0.0;       // pr_nextnext = 0; += pr_next L
+		const double old = sm ? sm->old_pr[j - base] : a->pr[j];
+		const double nw = nn + d;                    // pr = pr_nextnext + dangling
+		a->pr[j] = nw;
+		acc_res += old > nw ? old - nw : nw - old;
+		const double rsj = sm ? sm->rs[j - base] : a->rs[j];
+		if (rsj == 0.0) {                            // input of the next iteration
+			next_out[j] = 0.0;
+			acc_dang += nw;
+		} else {
+			next_out[j] = nw * rsj;
+		}
+	}
+};
+
+struct GatherRO {
+	const double *__restrict__ x;
+	__device__ __forceinline__ double operator()(uint32_t j) const { return __ldg(x + j); }
+};
+
+// set-up (:224-289 and the initial guess): row scales, pr, the pre-scaled
+// first input and the blocks' dangling mass
+__global__ void __launch_bounds__(256) k_pr_setup(PrStepArgs a) {
+	__shared__ double red[33];
+	const int lane = threadIdx.x & 31;
+	const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+	const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	double dang = 0.0;
+	for (int64_t i = warp; i < a.n; i += nwarps) {
+		const int64_t b = a.crs_ptr[i], e = a.crs_ptr[i + 1];
+		double cnt = 0.0;
+		for (int64_t k = b + lane; k < e; k += 32)
+			cnt += (a.crs_val == nullptr || a.crs_val[k] != 0.0) ? 1.0 : 0.0;
+		for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+		if (lane == 0) {
+			const double rsi = cnt > 0.0 ? a.alpha / cnt : 0.0;
+			a.rs[i] = rsi;
+			const double p = a.init_given ? a.pr[i] : 1.0 / double(a.n);
+			a.pr[i] = p;
+			if (rsi == 0.0) {
+				a.next0[i] = 0.0;
+				dang += p;
+			} else {
+				a.next0[i] = p * rsi;
+			}
+		}
+	}
+	dang = block_sum(dang, red);
+	if (threadIdx.x == 0) {
+		a.blk[blockIdx.x] = 0.0;
+		a.blk[a.grid + blockIdx.x] = dang;
+	}
+}
+
+__global__ void __launch_bounds__(32 * PRS_WARPS, 6) k_pr_step(PrStepArgs a, int parity) {
+	if (a.st->done) return;
+	__shared__ PrWarpSmem sm[PRS_WARPS];
+	__shared__ double red[33];
+	const int w = threadIdx.x >> 5;
+	PrStepEpi epi{&a, &sm[w], parity ? a.next0 : a.next1, a.st->d};
+	GatherRO xl{parity ? a.next1 : a.next0};
+	const int64_t nw = int64_t(gridDim.x) * PRS_WARPS;
+	int64_t t = int64_t(blockIdx.x) * PRS_WARPS + w;
+	WmMeta g = wm_meta(a.mt, t);
+	while (t < a.mt.ntiles) {
+		const WmMeta next = wm_meta(a.mt, t + nw);
+		warp_tile<RF>(t, g, a.mt, a.ccs_ptr, a.ccs_row, a.ccs_val, xl, epi, 0, sm[w].tile);
+		t += nw;
+		g = next;
+	}
+	const double s1 = block_sum(epi.acc_res, red);
+	const double s2 = block_sum(epi.acc_dang, red);
+	if (threadIdx.x == 0) {
+		a.blk[blockIdx.x] = s1;
+		a.blk[a.grid + blockIdx.x] = s2;
+	}
+}
+
+// columns that cross tiles: their partials summed in tile order (tail slots
+// of the first..last-1 tiles, head slot of the last), then the epilogue
+__global__ void __launch_bounds__(256) k_pr_fix(PrStepArgs a, int parity) {
+	if (a.st->done) return;
+	__shared__ double red[33];
+	const MergeTables &mt = a.mt;
+	PrStepEpi epi{&a, nullptr, parity ? a.next0 : a.next1, a.st->d};
+	const int lane = threadIdx.x & 31;
+	const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+	const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	for (int64_t base = warp * 32; base < mt.ntiles; base += nwarps * 32) {
+		const int64_t t = base + lane;
+		const int32_t n = t < mt.ntiles ? mt.span_len[t] : 0;
+		if (n > 0 && n <= 32) {
+			double v = 0.0;
+			for (int64_t k = t; k < t + n - 1; ++k) v += load_bits<double>(mt.tail_val + k);
+			v += load_bits<double>(mt.head_val + t + n - 1);
+			epi.row(mt.tile_row[t + 1], v, true);
+		}
+		unsigned long_rows = __ballot_sync(0xffffffffu, n > 32);
+		while (long_rows) {
+			const int src = __ffs(long_rows) - 1;
+			long_rows &= long_rows - 1;
+			const int64_t f = base + src;
+			const int32_t nn = __shfl_sync(0xffffffffu, n, src);
+			double v = 0.0;
+			for (int64_t k = f + lane; k < f + nn - 1; k += 32) v += load_bits<double>(mt.tail_val + k);
+			for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+			if (lane == 0) {
+				v += load_bits<double>(mt.head_val + f + nn - 1);
+				epi.row(mt.tile_row[f + 1], v, true);
+			}
+		}
+	}
+	const double s1 = block_sum(epi.acc_res, red);
+	const double s2 = block_sum(epi.acc_dang, red);
+	if (threadIdx.x == 0) {
+		a.fix[blockIdx.x] = s1;
+		a.fix[a.fix_grid + blockIdx.x] = s2;
+	}
+}
+
+// residual and dangling mass in a fixed order; the next teleport term; stop
+// after an iteration whose residual is <= conv (:490) or at max_iter.
+// setup != 0: only the first term (no iteration has run).
+__global__ void __launch_bounds__(256) k_pr_finish(PrStepArgs a, int setup) {
+	__shared__ double red[33];
+	PrStepState *st = a.st;
+	if (st->done) return;
+	const double r1 = block_sum_array(a.blk, a.grid, red);
+	const double d1 = block_sum_array(a.blk + a.grid, a.grid, red);
+	const double r2 = setup ? 0.0 : block_sum_array(a.fix, a.fix_grid, red);
+	const double d2 = setup ? 0.0 : block_sum_array(a.fix + a.fix_grid, a.fix_grid, red);
+	if (threadIdx.x == 0) {
+		const double dang = d1 + d2;
+		st->d = (a.alpha * dang + 1 - a.alpha) / double(a.n);     // (:390)
+		if (!setup) {
+			st->residual = r1 + r2;
+			st->iterations += 1;
+			if ((a.conv != 0.0 && st->residual <= a.conv) || st->iterations >= a.max_iter)
+				st->done = 1;
+		}
+	}
+}
+
+static int pagerank_steps(const PrStepArgs &tmpl, alpb_spmv_plan plan, int64_t *iterations,
+	double *residual, cudaStream_t s) {
+	PrStepArgs a = tmpl;
+	static int per_sm = 0;
+	if (!per_sm) {
+		ALPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_step,
+			32 * PRS_WARPS, 0));
+		if (per_sm < 1) per_sm = 1;
+	}
+	int64_t g = (plan->ntiles + PRS_WARPS - 1) / PRS_WARPS;
+	if (g > int64_t(per_sm) * sm_count()) g = int64_t(per_sm) * sm_count();
+	a.grid = int(g < 1 ? 1 : g);
+	a.fix_grid = int(grid_for((plan->ntiles + 31) / 32 * 32, 256));
+	double *part = nullptr;
+	PrStepState *st = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&part, size_t(2 * a.grid + 2 * a.fix_grid) * 8, s));
+	ALPB_CUDA(cudaMallocAsync(&st, sizeof(PrStepState), s));
+	ALPB_CUDA(cudaMemsetAsync(st, 0, sizeof(PrStepState), s));
+	a.blk = part;
+	a.fix = part + 2 * a.grid;
+	a.st = st;
+	k_pr_setup<<<a.grid, 256, 0, s>>>(a);
+	ALPB_LAUNCHED();
+	k_pr_finish<<<1, 256, 0, s>>>(a, 1);
+	ALPB_LAUNCHED();
+	PrStepState h{};
+	int64_t queued = 0;
+	while (queued < a.max_iter) {
+		const int64_t chunk = a.max_iter - queued < PRS_CHUNK ? a.max_iter - queued : PRS_CHUNK;
+		for (int64_t k = 0; k < chunk; ++k) {
+			const int parity = int((queued + k) & 1);
+			k_pr_step<<<a.grid, 32 * PRS_WARPS, 0, s>>>(a, parity);
+			ALPB_LAUNCHED();
+			k_pr_fix<<<a.fix_grid, 256, 0, s>>>(a, parity);
+			ALPB_LAUNCHED();
+			k_pr_finish<<<1, 256, 0, s>>>(a, 0);
+			ALPB_LAUNCHED();
+		}
+		queued += chunk;
+		ALPB_CUDA(cudaMemcpyAsync(&h, st, sizeof(PrStepState), cudaMemcpyDeviceToHost, s));
+		ALPB_CUDA(cudaStreamSynchronize(s));
+		if (h.done) break;
+	}
+	ALPB_CUDA(cudaFreeAsync(part, s));
+	ALPB_CUDA(cudaFreeAsync(st, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	*iterations = h.iterations;
+	*residual = h.residual;
+	if (!(h.residual <= a.conv)) {
+		set_error("alpb_pagerank: not converged after %lld iterations (residual %g)",
+			(long long) h.iterations, h.residual);
+		return ALPB_FAILED;
+	}
+	return ALPB_SUCCESS;
+}
+
+// Graphs from this many nonzeroes on take the per-step launches.
+constexpr int64_t kPrStepNnz = int64_t(1) << 23;
+
 // The solve proper.  plan: a WM_TILE plan of the CCS offsets, or null (one is
 // made and destroyed here); work: 3n doubles of scratch, or null.
 static int pagerank_run(int64_t n, const int64_t *crs_row_ptr, const double *crs_values,
@@ -185,6 +439,36 @@ static int pagerank_run(int64_t n, const int64_t *crs_row_ptr, const double *crs
 			WM_TILE, s);
 		if (rc != ALPB_SUCCESS) return rc;
 		plan = own_plan;
+	}
+	if (plan->nnz >= kPrStepNnz) {
+		double *vecs = work, *own_vecs = nullptr;
+		if (!vecs) {
+			ALPB_CUDA(cudaMallocAsync(&own_vecs, size_t(3 * n) * 8, s));
+			vecs = own_vecs;
+		}
+		PrStepArgs a{};
+		a.mt = merge_tables(*plan);
+		a.ccs_ptr = ccs_col_ptr;
+		a.ccs_row = ccs_row_idx;
+		a.ccs_val = ccs_values;
+		a.crs_ptr = crs_row_ptr;
+		a.crs_val = crs_values;
+		a.pr = pr;
+		a.rs = vecs;
+		a.next0 = vecs + n;
+		a.next1 = vecs + 2 * n;
+		a.n = n;
+		a.max_iter = max_iter;
+		a.alpha = alpha;
+		a.conv = conv;
+		a.init_given = init_given;
+		const int rc = pagerank_steps(a, plan, iterations, residual, s);
+		if (own_vecs) {
+			cudaFreeAsync(own_vecs, s);
+			cudaStreamSynchronize(s);
+		}
+		alpb_spmv_plan_destroy(own_plan);
+		return rc;
 	}
 	const int grid = solver_grid(k_pagerank, 32 * PR_WARPS, plan->ntiles, PR_WARPS);
 	if (grid <= 0) {

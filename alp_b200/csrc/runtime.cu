@@ -64,6 +64,14 @@ int alpb_init(int device) {
 	ALPB_CHECK(device >= 0 && device < n, ALPB_ILLEGAL, "alpb_init: device %d of %d", device, n);
 	ALPB_CUDA(cudaSetDevice(device));
 	ALPB_CUDA(cudaFree(nullptr));  // create the primary context now
+	// the entry points take their small per-call scratch (block partials,
+	// solver state) stream-ordered from the device's default pool: keep what
+	// they free in the pool instead of returning it to the driver at every
+	// synchronisation, so that repeated calls reuse it
+	cudaMemPool_t pool;
+	ALPB_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+	uint64_t keep = UINT64_MAX;
+	ALPB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
 	return ALPB_SUCCESS;
 }
 

@@ -216,14 +216,13 @@ struct WarpAccumulateY {
 	}
 };
 
-template <class R>
+template <class R, class XL>
 __global__ void __launch_bounds__(32 * WM_WARPS, ALPB_WM_MIN_BLOCKS)
 k_spmv_wmerge(MergeTables mt, const int64_t *__restrict__ offsets,
 	const uint32_t *__restrict__ indices, const typename R::T *__restrict__ values,
-	const typename R::T *__restrict__ x, typename R::T *__restrict__ y, int left) {
+	XL xl, typename R::T *__restrict__ y, int left) {
 	__shared__ WarpSmem<R> sm[WM_WARPS];
 	__shared__ typename R::T ybuf[WM_WARPS][WM_TILE];
-	PlainX<typename R::T> xl{x};
 	WarpAccumulateY<R> epi{y, ybuf[threadIdx.x >> 5]};
 	const int w = threadIdx.x >> 5;
 	const int64_t nw = int64_t(gridDim.x) * WM_WARPS;
@@ -245,7 +244,7 @@ k_spmv_wmerge(MergeTables mt, const int64_t *__restrict__ offsets,
 // memory.  Products and sums are those of k_spmv_wmerge, bit for bit.
 constexpr uint32_t kHotBit = 0x80000000u;
 #ifndef ALPB_HOT_WARPS
-#define ALPB_HOT_WARPS 16
+#define ALPB_HOT_WARPS 32
 #endif
 constexpr int HOT_WARPS = ALPB_HOT_WARPS;   // one block of these per SM
 
@@ -463,6 +462,7 @@ int launch_merge(const SpmvArgs &a, const alpb_spmv_plan_s &p, cudaStream_t s) {
 	using T = typename R::T;
 	if (p.ntiles == 0) return ALPB_SUCCESS;
 	if (p.tile == WM_TILE && p.hot_on && p.hot_k > 0 && a.indices == p.hot_src) {
+		// shared-memory slots (one block per SM)
 		const size_t smem = HotSmem<R>::bytes(p.hot_k);
 		static size_t smem_set = 0;
 		if (smem > smem_set) {
@@ -487,16 +487,16 @@ int launch_merge(const SpmvArgs &a, const alpb_spmv_plan_s &p, cudaStream_t s) {
 		static int blocks_per_sm = 0;
 		if (!blocks_per_sm) {
 			ALPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
-				k_spmv_wmerge<R>, 32 * WM_WARPS, 0));
+				k_spmv_wmerge<R, PlainX<T>>, 32 * WM_WARPS, 0));
 			if (blocks_per_sm < 1) blocks_per_sm = 1;
 		}
 		int64_t grid = (p.ntiles + WM_WARPS - 1) / WM_WARPS;
 		const int64_t cap = int64_t(sm_count()) * blocks_per_sm;
 		if (grid > cap) grid = cap;
 		const MergeTables mt = merge_tables(p);
-		k_spmv_wmerge<R><<<unsigned(grid), 32 * WM_WARPS, 0, s>>>(mt, a.offsets, a.indices,
-			reinterpret_cast<const T *>(a.values), reinterpret_cast<const T *>(a.v),
-			reinterpret_cast<T *>(a.u), a.left);
+		k_spmv_wmerge<R, PlainX<T>><<<unsigned(grid), 32 * WM_WARPS, 0, s>>>(mt, a.offsets,
+			a.indices, reinterpret_cast<const T *>(a.values),
+			PlainX<T>{reinterpret_cast<const T *>(a.v)}, reinterpret_cast<T *>(a.u), a.left);
 		ALPB_LAUNCHED();
 		// rows crossing tiles: one lane per 32 tiles' worth of first tiles
 		k_wm_fixup<R><<<grid_for((p.ntiles + 31) / 32 * 32, 256), 256, 0, s>>>(mt,
@@ -855,6 +855,8 @@ int alpb_spmv_plan_hot(alpb_spmv_plan p, int ring, int64_t n, const uint32_t *in
 	ALPB_CHECK(slots >= 0 && slots <= hot_slots_max(ring), ALPB_ILLEGAL,
 		"alpb_spmv_plan_hot: %lld slots (at most %lld for semiring %d)", (long long) slots,
 		(long long) hot_slots_max(ring), ring);
+	ALPB_CHECK(slots < n || slots == 0, ALPB_ILLEGAL,
+		"alpb_spmv_plan_hot: %lld slots for %lld columns", (long long) slots, (long long) n);
 	ALPB_CHECK(slots == 0 || (indices != nullptr && n > 0), ALPB_ILLEGAL,
 		"alpb_spmv_plan_hot: null indices");
 	ALPB_CHECK(slots == 0 || p->tile == WM_TILE, ALPB_UNSUPPORTED,
@@ -919,26 +921,33 @@ int alpb_spmv_autotune(alpb_spmv_plan p, int ring, int64_t n, const uint32_t *in
 	p->sched = cands[best_i].sched;
 	p->vw = cands[best_i].sched == ALPB_SCHED_VECTOR ? cands[best_i].w : saved_vw;
 	// skewed rows on the merge path: try the hot-column cache at two sizes
-	// (its shared memory bounds the slots for the ring's type)
+	// (beyond them its shared memory takes too much of the SM's L1)
 	hot_release(p);
 	if (p->sched == ALPB_SCHED_MERGE_PATH && p->tile == WM_TILE && n >= (int64_t(1) << 16) &&
 		p->nnz >= (int64_t(1) << 20)) {
-		const int64_t slots_max = hot_slots_max(ring);
-		int64_t best_k = 0;
-		for (const int64_t K : {slots_max / 2, slots_max}) {
-			int rc = hot_build(p, indices, n, K, s);
+		struct HotCand { int64_t k; } hc[2] = {{std::min<int64_t>(2048, hot_slots_max(ring))},
+			{std::min<int64_t>(4096, hot_slots_max(ring))}};
+		int best_c = -1;
+		for (int c = 0; c < 2; ++c) {
+			if (hc[c].k <= 0 || hc[c].k >= n) continue;
+			int rc = hot_build(p, indices, n, hc[c].k, s);
 			if (rc != ALPB_SUCCESS) {
-				ALPB_CUDA(cudaEventDestroy(e0));
-				ALPB_CUDA(cudaEventDestroy(e1));
+				cudaEventDestroy(e0);
+				cudaEventDestroy(e1);
 				return rc;
 			}
-			if (p->hot_k == 0) break;
+			if (p->hot_k == 0) continue;
 			p->hot_on = 1;
 			float total = 0;
 			for (int rep = 0; rep < 4; ++rep) {
 				ALPB_CUDA(cudaEventRecord(e0, s));
 				rc = dispatch_spmv(ring, a, p, ALPB_SCHED_MERGE_PATH, s);
-				if (rc != ALPB_SUCCESS) { hot_release(p); return rc; }
+				if (rc != ALPB_SUCCESS) {
+					hot_release(p);
+					cudaEventDestroy(e0);
+					cudaEventDestroy(e1);
+					return rc;
+				}
 				ALPB_CUDA(cudaEventRecord(e1, s));
 				ALPB_CUDA(cudaEventSynchronize(e1));
 				float ms = 0;
@@ -947,15 +956,15 @@ int alpb_spmv_autotune(alpb_spmv_plan p, int ring, int64_t n, const uint32_t *in
 			}
 			if (total < 0.98f * best) {
 				best = total;
-				best_k = K;
+				best_c = c;
 			}
 		}
-		if (best_k == 0) hot_release(p);
-		else if (best_k != p->hot_k) {
-			const int rc = hot_build(p, indices, n, best_k, s);
+		hot_release(p);
+		if (best_c >= 0) {
+			const int rc = hot_build(p, indices, n, hc[best_c].k, s);
 			if (rc != ALPB_SUCCESS) return rc;
+			p->hot_on = p->hot_k > 0 ? 1 : 0;
 		}
-		p->hot_on = p->hot_k > 0 ? 1 : 0;
 	}
 	ALPB_CUDA(cudaEventDestroy(e0));
 	ALPB_CUDA(cudaEventDestroy(e1));

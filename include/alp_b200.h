@@ -137,6 +137,9 @@ typedef struct alpb_spmv_plan_s *alpb_spmv_plan;
  * Runtime (replaces grb::init / grb::finalize,
  * src/graphblas/reference/init.cpp:45-113, include/graphblas/base/init.hpp)
  * ====================================================================== */
+/* Makes `device` current and its context ready; the device's default
+ * memory pool then keeps the stream-ordered scratch that entry points free
+ * (its release threshold is raised), so that repeated calls reuse it. */
 ALPB_API int alpb_init(int device);
 ALPB_API int alpb_finalize(void);
 ALPB_API const char *alpb_last_error(void);
@@ -249,12 +252,14 @@ ALPB_API int alpb_spmv_autotune(alpb_spmv_plan plan, int ring, int64_t n,
  * autotuner sets it up when it pays; this call sets it up by hand, or removes
  * it with slots = 0).  The `slots` most frequent columns of `indices` (the
  * storage's column indices, n columns, n < 2^31) get shared-memory slots:
- * each dense product then gathers x at those columns once, every block copies
- * them into shared memory, and their nonzeroes read x from there.  Results
- * are bit-identical to the merge path without it.  The plan keeps a marked
- * copy of `indices` (4 bytes per nonzero) and uses the cache only for products
- * given that same index array.  slots <= a per-ring maximum (shared memory:
- * 18,432 for 8-byte types); ALPB_ILLEGAL beyond it. */
+ * each dense product gathers x at those columns once, one block per SM
+ * copies them into shared memory, and their nonzeroes read x from there
+ * (random 8-byte shared loads cost a few L1 wavefronts per warp instead of
+ * one per lane).  Results are bit-identical to the merge path without it.
+ * The plan keeps a marked copy of `indices` (4 bytes per nonzero) and uses
+ * the cache only for products given that same index array.  slots <= a
+ * per-ring maximum (shared memory: 8,192 for 8-byte types); ALPB_ILLEGAL
+ * beyond it. */
 ALPB_API int alpb_spmv_plan_hot(alpb_spmv_plan plan, int ring, int64_t n,
 	const uint32_t *indices, int64_t slots, void *stream);
 /* slots in use (0: no cache) and the share of the nonzeroes they cover. */
@@ -445,8 +450,10 @@ ALPB_API int alpb_reduce_f64(double *result, int op, int64_t n, const double *x,
  * sqrt(r.r) < tol or after max_iter; *residual = r.r (not its root).  All
  * FP64.  Fused: two passes over HBM per iteration (SpMV + dot, then the
  * x/r/u updates + r.r), device-side scalars, no host sync per iteration.
- * x holds the initial guess on entry.  `work` is 4*n doubles of scratch or
- * NULL (allocated internally).  Returns ALPB_FAILED when not converged.  */
+ * x holds the initial guess on entry.  `work` is 4*n doubles of scratch
+ * (16-byte aligned; otherwise, or when NULL, the solver allocates its own);
+ * on return its first n doubles hold the final residual vector r.  Returns
+ * ALPB_FAILED when not converged.  */
 ALPB_API int alpb_cg_solve(int64_t n, const int64_t *row_ptr, const uint32_t *col_idx,
 	const double *values, const double *b, double *x, int64_t max_iter, double tol,
 	int64_t *iterations, double *residual, double *work, alpb_spmv_plan plan,

@@ -132,18 +132,28 @@ def test_pagerank_rmat_matches_restatement(cuda, oracle, scale):
     assert abs(pr.sum() - 1.0) < 1e-8
 
 
-def test_pagerank_planned_equals_plain(cuda):
+@pytest.mark.parametrize("scale", [14, 20])
+def test_pagerank_planned_equals_plain(cuda, oracle, scale):
     """alpb_pagerank_planned with a caller-held plan of the CCS and scratch
     gives alpb_pagerank's result bit for bit (same tiles, same grid), on two
-    solves in a row with the same plan; a plan of other offsets is refused."""
+    solves in a row with the same plan; a plan of other offsets is refused.
+    Scale 14 runs the single cooperative kernel, scale 20 (16 M nonzeroes)
+    the per-step launches of large graphs, which are also checked against
+    the restatement."""
     import torch
     from alp_b200 import _abi as abi
     dev = _dev()
-    L = dev.rmat(14, vtype=FP64, seed=8)
+    L = dev.rmat(scale, vtype=FP64, seed=8)
     L.values.fill_(1.0)
     LT = dev.transpose(L)
     rc, pr, it, res = pagerank_device(L, LT)
     assert rc == 0
+    if scale == 20:
+        o, i, v = L.to_host()
+        to, ti, tv = LT.to_host()
+        rc2, pr2, it2, _ = oracle.pagerank(o, i, v, to, ti, tv)
+        assert rc2 == 0 and it == it2
+        np.testing.assert_allclose(pr, pr2, rtol=1e-10, atol=1e-10 * np.abs(pr2).max())
     plan = dev.Plan(LT, sched=abi.SCHED_AUTO)
     work = torch.empty(3 * L.m, dtype=torch.float64, device="cuda")
     for use_work in (True, False):
