@@ -68,6 +68,7 @@ PROTOS: dict[str, list] = {
     "alpb_gen_edge_values": [P, I32, P, P, I64, I64, U64, C.c_int32, C.c_int32, P],
     "alpb_keys_sort_unique": [P, I64, PI64, P],
     "alpb_crs_from_sorted_keys": [P, I64, I64, P, P, P],
+    "alpb_mm_read": [C.c_char_p, I32, PI64, PI64, PI64, C.POINTER(P), C.POINTER(P), C.POINTER(P), P],
     "alpb_coo_to_crs": [I64, I64, I64, P, P, P, I32, P, P, P, P],
     "alpb_crs_transpose": [I64, I64, I64, P, P, P, I32, P, P, P, P],
     "alpb_gen_stencil_crs": [I32, PI64, D, D, I32, P, P, P, PI64, P],

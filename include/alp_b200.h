@@ -199,6 +199,20 @@ ALPB_API int alpb_crs_from_sorted_keys(const uint64_t *keys, int64_t nnz, int64_
 ALPB_API int alpb_coo_to_crs(int64_t m, int64_t n, int64_t nnz, const uint32_t *I,
 	const uint32_t *J, const void *values, int type, int64_t *row_ptr,
 	uint32_t *col_idx, void *out_values, void *stream);
+/* A MatrixMarket coordinate file (real, integer or pattern; general or
+ * symmetric) straight to the device, for buildMatrixUnique-style ingest
+ * (replaces ALP's host-side grb::utils::MatrixFileReader and its nonzero
+ * iterator, include/graphblas/utils/parser/matrixFileIterator.hpp, and
+ * src/graphblas/utils/hpparser.c).  The text is parsed on the host by all
+ * cores at once; *rows, *cols (uint32[*nnz]) and *values (*nnz values of
+ * value_type: FP64, INT32, BOOL (nonzero = true), or VOID for none) are new
+ * device allocations the caller releases with alpb_free.  Triples come in the
+ * order ALP's iterator yields them: file order, 0-based, a symmetric file's
+ * off-diagonal entries each followed by its mirror; a pattern file's values
+ * are 1.  ALPB_ILLEGAL for a malformed file, ALPB_UNSUPPORTED for complex or
+ * skew/Hermitian files. */
+ALPB_API int alpb_mm_read(const char *path, int value_type, int64_t *m, int64_t *n,
+	int64_t *nnz, uint32_t **rows, uint32_t **cols, void **values, void *stream);
 /* CCS (= CRS of the transpose) from CRS; stable, so within a column entries
  * appear in increasing row order. */
 ALPB_API int alpb_crs_transpose(int64_t m, int64_t n, int64_t nnz,

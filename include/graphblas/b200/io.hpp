@@ -7,11 +7,13 @@
 #define _H_GRB_B200_IO
 
 #include <cstdint>
+#include <string>
 #include <type_traits>
 #include <vector>
 
 #include <graphblas/base/io.hpp>
 #include <graphblas/blas0.hpp>
+
 #include <graphblas/b200/matrix.hpp>
 #include <graphblas/b200/runtime.hpp>
 #include <graphblas/b200/vector.hpp>
@@ -410,6 +412,49 @@ namespace grb {
 	template< typename InputType, typename RIT, typename CIT, typename NIT, typename... Args >
 	RC wait( const Matrix< InputType, b200, RIT, CIT, NIT > &, const Args &... ) {
 		return wait< b200 >();
+	}
+
+	/**
+	 * A MatrixMarket coordinate file straight into a b200 matrix: an extension
+	 * of the b200 backend with no counterpart in the reference, where a program
+	 * reads the file through grb::utils::MatrixFileReader and passes its
+	 * nonzero iterator to buildMatrixUnique (the text parsed and the storage
+	 * built on one host core).  Here the file is parsed by every host core
+	 * (alpb_mm_read), the triples go to the device in one copy, and the device
+	 * builds both orientations -- the same matrix, nonzero for nonzero and in
+	 * the same in-row order, as ALP's reader followed by buildMatrixUnique.
+	 * Symmetric files are expanded as ALP's reader expands them; a pattern
+	 * file's entries take the value one.  Value types: double, int, bool and
+	 * void (pattern).  MISMATCH when the file's dimensions are not A's.
+	 */
+	template< typename D, typename RIT, typename CIT, typename NIT >
+	RC buildMatrixUniqueFromFile( Matrix< D, b200, RIT, CIT, NIT > &A, const std::string &path ) {
+		using namespace internal::b200rt;
+		const int vt = type_code< D >::value;
+		if( vt != ALPB_FP64 && vt != ALPB_INT32 && vt != ALPB_BOOL && vt != ALPB_VOID ) {
+			return UNSUPPORTED;
+		}
+		int64_t m = 0, n = 0, nz = 0;
+		uint32_t *I = nullptr, *J = nullptr;
+		void *V = nullptr;
+		RC rc = check( alpb_mm_read( path.c_str(), vt, &m, &n, &nz, &I, &J, &V, stream() ),
+			"buildMatrixUniqueFromFile" );
+		if( rc != SUCCESS ) { return rc; }
+		if( size_t( m ) != A.b200_rows() || size_t( n ) != A.b200_cols() ) {
+			rc = MISMATCH;
+		} else {
+			try {
+				rc = A.b200_build_device( I, J,
+					static_cast< const typename Matrix< D, b200, RIT, CIT, NIT >::storage_type * >( V ),
+					static_cast< size_t >( nz ) );
+			} catch( ... ) {
+				rc = OUTOFMEM;
+			}
+		}
+		release( I );
+		release( J );
+		release( V );
+		return rc;
 	}
 
 }

@@ -406,16 +406,33 @@ namespace grb {
 				const size_t nz = I.size();
 				const int vt = type_code< D >::value;
 				if( vt < 0 ) { return UNSUPPORTED; }
-				_crs.release_all();
-				_ccs.release_all();
-				init( _m, _n, nz > _cap ? nz : _cap );
-				if( nz == 0 ) { return SUCCESS; }
+				if( nz == 0 ) { return b200_build_device( nullptr, nullptr, nullptr, 0 ); }
 				uint32_t * dI = alloc< uint32_t >( nz );
 				uint32_t * dJ = alloc< uint32_t >( nz );
 				storage_type * dV = vt == ALPB_VOID ? nullptr : alloc< storage_type >( nz );
 				(void) alpb_memcpy_h2d( dI, I.data(), nz * 4, stream() );
 				(void) alpb_memcpy_h2d( dJ, J.data(), nz * 4, stream() );
 				if( dV ) { (void) alpb_memcpy_h2d( dV, V.data(), nz * sizeof( storage_type ), stream() ); }
+				const RC rc = b200_build_device( dI, dJ, dV, nz );
+				release( dI );
+				release( dJ );
+				release( dV );
+				return rc;
+			}
+
+			/** Both orientations from device triples (I, J, V: nz entries, V of
+			 *  this matrix's storage type or null for a pattern), in the
+			 *  reference's in-row order; the triples stay the caller's. */
+			RC b200_build_device( const uint32_t * const dI, const uint32_t * const dJ,
+				const storage_type * const dV, const size_t nz
+			) {
+				using namespace internal::b200rt;
+				const int vt = type_code< D >::value;
+				if( vt < 0 ) { return UNSUPPORTED; }
+				_crs.release_all();
+				_ccs.release_all();
+				init( _m, _n, nz > _cap ? nz : _cap );
+				if( nz == 0 ) { return SUCCESS; }
 				_crs.indices = alloc< uint32_t >( nz );
 				_ccs.indices = alloc< uint32_t >( nz );
 				if( dV ) {
@@ -429,9 +446,6 @@ namespace grb {
 						_ccs.values, stream() ), "buildMatrixUnique (CCS)" );
 				}
 				(void) alpb_stream_sync( stream() );
-				release( dI );
-				release( dJ );
-				release( dV );
 				if( rc == SUCCESS ) { _nz = nz; }
 				return rc;
 			}
