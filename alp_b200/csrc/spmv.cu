@@ -318,6 +318,171 @@ k_spmv_wmerge_hot(MergeTables mt, const int64_t *__restrict__ offsets,
 	}
 }
 
+// ---------------------------------------------- boolean lor/land (dense) --
+// u_i = u_i OR (OR_k a_ik AND x_j) on the dense fast path.  The lor monoid has
+// immutable nonzeroes (grb::has_immutable_nonzeroes, monoid.hpp:139-146): once
+// u_i is true no product changes it.  So a row whose u_i is already true is
+// skipped, as the reference's gather does (blas2.hpp:351-357), and a row stops
+// at its first true product.  OR is idempotent and order-free, so the result
+// is the full gather's, bit for bit, whatever order the products run in.
+//  * k_lor_head: LOR_W lanes per row over the row's first LOR_HEAD nonzeroes,
+//    LOR_W products per round, the group's ballot ends the row;
+//  * k_lor_tail: one warp per chunk of LOR_CHUNK nonzeroes of the rest of a
+//    long row (the plan's chunk list), skipped when the row is already true.
+// Without early exits (x mostly false, as a BFS frontier) every product is
+// gathered once, load-balanced by the chunks.
+constexpr int LOR_W = 4;
+constexpr int LOR_HEAD = 32;
+constexpr int LOR_CHUNK = 256;
+
+template <bool VALUED>
+__global__ void __launch_bounds__(256)
+k_lor_head(const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
+	const uint8_t *__restrict__ values, const uint8_t *__restrict__ x, uint8_t *__restrict__ y,
+	int64_t m) {
+	constexpr int RPW = 32 / LOR_W;
+	const int lane = threadIdx.x & (LOR_W - 1);
+	const int sub = (threadIdx.x & 31) / LOR_W;
+	const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+	const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	for (int64_t base = warp * RPW; base < m; base += nwarps * RPW) {
+		const int64_t i = base + sub;
+		int64_t b = 0, e = 0;
+		if (i < m && y[i] == 0) {
+			b = offsets[i];
+			e = offsets[i + 1];
+			if (e > b + LOR_HEAD) e = b + LOR_HEAD;
+		}
+		bool act = b < e, found = false;
+		for (int64_t k0 = b; __any_sync(WM_FULL, act); k0 += LOR_W) {
+			bool t = false;
+			const int64_t k = k0 + lane;
+			if (act && k < e) {
+				t = x[__ldcs(indices + k)] != 0;
+				if (VALUED) t = t && __ldcs(values + k) != 0;
+			}
+			const unsigned g = (__ballot_sync(WM_FULL, t) >> (sub * LOR_W)) & ((1u << LOR_W) - 1);
+			if (act && g) found = true;
+			if (k0 + LOR_W >= e || g) act = false;
+		}
+		if (found && lane == 0) y[i] = 1;
+	}
+}
+
+template <bool VALUED>
+__global__ void __launch_bounds__(256)
+k_lor_tail(const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
+	const uint8_t *__restrict__ values, const uint8_t *__restrict__ x, uint8_t *y,
+	const int64_t *__restrict__ rows, const int64_t *__restrict__ k0s, int64_t nchunks) {
+	const int lane = threadIdx.x & 31;
+	const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+	const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+	for (int64_t c = warp; c < nchunks; c += nwarps) {
+		const int64_t i = rows[c];
+		// an earlier chunk (or the head) may have set the row: read through L2
+		if (__ldcg(y + i) != 0) continue;
+		const int64_t k0 = k0s[c];
+		int64_t e = offsets[i + 1];
+		if (e > k0 + LOR_CHUNK) e = k0 + LOR_CHUNK;
+		for (int64_t kb = k0; kb < e; kb += 32) {
+			const int64_t k = kb + lane;
+			bool t = false;
+			if (k < e) {
+				t = x[__ldcs(indices + k)] != 0;
+				if (VALUED) t = t && __ldcs(values + k) != 0;
+			}
+			if (__any_sync(WM_FULL, t)) {
+				if (lane == 0) y[i] = 1;
+				break;
+			}
+		}
+	}
+}
+
+// chunk list of the lor path: per row beyond LOR_HEAD, ceil((len - HEAD) /
+// CHUNK) chunks; pass 1 counts (out == nullptr), pass 2 writes them at
+// positions taken from *count (any order: the results do not depend on it)
+__global__ void k_lor_chunks(const int64_t *__restrict__ offsets, int64_t m,
+	unsigned long long *count, int64_t *rows, int64_t *k0s) {
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m;
+		 i += int64_t(gridDim.x) * blockDim.x) {
+		const int64_t b = offsets[i] + LOR_HEAD, e = offsets[i + 1];
+		if (e <= b) continue;
+		const int64_t n = (e - b + LOR_CHUNK - 1) / LOR_CHUNK;
+		const unsigned long long at = atomicAdd(count, (unsigned long long) n);
+		if (rows)
+			for (int64_t c = 0; c < n; ++c) {
+				rows[at + c] = i;
+				k0s[at + c] = b + c * LOR_CHUNK;
+			}
+	}
+}
+
+static void lor_release(alpb_spmv_plan_s *p) {
+	cudaFree(p->lor_row);
+	cudaFree(p->lor_k0);
+	p->lor_row = nullptr;
+	p->lor_k0 = nullptr;
+	p->lor_n = -1;
+}
+
+static int lor_build(alpb_spmv_plan_s *p, cudaStream_t s) {
+	lor_release(p);
+	if (p->m == 0) {
+		p->lor_n = 0;
+		return ALPB_SUCCESS;
+	}
+	unsigned long long *cnt = nullptr, h = 0;
+	ALPB_CUDA(cudaMallocAsync(&cnt, 8, s));
+	ALPB_CUDA(cudaMemsetAsync(cnt, 0, 8, s));
+	k_lor_chunks<<<grid_for(p->m, 256, 4), 256, 0, s>>>(p->offsets, p->m, cnt, nullptr, nullptr);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cudaMemcpyAsync(&h, cnt, 8, cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	if (h > 0) {
+		if (cudaMalloc(&p->lor_row, size_t(h) * 8) != cudaSuccess ||
+			cudaMalloc(&p->lor_k0, size_t(h) * 8) != cudaSuccess) {
+			cudaGetLastError();
+			cudaFreeAsync(cnt, s);
+			cudaStreamSynchronize(s);
+			lor_release(p);
+			set_error("alpb_spmv_plan_create: out of device memory for the lor chunk list");
+			return ALPB_OUTOFMEM;
+		}
+		ALPB_CUDA(cudaMemsetAsync(cnt, 0, 8, s));
+		k_lor_chunks<<<grid_for(p->m, 256, 4), 256, 0, s>>>(p->offsets, p->m, cnt, p->lor_row,
+			p->lor_k0);
+		ALPB_LAUNCHED();
+	}
+	ALPB_CUDA(cudaFreeAsync(cnt, s));
+	p->lor_n = int64_t(h);
+	return ALPB_SUCCESS;
+}
+
+static int launch_lor(const SpmvArgs &a, const alpb_spmv_plan_s &p, cudaStream_t s) {
+	const uint8_t *x = static_cast<const uint8_t *>(a.v);
+	const uint8_t *vals = static_cast<const uint8_t *>(a.values);
+	uint8_t *y = static_cast<uint8_t *>(a.u);
+	const int64_t threads = (a.m_out + 32 / LOR_W - 1) / (32 / LOR_W) * 32;
+	if (vals)
+		k_lor_head<true><<<grid_for(threads, 256, 8), 256, 0, s>>>(a.offsets, a.indices, vals, x,
+			y, a.m_out);
+	else
+		k_lor_head<false><<<grid_for(threads, 256, 8), 256, 0, s>>>(a.offsets, a.indices, vals, x,
+			y, a.m_out);
+	ALPB_LAUNCHED();
+	if (p.lor_n > 0) {
+		if (vals)
+			k_lor_tail<true><<<grid_for(p.lor_n * 32, 256, 8), 256, 0, s>>>(a.offsets, a.indices,
+				vals, x, y, p.lor_row, p.lor_k0, p.lor_n);
+		else
+			k_lor_tail<false><<<grid_for(p.lor_n * 32, 256, 8), 256, 0, s>>>(a.offsets, a.indices,
+				vals, x, y, p.lor_row, p.lor_k0, p.lor_n);
+		ALPB_LAUNCHED();
+	}
+	return ALPB_SUCCESS;
+}
+
 // ------------------------------------------------------ vector schedules --
 // Rows are handed out per warp (32/W rows at a time) so that every lane of a
 // warp runs the same number of outer iterations and the width-W shuffles
@@ -578,6 +743,9 @@ int run_spmv(const SpmvArgs &a, const alpb_spmv_plan_s *p, int force_sched, cuda
 	}
 	const bool fast = a.dense_all && !a.masked && !a.input_masked &&
 		!(a.descr & (ALPB_DESC_ADD_IDENTITY | ALPB_DESC_USE_INDEX));
+	if constexpr (std::is_same<R, RingLorLandBool>::value) {
+		if (fast && !force_sched && p && p->lor_n >= 0) return launch_lor(a, *p, s);
+	}
 	int sched = force_sched ? force_sched : (p ? p->sched : ALPB_SCHED_VECTOR);
 	int W = p ? p->vw : default_width(a.m_out ? double(a.nnz) / double(a.m_out) : 1.0);
 	if (fast && sched == ALPB_SCHED_MERGE_PATH && p && p->tile_row)
@@ -686,8 +854,15 @@ int alpb_spmv_plan_create(alpb_spmv_plan *plan, int64_t m, int64_t nnz, const in
 	int sched, int vector_width, void *stream) {
 	ALPB_CHECK(plan != nullptr, ALPB_ILLEGAL, "alpb_spmv_plan_create: null plan");
 	*plan = nullptr;
-	return plan_create_tiles(plan, m, nnz, offsets, sched, vector_width, WM_TILE,
-		as_stream(stream));
+	cudaStream_t s = as_stream(stream);
+	int rc = plan_create_tiles(plan, m, nnz, offsets, sched, vector_width, WM_TILE, s);
+	if (rc != ALPB_SUCCESS) return rc;
+	rc = lor_build(*plan, s);
+	if (rc != ALPB_SUCCESS) {
+		alpb_spmv_plan_destroy(*plan);
+		*plan = nullptr;
+	}
+	return rc;
 }
 
 } // extern "C"
@@ -741,6 +916,8 @@ int alpb_spmv_plan_destroy(alpb_spmv_plan p) {
 	cudaFree(p->hot_idx);
 	cudaFree(p->hot_cols);
 	cudaFree(p->hot_x);
+	cudaFree(p->lor_row);
+	cudaFree(p->lor_k0);
 	delete p;
 	return ALPB_SUCCESS;
 }

@@ -41,6 +41,13 @@ struct alpb_spmv_plan_s {
 	uint32_t *hot_idx = nullptr;        // nnz
 	uint32_t *hot_cols = nullptr;       // hot_k
 	uint64_t *hot_x = nullptr;          // hot_k values (8 bytes hold any ring's type)
+	// Boolean lor/land path: the nonzeroes of every row beyond its first
+	// LOR_HEAD, cut in chunks of LOR_CHUNK; chunk c covers
+	// [lor_k0[c], min(lor_k0[c] + LOR_CHUNK, offsets[lor_row[c] + 1])).
+	// lor_n < 0: not built (the plan was made for a fused solver).
+	int64_t lor_n = -1;
+	int64_t *lor_row = nullptr;
+	int64_t *lor_k0 = nullptr;
 };
 
 namespace alpb {

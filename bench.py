@@ -329,6 +329,55 @@ def timed(fn, reps: int, stream):
     return e0.elapsed_time(e1) / reps
 
 
+def semiring_sweeps(stream, A) -> dict:
+    """The scale-22 sweep in the two other semirings: boolean lor/land with a
+    50% dense output mask (x 50% and 1% true), and int32 min-plus."""
+    import torch
+    from alp_b200 import _abi as abi
+    from alp_b200 import device as dev
+    out = {}
+    # boolean lor/land, value mask with 50% true, dense: the reference reads a
+    # non-inverted mask on its CRS gather by structure, so every row runs
+    Ab = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices, None, abi.VOID)
+    xb = dev.gen_values(A.n, abi.BOOL, seed=11, p=0.5)
+    mk = dev.gen_values(A.m, abi.BOOL, seed=12, p=0.5)
+    ub = torch.zeros(A.m, dtype=torch.uint8, device="cuda")
+    pb = dev.Plan(Ab, sched=abi.SCHED_MERGE_PATH)
+
+    def lor_step(x):
+        # u starts false every step: rows already true would be skipped (the
+        # reference's immutable-nonzero shortcut), so a kept u would time less work
+        ub.zero_()
+        dev.mxv(abi.RING_LOR_LAND_BOOL, Ab, ub, x, u_mask=mk, u_mask_count=A.m, plan=pb)
+
+    nb = A.nnz * 4 + (A.m + 1) * 8 + A.m + A.n + 2 * A.m
+    ms = timed(lambda: lor_step(xb), 20, stream)
+    out["mxv_lor_land_masked50"] = {
+        "ms": round(ms, 4), "GB/s": round(nb / ms / 1e6, 1), "bytes": nb,
+        "matrix": "pattern (void)", "x": "50% true",
+        "note": "early exit at a row's first true product; GB/s over the full sweep's "
+                "bytes; includes zeroing u each step"}
+    # the same sweep from a 1%-true x (a BFS frontier): almost no early exits
+    xf = dev.gen_values(A.n, abi.BOOL, seed=14, p=0.01)
+    ms = timed(lambda: lor_step(xf), 20, stream)
+    out["mxv_lor_land_frontier1"] = {
+        "ms": round(ms, 4), "GB/s": round(nb / ms / 1e6, 1), "bytes": nb,
+        "matrix": "pattern (void)", "x": "1% true", "note": "includes zeroing u each step"}
+    del xf
+    # int32 min-plus, weights U{1..100}
+    Ai = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices,
+                 torch.empty(A.nnz, dtype=torch.int32, device="cuda"), abi.INT32)
+    abi.call("alpb_gen_edge_values", dev.ptr(Ai.values), abi.INT32, dev.ptr(A.offsets),
+             dev.ptr(A.indices), A.m, A.nnz, SEED + 1, 1, 100, dev.stream_ptr())
+    xi = dev.gen_values(A.n, abi.INT32, seed=13, lo=0, hi=1000)
+    ui = torch.full((A.m,), 2**31 - 1, dtype=torch.int32, device="cuda")
+    ms = timed(lambda: dev.mxv(abi.RING_MIN_PLUS_I32, Ai, ui, xi, plan=pb), 20, stream)
+    nb = algorithmic_bytes(A.m, A.n, A.nnz, 4, 4)
+    out["mxv_min_plus_i32"] = {"ms": round(ms, 4), "GB/s": round(nb / ms / 1e6, 1), "bytes": nb}
+    del Ai, xi, ui
+    return out
+
+
 def extra_workloads(args, A, plan, cpu: bool) -> dict:
     """Secondary workloads of the same sweep, timed the same way (not part of
     `value`): boolean lor/land with a 50% dense output mask, int32 min-plus,
@@ -341,31 +390,8 @@ def extra_workloads(args, A, plan, cpu: bool) -> dict:
     from alp_b200 import _abi as abi
     from alp_b200 import device as dev
     stream = torch.cuda.current_stream()
-    out = {}
     later = []     # host reference runs, after the device timings
-    # boolean lor/land, value mask with 50% true, dense: the reference reads a
-    # non-inverted mask on its CRS gather by structure, so every row runs
-    Ab = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices, None, abi.VOID)
-    xb = dev.gen_values(A.n, abi.BOOL, seed=11, p=0.5)
-    mk = dev.gen_values(A.m, abi.BOOL, seed=12, p=0.5)
-    ub = torch.zeros(A.m, dtype=torch.uint8, device="cuda")
-    pb = dev.Plan(Ab, sched=abi.SCHED_MERGE_PATH)
-    ms = timed(lambda: dev.mxv(abi.RING_LOR_LAND_BOOL, Ab, ub, xb, u_mask=mk,
-                               u_mask_count=A.m, plan=pb), 20, stream)
-    nb = A.nnz * 4 + (A.m + 1) * 8 + A.m + A.n + 2 * A.m
-    out["mxv_lor_land_masked50"] = {"ms": round(ms, 4), "GB/s": round(nb / ms / 1e6, 1),
-                                    "bytes": nb, "matrix": "pattern (void)"}
-    # int32 min-plus, weights U{1..100}
-    Ai = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices,
-                 torch.empty(A.nnz, dtype=torch.int32, device="cuda"), abi.INT32)
-    abi.call("alpb_gen_edge_values", dev.ptr(Ai.values), abi.INT32, dev.ptr(A.offsets),
-             dev.ptr(A.indices), A.m, A.nnz, SEED + 1, 1, 100, dev.stream_ptr())
-    xi = dev.gen_values(A.n, abi.INT32, seed=13, lo=0, hi=1000)
-    ui = torch.full((A.m,), 2**31 - 1, dtype=torch.int32, device="cuda")
-    ms = timed(lambda: dev.mxv(abi.RING_MIN_PLUS_I32, Ai, ui, xi, plan=pb), 20, stream)
-    nb = algorithmic_bytes(A.m, A.n, A.nnz, 4, 4)
-    out["mxv_min_plus_i32"] = {"ms": round(ms, 4), "GB/s": round(nb / ms / 1e6, 1), "bytes": nb}
-    del Ai, xi, ui
+    out = semiring_sweeps(stream, A)
     out["pagerank_rmat22"] = pagerank_workload(stream, A, cpu, later)
     out["cg_27pt_32"] = cg_workload(stream, 32, cpu, later)
     out["batched_cg"] = batched_cg_workload(stream, cpu=cpu, later=later)
@@ -914,7 +940,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale (22 is the benchmark; smaller for profiling captures)")
-    ap.add_argument("--only", choices=["batched_cg", "hpcg", "adjoint_cg", "ppr", "pagerank", "cg"],
+    ap.add_argument("--only", choices=["batched_cg", "hpcg", "adjoint_cg", "ppr", "pagerank", "cg",
+                                       "sweeps"],
                     help="run one secondary workload alone and print its line (profiling)")
     ap.add_argument("--hpcg-side", type=int, default=256)
     ap.add_argument("--hpcg-levels", type=int, default=3)
@@ -945,7 +972,9 @@ def main():
                "ppr": lambda: ppr_workload(stream, args.ppr_scale, args.ppr_seeds),
                "pagerank": lambda: pagerank_workload(
                    stream, dev.rmat(args.scale, EDGE_FACTOR, seed=SEED, vtype=abi.FP64)),
-               "cg": lambda: cg_workload(stream, args.cg_side)}[args.only]
+               "cg": lambda: cg_workload(stream, args.cg_side),
+               "sweeps": lambda: semiring_sweeps(
+                   stream, dev.rmat(args.scale, EDGE_FACTOR, seed=SEED, vtype=abi.FP64))}[args.only]
         if rank == 0:
             print(json.dumps({"workload": args.only, **run()}), flush=True)
         return

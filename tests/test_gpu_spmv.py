@@ -226,6 +226,49 @@ def test_mxv_golden_reference(cuda, oracle, name):
     assert_ring_equal(ring, _np(tu)[ref_a], c["u_out"][ref_a], name)
 
 
+@pytest.mark.parametrize("xcase", ["half", "sparse", "none", "one_late"])
+@pytest.mark.parametrize("valued", [False, True], ids=["void", "bool"])
+@pytest.mark.parametrize("form", [2, 1], ids=["mxv", "vxm"])
+def test_lor_land_early_exit_path(cuda, oracle, xcase, valued, form):
+    """The lor/land dense path (row heads of 32 nonzeroes, chunks of 256 for
+    the rest of long rows, early exit at the first true product, rows already
+    true skipped) is bit-exact against the oracle's full gather: x half true,
+    1% true (a BFS frontier), all false (no early exit anywhere), and one true
+    entry at the column that only the last nonzero of the longest row reads;
+    pattern and bool-valued matrices (30% false values); u 20% true."""
+    import torch
+    dev = _dev()
+    A = dev.rmat(13, vtype=BOOL, seed=31)
+    if valued:
+        A.values.copy_(dev.gen_values(A.nnz, BOOL, seed=32, p=0.7))
+    else:
+        A = dev.CRS(A.m, A.n, A.nnz, A.offsets, A.indices, None, VOID)
+    S = A if form == 2 else dev.transpose(A)
+    o, i, v = S.to_host()
+    if xcase == "half":
+        x = dev.gen_values(S.n, BOOL, seed=4, p=0.5)
+    elif xcase == "sparse":
+        x = dev.gen_values(S.n, BOOL, seed=4, p=0.01)
+    else:
+        x = torch.zeros(S.n, dtype=torch.uint8, device="cuda")
+        if xcase == "one_late":
+            r = int(np.argmax(np.diff(o)))
+            assert o[r + 1] - o[r] > 32 + 256, "the longest row must reach a tail chunk"
+            x[int(i[o[r + 1] - 1])] = 1
+    u0 = dev.gen_values(S.m, BOOL, seed=6, p=0.2)
+    u = u0.clone()
+    plan = dev.Plan(S, sched=1)
+    dev.mxv(1, S, u, x, form=form, plan=plan)
+    torch.cuda.synchronize()
+    want = _np(u0).copy()
+    rc, _ = oracle.mxv(1, 0, form, S.m, S.n, o, i[:S.nnz], None if v is None else v[:S.nnz],
+                       BOOL if valued else VOID, want, v=_np(x))
+    assert rc == 0
+    np.testing.assert_array_equal(_np(u), want)
+    if xcase == "one_late":
+        assert int(_np(u)[r]) == 1
+
+
 def test_mxv_error_codes(cuda):
     import torch
     from alp_b200 import _abi as abi
