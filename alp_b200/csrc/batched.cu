@@ -759,6 +759,483 @@ k_batched_cg(BcgArgs a) {
 	}
 }
 
+
+// ------------------------------------ sliced batched CG, two barriers --
+// Systems whose rows hold at most 32 nonzeroes, on the sliced storage (slices
+// of 32 rows of one instance, entry q of the slice's rows contiguous).  One
+// CG iteration of every active instance is
+//     phase A (products) | grid barrier | phase B (updates) | grid barrier |
+//     scalar step (no barrier of its own)
+// Work split: the active instances' slices, in instance order, are cut in ONE
+// contiguous run per warp (warp g of nw takes items [ntot g / nw,
+// ntot (g+1) / nw)), so a warp streams consecutive slices and rows.  A warp
+// leaves one partial per instance its run touches, in slot slot0[j] + g -
+// (first warp of instance j); an instance's sum is the sum of its slots in
+// slot order, formed by whoever needs it -- the same slots in the same order,
+// hence the same bits everywhere.  So the phase-B warps form alpha themselves,
+// and after the second barrier every block forms every active instance's r.r,
+// convergence test, gamma and sigma in its own shared memory (identical in
+// all blocks) and rebuilds its active list; block 0 publishes the results.
+// The search direction travels with the residual as a 16-byte pair (r_i,
+// p_i), double-buffered by iteration: a product gathers ONE pair per nonzero
+// and forms p_j = r_j + gamma p_j(old); phase B forms p_i the same way (same
+// operands, same bits), updates x and r and writes the next pair.  Per row
+// the arithmetic is that of k_batched_cg and of the single-system solver;
+// only the grouping of the instance dot products differs.
+#ifndef ALPB_BCS_WARPS
+#define ALPB_BCS_WARPS 8
+#endif
+#ifndef ALPB_BCS_MINB
+#define ALPB_BCS_MINB 3
+#endif
+#ifndef ALPB_BCS_WMAX
+#define ALPB_BCS_WMAX 6
+#endif
+#ifndef ALPB_BCS_RB
+#define ALPB_BCS_RB 2
+#endif
+#ifndef ALPB_BCS_SU
+#define ALPB_BCS_SU 4
+#endif
+constexpr int BCS_WARPS = ALPB_BCS_WARPS;  // warps per block (ALPB_BCS_MINB blocks per SM)
+constexpr int BCS_WMAX = ALPB_BCS_WMAX;    // widest slice of the unrolled product path
+constexpr int BCS_RB = ALPB_BCS_RB;        // rows per lane whose loads phase B issues together
+constexpr int BCS_SU = ALPB_BCS_SU;        // instances whose slot sums a warp forms together
+// Slices per warp at least, when fewer than all warps suffice: in the tail,
+// when few instances are left, their sums then have fewer slots to add.
+constexpr int32_t BCS_MINRUN = 8;
+
+struct BcsArgs {
+	const int64_t *seg_rows;       // [nseg+1]
+	const int64_t *seg_slice;      // [nseg+1]
+	const int64_t *sl_off;         // [nslices+1]
+	const uint32_t *sl_idx;
+	const double *sl_val;
+	const uint8_t *sl_len;         // [n]
+	const double *b;
+	double *x;
+	double2 *pair[2];              // (r_i, p_i) of the current / next iteration
+	double *temp;                  // A p
+	double *slot_a, *slot_b;       // per-(warp, instance) partials
+	BcgInst *inst;
+	int64_t nseg, max_iter;
+	double tol;
+	GridSync *gs;
+};
+
+struct BcsShared {
+	int32_t n;                             // active instances
+	int32_t ntot;                          // their slices
+	int64_t nwe;                           // warps with a run (at most ntot / BCS_MINRUN)
+	int32_t seg[BCG_LIST_MAX];
+	int32_t off[BCG_LIST_MAX + 1];         // slice prefix of the active instances
+	int32_t slot0[BCG_LIST_MAX + 1];       // first partial slot of each
+	int32_t nsl[BCG_LIST_MAX];             // slices of every instance
+	double sigma[BCG_LIST_MAX], gamma[BCG_LIST_MAX], tol_abs[BCG_LIST_MAX];
+	uint8_t done[BCG_LIST_MAX];
+	int32_t scan[32];
+};
+
+// first item of warp g's run
+__device__ __forceinline__ int64_t bcs_kb(int64_t ntot, int64_t g, int64_t nw) {
+	return ntot * g / nw;
+}
+// warp whose run holds item k: the largest g with bcs_kb(g) <= k
+__device__ __forceinline__ int64_t bcs_warp_of(int64_t ntot, int64_t k, int64_t nw) {
+	return ((k + 1) * nw - 1) / ntot;
+}
+
+// block-wide exclusive scan of one int per thread (thread order); returns
+// the thread's prefix, *total the sum.  buf: one int per warp.
+__device__ __forceinline__ int32_t bcs_scan(int32_t v, int32_t *buf, int32_t *total) {
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	const int nwarps = int(blockDim.x + 31) >> 5;
+	int32_t x = v;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+		if (lane >= o) x += y;
+	}
+	if (lane == 31) buf[wid] = x;
+	__syncthreads();
+	if (wid == 0) {
+		int32_t t = lane < nwarps ? buf[lane] : 0;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int32_t y = __shfl_up_sync(0xffffffffu, t, o);
+			if (lane >= o) t += y;
+		}
+		if (lane < nwarps) buf[lane] = t;
+	}
+	__syncthreads();
+	const int32_t before = wid > 0 ? buf[wid - 1] : 0;
+	*total = buf[nwarps - 1];
+	__syncthreads();  // buf is reused by the next scan
+	return before + x - v;
+}
+
+// Active list of the instances not done, their slice prefix and their slot
+// layout for nw warps; identical in every block.
+__device__ __noinline__ void bcs_build_list(BcsShared &S, int64_t nseg, int64_t nw) {
+	const int tid = threadIdx.x, nth = blockDim.x;
+	const int per = int((nseg + nth - 1) / nth);
+	const int s0 = tid * per, s1 = s0 + per < int(nseg) ? s0 + per : int(nseg);
+	int32_t ci = 0, ct = 0;
+	for (int s = s0; s < s1; ++s)
+		if (!S.done[s]) {
+			++ci;
+			ct += S.nsl[s];
+		}
+	int32_t ni, ntot;
+	int32_t pi = bcs_scan(ci, S.scan, &ni);
+	int32_t pt = bcs_scan(ct, S.scan, &ntot);
+	for (int s = s0; s < s1; ++s)
+		if (!S.done[s]) {
+			S.seg[pi] = s;
+			S.off[pi] = pt;
+			++pi;
+			pt += S.nsl[s];
+		}
+	if (tid == 0) {
+		S.n = ni;
+		S.ntot = ntot;
+		S.off[ni] = ntot;
+		const int64_t want = (int64_t(ntot) + BCS_MINRUN - 1) / BCS_MINRUN;
+		S.nwe = nw < want ? nw : want;
+	}
+	__syncthreads();
+	// slots: warps whose runs touch instance j (every active instance has at
+	// least one slice, so at least one warp; with nwe warps every run holds at
+	// least one item, so each warp from the instance's first to its last
+	// writes its slot)
+	nw = S.nwe;
+	const int pj = (ni + nth - 1) / nth;
+	const int j0 = tid * pj, j1 = j0 + pj < ni ? j0 + pj : ni;
+	int32_t cs = 0;
+	for (int j = j0; j < j1; ++j)
+		cs += int32_t(bcs_warp_of(ntot, S.off[j + 1] - 1, nw) - bcs_warp_of(ntot, S.off[j], nw) + 1);
+	int32_t nslots;
+	int32_t ps = bcs_scan(cs, S.scan, &nslots);
+	for (int j = j0; j < j1; ++j) {
+		S.slot0[j] = ps;
+		ps += int32_t(bcs_warp_of(ntot, S.off[j + 1] - 1, nw) - bcs_warp_of(ntot, S.off[j], nw) + 1);
+	}
+	if (tid == 0) S.slot0[ni] = nslots;
+	__syncthreads();
+}
+
+// list entry holding item k (off[j] <= k < off[j+1])
+__device__ __forceinline__ int bcs_find(const BcsShared &S, int64_t k) {
+	int lo = 0, hi = S.n - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (S.off[mid] <= k) lo = mid; else hi = mid - 1;
+	}
+	return lo;
+}
+
+// sum of slots [a, b) in a fixed order, the same in every lane
+__device__ __forceinline__ double bcs_slot_sum(const double *slots, int32_t a, int32_t b,
+	int lane) {
+	double v = 0.0;
+	int32_t k = a + lane;
+	for (; k + 7 * 32 < b; k += 8 * 32) {   // eight loads in flight, added in order
+		double t[8];
+#pragma unroll
+		for (int u = 0; u < 8; ++u) t[u] = __ldcg(slots + k + 32 * u);
+#pragma unroll
+		for (int u = 0; u < 8; ++u) v += t[u];
+	}
+	for (; k < b; k += 32) v += __ldcg(slots + k);
+	return warp_sum(v);
+}
+
+// The same sums for list entries j0 .. j0 + BCS_SU - 1 (those below S.n),
+// their first loads issued together; out[u] in every lane.
+__device__ __forceinline__ void bcs_slot_sums(const double *slots, const BcsShared &S, int j0,
+	int lane, double *out) {
+	double v[BCS_SU];
+#pragma unroll
+	for (int u = 0; u < BCS_SU; ++u) {
+		v[u] = 0.0;
+		if (j0 + u < S.n) {
+			const int32_t a = S.slot0[j0 + u], b = S.slot0[j0 + u + 1];
+			if (a + lane < b) v[u] = __ldcg(slots + a + lane);
+		}
+	}
+#pragma unroll
+	for (int u = 0; u < BCS_SU; ++u) {
+		if (j0 + u < S.n) {
+			const int32_t a = S.slot0[j0 + u], b = S.slot0[j0 + u + 1];
+			int32_t k = a + lane + 32;
+			for (; k + 7 * 32 < b; k += 8 * 32) {
+				double t[8];
+#pragma unroll
+				for (int q = 0; q < 8; ++q) t[q] = __ldcg(slots + k + 32 * q);
+#pragma unroll
+				for (int q = 0; q < 8; ++q) v[u] += t[q];
+			}
+			for (; k < b; k += 32) v[u] += __ldcg(slots + k);
+		}
+		out[u] = warp_sum(v[u]);
+	}
+}
+
+// Products of ns consecutive slices of one instance, the first at slice t0
+// and row r0 (slice c holds rows r0 + 32c .. , up to the instance end rend):
+// lane l of slice c computes row i = r0 + 32c + l as the sum, in storage order,
+// of the rounded products (as the restated CG).  pre(i, valid) loads what the
+// row epilogue needs before the gathers are issued; row(i, acc, pre) finishes
+// the row.  The slices' entry offsets are fetched 32 slices at a time.
+template <class XF, class PreF, class RowF>
+__device__ __forceinline__ void bcs_products(const BcsArgs &a, int64_t t0, int64_t ns,
+	int64_t r0, int64_t rend, int lane, const XF &xf, const PreF &pre, RowF &&row) {
+	for (int64_t cb = 0; cb < ns; cb += 32) {
+		const int cnt = ns - cb < 32 ? int(ns - cb) : 32;
+		const int64_t my_off = lane < cnt ? __ldg(a.sl_off + t0 + cb + lane) : 0;
+		const int64_t end_off = __ldg(a.sl_off + t0 + cb + cnt);
+		// the column indices and row length of slice c (narrow slices only),
+		// fetched one slice ahead so that they arrive while the slice before
+		// gathers
+		const auto fetch = [&](int c, uint32_t *j, int &len) {
+			const int64_t e0 = __shfl_sync(0xffffffffu, my_off, c);
+			const int64_t e1 = c + 1 < cnt ? __shfl_sync(0xffffffffu, my_off, c + 1) : end_off;
+			const int w = int((e1 - e0) >> 5);
+			const int64_t i = r0 + 32 * (cb + c) + lane;
+			len = i < rend ? int(__ldg(a.sl_len + i)) : 0;
+#pragma unroll
+			for (int q = 0; q < BCS_WMAX; ++q)
+				j[q] = q < w && w <= BCS_WMAX ? __ldcs(a.sl_idx + e0 + 32 * q + lane) : 0u;
+		};
+		uint32_t jn[BCS_WMAX];
+		int lenn;
+		fetch(0, jn, lenn);
+		for (int c = 0; c < cnt; ++c) {
+			uint32_t j[BCS_WMAX];
+#pragma unroll
+			for (int q = 0; q < BCS_WMAX; ++q) j[q] = jn[q];
+			const int len = lenn;
+			const int64_t e0 = __shfl_sync(0xffffffffu, my_off, c);
+			const int64_t e1 = c + 1 < cnt ? __shfl_sync(0xffffffffu, my_off, c + 1) : end_off;
+			const int w = int((e1 - e0) >> 5);
+			const int64_t i = r0 + 32 * (cb + c) + lane;
+			const bool valid = i < rend;
+			if (c + 1 < cnt) fetch(c + 1, jn, lenn);
+			double acc = 0.0;
+			if (w <= BCS_WMAX) {
+				double v[BCS_WMAX], g[BCS_WMAX];
+#pragma unroll
+				for (int q = 0; q < BCS_WMAX; ++q)
+					v[q] = q < w ? __ldcs(a.sl_val + e0 + 32 * q + lane) : 0.0;
+				const auto own = pre(i, valid);
+#pragma unroll
+				for (int q = 0; q < BCS_WMAX; ++q) g[q] = q < len ? xf(j[q]) : 0.0;
+#pragma unroll
+				for (int q = 0; q < BCS_WMAX; ++q)
+					if (q < len) acc = __dadd_rn(acc, __dmul_rn(v[q], g[q]));
+				if (valid) row(i, acc, own);
+			} else {
+				const auto own = pre(i, valid);
+				for (int q0 = 0; q0 < w; q0 += 4) {
+					uint32_t jj[4];
+					double v[4], g[4];
+#pragma unroll
+					for (int u = 0; u < 4; ++u) {
+						const int64_t e = e0 + 32 * int64_t(q0 + u) + lane;
+						jj[u] = q0 + u < w ? __ldcs(a.sl_idx + e) : 0u;
+						v[u] = q0 + u < w ? __ldcs(a.sl_val + e) : 0.0;
+					}
+#pragma unroll
+					for (int u = 0; u < 4; ++u) g[u] = q0 + u < len ? xf(jj[u]) : 0.0;
+#pragma unroll
+					for (int u = 0; u < 4; ++u)
+						if (q0 + u < len) acc = __dadd_rn(acc, __dmul_rn(v[u], g[u]));
+				}
+				if (valid) row(i, acc, own);
+			}
+		}
+	}
+}
+
+// The warp's run, instance by instance: fn(j, s, k, e) for its items [k, e)
+// of list entry j (instance s).  Warps from nwe on have none.
+template <class F>
+__device__ __forceinline__ void bcs_walk(const BcsShared &S, int64_t g, F &&fn) {
+	const int64_t ntot = S.ntot, nw = S.nwe;
+	if (g >= nw) return;
+	int64_t k = bcs_kb(ntot, g, nw);
+	const int64_t kend = bcs_kb(ntot, g + 1, nw);
+	if (k >= kend) return;
+	int j = bcs_find(S, k);
+	while (k < kend) {
+		const int64_t e = kend < S.off[j + 1] ? kend : S.off[j + 1];
+		fn(j, S.seg[j], k, e);
+		k = e;
+		++j;
+	}
+}
+
+// Convergence test of instance s after an iteration with residual r.r = rr
+// (conjugate_gradient.hpp:437), then gamma and sigma for the next one; block
+// 0 publishes the instance's state.
+__device__ __forceinline__ void bcs_instance_step(const BcsArgs &a, BcsShared &S, int s,
+	double rr, int64_t iter) {
+	const bool fin = sqrt(rr) < S.tol_abs[s] || iter >= a.max_iter;
+	if (blockIdx.x == 0) {
+		BcgInst *in = a.inst + s;
+		in->rr = rr;
+		in->iterations = iter;
+		if (fin) {
+			in->converged = sqrt(rr) < S.tol_abs[s] ? 1 : 0;
+			in->done = 1;
+		}
+	}
+	if (fin) {
+		S.done[s] = 1;
+	} else {
+		S.gamma[s] = rr / S.sigma[s];
+		S.sigma[s] = rr;
+	}
+}
+
+__global__ void __launch_bounds__(32 * BCS_WARPS, ALPB_BCS_MINB) k_bcg_sliced(BcsArgs a) {
+	__shared__ BcsShared S;
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int64_t g = int64_t(blockIdx.x) * BCS_WARPS + w;
+	const int64_t nw = int64_t(gridDim.x) * BCS_WARPS;
+	for (int s = threadIdx.x; s < int(a.nseg); s += blockDim.x) {
+		S.nsl[s] = int32_t(a.seg_slice[s + 1] - a.seg_slice[s]);
+		S.done[s] = 0;
+		S.gamma[s] = 0.0;
+		if (blockIdx.x == 0) {
+			BcgInst *in = a.inst + s;
+			in->iterations = 0;
+			in->done = 0;
+			in->converged = 0;
+		}
+	}
+	__syncthreads();
+	bcs_build_list(S, a.nseg, nw);
+
+	// prelude: r = b - A x, pairs (r, 0); partials r.r -> slot_a, b.b -> slot_b
+	bcs_walk(S, g, [&](int j, int s, int64_t k, int64_t e) {
+		const int64_t q0 = k - S.off[j];
+		const int64_t R0 = __ldg(a.seg_rows + s), R1 = __ldg(a.seg_rows + s + 1);
+		double rr = 0.0, bb = 0.0;
+		bcs_products(a, __ldg(a.seg_slice + s) + q0, e - k, R0 + 32 * q0, R1, lane,
+			[&](uint32_t c) { return __ldcg(a.x + c); },
+			[&](int64_t i, bool valid) { return valid ? a.b[i] : 0.0; },
+			[&](int64_t i, double v, double bi) {
+				const double ri = (0.0 + bi) - v;
+				a.pair[0][i] = make_double2(ri, 0.0);
+				rr += ri * ri;
+				bb += bi * bi;
+			});
+		const double s1 = warp_sum(rr), s2 = warp_sum(bb);
+		if (lane == 0) {
+			const int32_t sl = S.slot0[j] + int32_t(g - bcs_warp_of(S.ntot, S.off[j], S.nwe));
+			a.slot_a[sl] = s1;
+			a.slot_b[sl] = s2;
+		}
+	});
+	if (!grid_sync(a.gs)) return;
+	for (int j0 = w * BCS_SU; j0 < S.n; j0 += BCS_WARPS * BCS_SU) {
+		double sg[BCS_SU], bn[BCS_SU];
+		bcs_slot_sums(a.slot_a, S, j0, lane, sg);
+		bcs_slot_sums(a.slot_b, S, j0, lane, bn);
+		if (lane == 0)
+			for (int u = 0; u < BCS_SU && j0 + u < S.n; ++u) {
+				const int s = S.seg[j0 + u];
+				S.sigma[s] = sg[u];
+				S.tol_abs[s] = a.tol * sqrt(bn[u]);
+			}
+	}
+	__syncthreads();
+
+	int cur = 0;
+	for (int64_t iter = 1;; ++iter) {
+		const double2 *pc = a.pair[cur];
+		double2 *pn = a.pair[cur ^ 1];
+		// phase A: temp = A p, partials p.(A p) -> slot_a
+		bcs_walk(S, g, [&](int j, int s, int64_t k, int64_t e) {
+			const int64_t q0 = k - S.off[j];
+			const int64_t R0 = __ldg(a.seg_rows + s), R1 = __ldg(a.seg_rows + s + 1);
+			const double gamma = S.gamma[s];
+			double acc = 0.0;
+			bcs_products(a, __ldg(a.seg_slice + s) + q0, e - k, R0 + 32 * q0, R1, lane,
+				[&](uint32_t c) {
+					const double2 p = __ldcg(pc + c);
+					return p.x + gamma * p.y;
+				},
+				[&](int64_t i, bool valid) { return valid ? __ldcg(pc + i) : make_double2(0.0, 0.0); },
+				[&](int64_t i, double v, double2 p) {
+					a.temp[i] = v;
+					const double un = p.x + gamma * p.y;
+					acc += v * un;
+				});
+			const double part = warp_sum(acc);
+			if (lane == 0) a.slot_a[S.slot0[j] + int32_t(g - bcs_warp_of(S.ntot, S.off[j], S.nwe))] = part;
+		});
+		if (!grid_sync(a.gs)) return;
+		// phase B: alpha from the instance's slots; x += alpha p, r -= alpha A p,
+		// the next pairs; partials r.r -> slot_b
+		bcs_walk(S, g, [&](int j, int s, int64_t k, int64_t e) {
+			const double alpha = S.sigma[s] / bcs_slot_sum(a.slot_a, S.slot0[j], S.slot0[j + 1], lane);
+			const double gamma = S.gamma[s];
+			const int64_t q0 = k - S.off[j];
+			const int64_t R0 = __ldg(a.seg_rows + s), R1 = __ldg(a.seg_rows + s + 1);
+			const int64_t i0 = R0 + 32 * q0;
+			int64_t i1 = R0 + 32 * (e - S.off[j]);
+			if (i1 > R1) i1 = R1;
+			double part = 0.0;
+			for (int64_t ib = i0; ib < i1; ib += 32 * BCS_RB) {
+				double2 p[BCS_RB];
+				double xv[BCS_RB], tv[BCS_RB];
+#pragma unroll
+				for (int u = 0; u < BCS_RB; ++u) {
+					const int64_t i = ib + lane + 32 * u;
+					if (i < i1) {
+						p[u] = __ldcg(pc + i);
+						xv[u] = __ldcg(a.x + i);
+						tv[u] = __ldcg(a.temp + i);
+					}
+				}
+#pragma unroll
+				for (int u = 0; u < BCS_RB; ++u) {
+					const int64_t i = ib + lane + 32 * u;
+					if (i < i1) {
+						const double un = p[u].x + gamma * p[u].y;
+						a.x[i] = xv[u] + alpha * un;
+						const double ri = p[u].x - alpha * tv[u];
+						pn[i] = make_double2(ri, un);
+						part += ri * ri;
+					}
+				}
+			}
+			part = warp_sum(part);
+			if (lane == 0) a.slot_b[S.slot0[j] + int32_t(g - bcs_warp_of(S.ntot, S.off[j], S.nwe))] = part;
+		});
+		if (!grid_sync(a.gs)) return;
+		// scalar step, in every block: r.r, convergence, gamma, sigma; a warp
+		// takes BCS_SU instances at a time, their slot loads issued together
+		for (int j0 = w * BCS_SU; j0 < S.n; j0 += BCS_WARPS * BCS_SU) {
+			double rr[BCS_SU];
+			bcs_slot_sums(a.slot_b, S, j0, lane, rr);
+			if (lane < BCS_SU && j0 + lane < S.n) {
+				double v = rr[0];
+#pragma unroll
+				for (int u = 1; u < BCS_SU; ++u)
+					if (lane == u) v = rr[u];
+				bcs_instance_step(a, S, S.seg[j0 + lane], v, iter);
+			}
+		}
+		__syncthreads();
+		bcs_build_list(S, a.nseg, nw);
+		if (S.n == 0) break;
+		cur ^= 1;
+	}
+}
+
 } // namespace alpb
 
 using namespace alpb;
@@ -845,6 +1322,7 @@ struct alpb_batched_cg_s {
 	uint32_t *sl_idx = nullptr;
 	double *sl_val = nullptr;
 	uint8_t *sl_len = nullptr;
+	int64_t nslots = 0;         // partial slots of each kind (sliced solver)
 	cudaGraphExec_t graph = nullptr;
 	const double *g_b = nullptr;
 	double *g_x = nullptr;
@@ -954,7 +1432,27 @@ static int bcg_launch(alpb_batched_cg_s *h, const double *b, double *x, int64_t 
 	cfg.attrs = attr;
 	cfg.numAttrs = 1;
 	if (h->rows) {
-		ALPB_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg<true, true>, a));
+		BcsArgs c;
+		c.seg_rows = h->st.seg_rows;
+		c.seg_slice = h->seg_slice;
+		c.sl_off = h->sl_off;
+		c.sl_idx = h->sl_idx;
+		c.sl_val = h->sl_val;
+		c.sl_len = h->sl_len;
+		c.b = b;
+		c.x = x;
+		c.pair[0] = reinterpret_cast<double2 *>(h->work);
+		c.pair[1] = reinterpret_cast<double2 *>(h->work + 2 * h->n);
+		c.temp = h->work + 4 * h->n;
+		c.slot_a = h->scratch;
+		c.slot_b = h->scratch + h->nslots;
+		c.inst = h->inst;
+		c.nseg = h->nseg;
+		c.max_iter = max_iter;
+		c.tol = tol;
+		c.gs = h->gs;
+		cfg.blockDim = dim3(32 * BCS_WARPS);
+		ALPB_CUDA(cudaLaunchKernelEx(&cfg, k_bcg_sliced, c));
 	} else if (h->list) {
 		ALPB_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg<true, false>, a));
 	} else {
@@ -1003,7 +1501,7 @@ int alpb_batched_cg_create(alpb_batched_cg *out, int64_t n, int64_t nnz, const i
 		if (h->nslices > nt) nt = h->nslices;
 	}
 	if (h->rows)
-		h->grid = solver_grid(k_batched_cg<true, true>, 32 * BCG_WARPS, h->nslices, BCG_WARPS);
+		h->grid = solver_grid(k_bcg_sliced, 32 * BCS_WARPS, h->nslices, BCS_WARPS);
 	else if (h->list)
 		h->grid = solver_grid(k_batched_cg<true, false>, 32 * BCG_WARPS, nt, BCG_WARPS);
 	else
@@ -1013,8 +1511,12 @@ int alpb_batched_cg_create(alpb_batched_cg *out, int64_t n, int64_t nnz, const i
 		set_error("alpb_batched_cg_create: no cooperative occupancy");
 		return ALPB_PANIC;
 	}
-	if (cudaMalloc(&h->work, size_t(4 * n) * 8) != cudaSuccess ||
-		cudaMalloc(&h->scratch, size_t(2 * nt) * 8) != cudaSuccess ||
+	// sliced solver: pairs (r, p) twice and A p; slots for every (warp,
+	// instance) pair a run can make: at most one per warp plus one per instance
+	h->nslots = h->rows ? int64_t(h->grid) * BCS_WARPS + nseg : 0;
+	const int64_t nscratch = h->rows ? 2 * h->nslots : 2 * nt;
+	if (cudaMalloc(&h->work, size_t((h->rows ? 5 : 4) * n) * 8) != cudaSuccess ||
+		cudaMalloc(&h->scratch, size_t(nscratch) * 8) != cudaSuccess ||
 		cudaMalloc(&h->inst, size_t(nseg) * sizeof(BcgInst)) != cudaSuccess ||
 		cudaMalloc(&h->active, 8) != cudaSuccess || cudaMalloc(&h->gs, sizeof(GridSync)) != cudaSuccess) {
 		cudaGetLastError();

@@ -166,8 +166,15 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> dict | None:
     A = dev.rmat(args.scale, EDGE_FACTOR, seed=SEED, vtype=abi.FP64)
     x = dev.gen_values(A.n, abi.FP64, seed=SEED + 7)
     u = torch.zeros(A.m, dtype=torch.float64, device="cuda")
-    plan = dev.Plan(A, sched=abi.SCHED_AUTO)
-    plan.autotune(abi.RING_PLUS_TIMES_F64, x, u)
+    if args.hot_slots is None:
+        plan = dev.Plan(A, sched=abi.SCHED_AUTO)
+        plan.autotune(abi.RING_PLUS_TIMES_F64, x, u)
+    else:
+        # the autotuner's choice pinned (profiling: under ncu its event timings
+        # are not the kernels' own, so it may choose otherwise)
+        plan = dev.Plan(A, sched=abi.SCHED_MERGE_PATH)
+        abi.call("alpb_spmv_plan_hot", plan.h, abi.RING_PLUS_TIMES_F64, A.n, dev.ptr(A.indices),
+                 args.hot_slots, dev.stream_ptr())
     sched, vw, tiles = plan.info()
     hot_slots, hot_cover = C.c_int64(), C.c_double()
     abi.call("alpb_spmv_plan_hot_info", plan.h, C.byref(hot_slots), C.byref(hot_cover))
@@ -943,6 +950,8 @@ def main():
     ap.add_argument("--only", choices=["batched_cg", "hpcg", "adjoint_cg", "ppr", "pagerank", "cg",
                                        "sweeps"],
                     help="run one secondary workload alone and print its line (profiling)")
+    ap.add_argument("--hot-slots", type=int, default=None,
+                    help="merge path with this many hot-column slots instead of the autotuner")
     ap.add_argument("--hpcg-side", type=int, default=256)
     ap.add_argument("--hpcg-levels", type=int, default=3)
     ap.add_argument("--ppr-scale", type=int, default=24)
