@@ -253,16 +253,37 @@ struct HotX {
 	const T *xs;
 	const T *__restrict__ x;
 	__device__ __forceinline__ T operator()(uint32_t c) const {
-		return (c & kHotBit) ? xs[c ^ kHotBit] : __ldg(x + c);
+		// the cold columns' x through L2 only: L1 space is left to the misses
+		// in flight (with most of the SM's memory given to shared slots, an
+		// allocating load held the gathers back measurably at 12 K+ slots)
+		return (c & kHotBit) ? xs[c ^ kHotBit] : __ldcg(x + c);
 	}
 };
 
+// Shared memory of one block: the warps' compact tiles (products, row ends
+// and the y of the tile's rows), then the hot-column slots.
 template <class R>
 struct HotSmem {
-	static constexpr size_t warp_bytes = (sizeof(WarpSmem<R>) + 15) / 16 * 16;
-	static constexpr size_t y_off = warp_bytes * HOT_WARPS;
-	static constexpr size_t x_off = y_off + size_t(HOT_WARPS) * WM_TILE * sizeof(typename R::T);
+	static constexpr size_t warp_bytes = (sizeof(WarpSmemCompact<R>) + 15) / 16 * 16;
+	static constexpr size_t x_off = warp_bytes * HOT_WARPS;
 	static size_t bytes(int64_t hot_k) { return x_off + size_t(hot_k) * sizeof(typename R::T); }
+};
+
+// y_r = y_r (+) row sum, with the y of the tile's rows fetched into the
+// compact tile's buffer at the start of the tile (as WarpAccumulateY).
+template <class R>
+struct HotAccumulateY {
+	using T = typename R::T;
+	T *__restrict__ y;
+	WarpSmemCompact<R> *sm;
+	int64_t base = 0;
+	__device__ __forceinline__ void begin_tile(int64_t i0, int nrows, int lane) {
+		base = i0;
+		for (int k = lane; k < nrows; k += 32) sm->y(k) = y[i0 + k];
+	}
+	__device__ __forceinline__ void row(int64_t r, T v, bool has) {
+		if (has) y[r] = R::add(sm->y(int(r - base)), v);  // foldl( y_r, row sum )
+	}
 };
 
 __global__ void k_col_counts(const uint32_t *__restrict__ idx, int64_t nnz, uint32_t *cnt) {
@@ -297,16 +318,14 @@ k_spmv_wmerge_hot(MergeTables mt, const int64_t *__restrict__ offsets,
 	typename R::T *__restrict__ y, int left) {
 	using T = typename R::T;
 	extern __shared__ __align__(16) unsigned char hot_smem[];
-	WarpSmem<R> *sm = reinterpret_cast<WarpSmem<R> *>(hot_smem);
-	T *ybuf = reinterpret_cast<T *>(hot_smem + HotSmem<R>::y_off);
 	T *xs = reinterpret_cast<T *>(hot_smem + HotSmem<R>::x_off);
 	for (int64_t i = threadIdx.x; i < hot_k; i += blockDim.x) xs[i] = hx[i];
 	__syncthreads();
 	const int w = threadIdx.x >> 5;
 	HotX<T> xl{xs, x};
-	WarpAccumulateY<R> epi{y, ybuf + size_t(w) * WM_TILE};
-	WarpSmem<R> &mine = *reinterpret_cast<WarpSmem<R> *>(hot_smem + HotSmem<R>::warp_bytes * w);
-	(void) sm;
+	WarpSmemCompact<R> &mine =
+		*reinterpret_cast<WarpSmemCompact<R> *>(hot_smem + HotSmem<R>::warp_bytes * w);
+	HotAccumulateY<R> epi{y, &mine};
 	const int64_t nw = int64_t(gridDim.x) * HOT_WARPS;
 	int64_t t = int64_t(blockIdx.x) * HOT_WARPS + w;
 	WmMeta g = wm_meta(mt, t);
@@ -1097,15 +1116,17 @@ int alpb_spmv_autotune(alpb_spmv_plan p, int ring, int64_t n, const uint32_t *in
 	}
 	p->sched = cands[best_i].sched;
 	p->vw = cands[best_i].sched == ALPB_SCHED_VECTOR ? cands[best_i].w : saved_vw;
-	// skewed rows on the merge path: try the hot-column cache at two sizes
-	// (beyond them its shared memory takes too much of the SM's L1)
+	// skewed rows on the merge path: try the hot-column cache at four sizes,
+	// up to what the shared memory left by the warps' tiles holds
 	hot_release(p);
 	if (p->sched == ALPB_SCHED_MERGE_PATH && p->tile == WM_TILE && n >= (int64_t(1) << 16) &&
 		p->nnz >= (int64_t(1) << 20)) {
-		struct HotCand { int64_t k; } hc[2] = {{std::min<int64_t>(2048, hot_slots_max(ring))},
-			{std::min<int64_t>(4096, hot_slots_max(ring))}};
+		constexpr int NH = 4;
+		struct HotCand { int64_t k; } hc[NH] = {{std::min<int64_t>(4096, hot_slots_max(ring))},
+			{std::min<int64_t>(8192, hot_slots_max(ring))},
+			{std::min<int64_t>(12288, hot_slots_max(ring))}, {hot_slots_max(ring)}};
 		int best_c = -1;
-		for (int c = 0; c < 2; ++c) {
+		for (int c = 0; c < NH; ++c) {
 			if (hc[c].k <= 0 || hc[c].k >= n) continue;
 			int rc = hot_build(p, indices, n, hc[c].k, s);
 			if (rc != ALPB_SUCCESS) {

@@ -38,8 +38,23 @@ __device__ __forceinline__ int wm_pad(int k) { return k ^ ((k >> 3) & 15); }
 
 template <class R>
 struct WarpSmem {
+	using End = int32_t;
 	typename R::T prod[WM_TILE < 128 ? 128 : WM_TILE];
-	int32_t row_end[WM_TILE + 2];  // [k] = end of tile row k-1, relative to j0, clamped
+	End row_end[WM_TILE + 2];  // [k] = end of tile row k-1, relative to j0, clamped
+};
+
+// Compact variant (2.7 KB per warp for FP64 instead of 3 KB plus a separate
+// y buffer): row ends fit 16 bits (they are clamped to [-1, WM_TILE + 1]),
+// and the y values of the tile's rows share the product buffer, from its far
+// end down: products occupy [0, nnzt rounded up to 16) (the swizzle stays
+// inside aligned groups of 16) and y of row k sits at prod[WM_TILE + 15 - k];
+// the two never meet since rows + nonzeroes of a tile are at most WM_TILE.
+template <class R>
+struct WarpSmemCompact {
+	using End = int16_t;
+	typename R::T prod[WM_TILE + 16];
+	End row_end[WM_TILE + 2];
+	__device__ __forceinline__ typename R::T &y(int k) { return prod[WM_TILE + 15 - k]; }
 };
 
 template <class T>
@@ -74,11 +89,11 @@ __device__ __forceinline__ T wm_load_slot(const uint64_t *p) {
 // end in the tile (its shared-memory writes are visible to epi.row).  Leaves in every lane:
 // head_v/head_h (the partial of row i0 up to its end, in the lane whose first
 // finished row is row 0) and sv/sh (lane 31: the partial of the tail row).
-template <class R, class XL, class Epi>
+template <class R, class XL, class Epi, class SM>
 __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
 	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
-	WarpSmem<R> &sm, int64_t i0, int64_t i1, int64_t hf, int &first_row,
+	SM &sm, int64_t i0, int64_t i1, int64_t hf, int &first_row,
 	typename R::T &head_v, bool &head_h, typename R::T &sv, bool &sh) {
 	using T = typename R::T;
 	const int lane = threadIdx.x & 31;
@@ -108,7 +123,7 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 		}
 		if (v > WM_TILE + 1) v = WM_TILE + 1;
 		if (v < -1) v = -1;
-		sm.row_end[k] = int32_t(v);
+		sm.row_end[k] = static_cast<typename SM::End>(v);
 	}
 	{
 		uint32_t col[WM_IPT];
@@ -228,11 +243,11 @@ __device__ __forceinline__ WmMeta wm_meta(const MergeTables &mt, int64_t t) {
 // head_val[t] (the row ends here) or tail_val[t] (it continues), and
 // k_wm_fixup finishes it.  A spanning row always holds nonzeroes, so its
 // partials need no presence flag: an empty partial is the additive identity.
-template <class R, class XL, class Epi>
+template <class R, class XL, class Epi, class SM>
 __device__ __forceinline__ void warp_tile(int64_t t, const WmMeta &g, const MergeTables &mt,
 	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
 	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
-	WarpSmem<R> &sm) {
+	SM &sm) {
 	using T = typename R::T;
 	const int lane = threadIdx.x & 31;
 	int first_row;

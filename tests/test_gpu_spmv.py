@@ -505,9 +505,10 @@ def test_vec_engine_integer_domains(cuda):
     assert got == wrapped.min() and wrapped.min() != (a.astype(np.int64) + b).min()
 
 
+@pytest.mark.parametrize("slots", [4096, 16384])
 @pytest.mark.parametrize("ring", [0, 1, 2, 5])
 @pytest.mark.parametrize("form", [2, 1], ids=["mxv", "vxm"])
-def test_hot_column_cache_bit_identical(cuda, oracle, ring, form):
+def test_hot_column_cache_bit_identical(cuda, oracle, ring, form, slots):
     """The merge path with the hot-column cache (alpb_spmv_plan_hot: the most
     frequent columns' x values in shared memory) gives the merge path's
     result bit for bit -- same products, same sums in the same order -- for
@@ -536,18 +537,19 @@ def test_hot_column_cache_bit_identical(cuda, oracle, ring, form):
     plan = dev.Plan(S, sched=abi.SCHED_MERGE_PATH)
     want = u0.clone()
     dev.mxv(ring, S, want, x, form=form, plan=plan)
-    abi.call("alpb_spmv_plan_hot", plan.h, ring, S.n, dev.ptr(S.indices), 4096, dev.stream_ptr())
-    slots, cover = C.c_int64(), C.c_double()
-    abi.call("alpb_spmv_plan_hot_info", plan.h, C.byref(slots), C.byref(cover))
-    assert slots.value == 4096 and 0.1 < cover.value < 1.0, (slots.value, cover.value)
+    abi.call("alpb_spmv_plan_hot", plan.h, ring, S.n, dev.ptr(S.indices), slots,
+             dev.stream_ptr())
+    nslots, cover = C.c_int64(), C.c_double()
+    abi.call("alpb_spmv_plan_hot_info", plan.h, C.byref(nslots), C.byref(cover))
+    assert nslots.value == slots and 0.1 < cover.value < 1.0, (nslots.value, cover.value)
     for _ in range(2):
         got = u0.clone()
         dev.mxv(ring, S, got, x, form=form, plan=plan)
         torch.cuda.synchronize()
         assert torch.equal(got, want)
     abi.call("alpb_spmv_plan_hot", plan.h, ring, S.n, dev.ptr(S.indices), 0, dev.stream_ptr())
-    abi.call("alpb_spmv_plan_hot_info", plan.h, C.byref(slots), C.byref(cover))
-    assert slots.value == 0
+    abi.call("alpb_spmv_plan_hot_info", plan.h, C.byref(nslots), C.byref(cover))
+    assert nslots.value == 0
     got = u0.clone()
     dev.mxv(ring, S, got, x, form=form, plan=plan)
     torch.cuda.synchronize()
@@ -557,7 +559,7 @@ def test_hot_column_cache_bit_identical(cuda, oracle, ring, form):
     assert rc == abi.ILLEGAL
 
 
-@pytest.mark.parametrize("slots", [2048, 4096])
+@pytest.mark.parametrize("slots", [4096, 16384])
 def test_hot_column_cache_matches_restatement_rmat22(cuda, oracle, slots):
     """The benchmark's product (R-MAT scale 22, FP64 plus-times) through a plan
     with the hot-column cache, against the restatement (1e-12 relative)."""
