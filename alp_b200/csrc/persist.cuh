@@ -6,12 +6,13 @@
 namespace alpb {
 
 // Barrier state in device memory; zero-initialise before the launch.  The
-// arrival counter and the polled words sit on separate 128-byte lines, so
-// that the pollers do not contend with the arrivals' atomics.
+// arrival counter only grows: barrier k of the launch completes when it
+// reaches k * gridDim.x, so no block resets it and no second word is flipped.
+// The counter and the error flag sit on separate 128-byte lines.
 struct alignas(128) GridSync {
-	unsigned int count;
-	unsigned int pad0[31];
-	unsigned int gen;
+	unsigned long long count;
+	unsigned int pad0[30];
+	unsigned int gen;   // not used by grid_sync (kept for the layout)
 	int err;    // 1: a barrier or tile wait gave up (the kernel exits; host reports PANIC)
 	unsigned int pad1[30];
 };
@@ -21,30 +22,36 @@ struct alignas(128) GridSync {
 constexpr long long kSpinLimit = 1ll << 24;
 
 // All blocks of a cooperative launch call this the same number of times.
-// Returns false once any block has timed out; callers then leave their loop.
+// Thread 0 arrives with one acquire-release add (its block's writes before
+// the barrier are released; the last arrival acquires everyone's) and the
+// others poll the counter with acquire loads until their barrier's target,
+// so the last block to arrive goes on after one atomic round trip and the
+// others one poll later.  Returns false once any block has timed out; callers
+// then leave their loop.
 __device__ __forceinline__ bool grid_sync(GridSync *gs) {
 	__syncthreads();
 	if (threadIdx.x == 0) {
-		volatile unsigned int *vgen = &gs->gen;
-		volatile int *verr = &gs->err;
-		const unsigned int g = *vgen;
-		__threadfence();
-		const unsigned int arrived = atomicAdd(&gs->count, 1u);
-		if (arrived == gridDim.x - 1) {
-			gs->count = 0;
-			__threadfence();
-			atomicExch(&gs->gen, g + 1);
-		} else {
+		const unsigned long long G = gridDim.x;
+		unsigned long long old;
+		asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], 1;"
+					 : "=l"(old) : "l"(&gs->count) : "memory");
+		const unsigned long long target = (old / G + 1) * G;
+		if (old + 1 != target) {
+			volatile int *verr = &gs->err;
 			long long spins = 0;
-			while (*vgen == g && *verr == 0) {
-				if (++spins > kSpinLimit) {
+			for (;;) {
+				unsigned long long c;
+				asm volatile("ld.acquire.gpu.global.u64 %0, [%1];"
+							 : "=l"(c) : "l"(&gs->count) : "memory");
+				if (c >= target) break;
+				if ((++spins & 63) == 0 && *verr) break;
+				if (spins > kSpinLimit) {
 					atomicExch(&gs->err, 1);
 					break;
 				}
-				__nanosleep(64);
+				__nanosleep(32);
 			}
 		}
-		__threadfence();
 	}
 	__syncthreads();
 	return *((volatile int *) &gs->err) == 0;
@@ -91,8 +98,8 @@ int cooperative_grid(K kernel, int block, size_t smem, int64_t want) {
 // co-resident maximum.  Every grid barrier and every scalar reduction costs
 // time in proportion to the block count, so small systems get small grids.
 template <class K>
-int solver_grid(K kernel, int block, int64_t ntiles, int warps_per_block) {
-	const int max_grid = cooperative_grid(kernel, block, 0, 0);
+int solver_grid(K kernel, int block, int64_t ntiles, int warps_per_block, size_t smem = 0) {
+	const int max_grid = cooperative_grid(kernel, block, smem, 0);
 	int64_t g = ntiles / (4 * int64_t(warps_per_block));
 	if (g < 2 * int64_t(sm_count())) g = 2 * int64_t(sm_count());
 	if (g > max_grid) g = max_grid;
