@@ -768,11 +768,12 @@ k_batched_cg(BcgArgs a) {
 //     scalar step (no barrier of its own)
 // Work split: the active instances' slices, in instance order, are cut in ONE
 // contiguous run per warp (warp g of nw takes items [ntot g / nw,
-// ntot (g+1) / nw)), so a warp streams consecutive slices and rows.  A warp
-// leaves one partial per instance its run touches, in slot slot0[j] + g -
-// (first warp of instance j); an instance's sum is the sum of its slots in
-// slot order, formed by whoever needs it -- the same slots in the same order,
-// hence the same bits everywhere.  So the phase-B warps form alpha themselves,
+// ntot (g+1) / nw)), so a warp streams consecutive slices and rows.  A block
+// leaves one partial per instance its warps' runs touch (the warps' partials
+// added in warp order), in slot slot0[j] + b - (first block of instance j);
+// an instance's sum is the sum of its slots in slot order, formed by whoever
+// needs it -- the same slots in the same order, hence the same bits
+// everywhere.  So the phase-B warps form alpha themselves,
 // and after the second barrier every block forms every active instance's r.r,
 // convergence test, gamma and sigma in its own shared memory (identical in
 // all blocks) and rebuilds its active list; block 0 publishes the results.
@@ -801,9 +802,12 @@ constexpr int BCS_WARPS = ALPB_BCS_WARPS;  // warps per block (ALPB_BCS_MINB blo
 constexpr int BCS_WMAX = ALPB_BCS_WMAX;    // widest slice of the unrolled product path
 constexpr int BCS_RB = ALPB_BCS_RB;        // rows per lane whose loads phase B issues together
 constexpr int BCS_SU = ALPB_BCS_SU;        // instances whose slot sums a warp forms together
-// Slices per warp at least, when fewer than all warps suffice: in the tail,
-// when few instances are left, their sums then have fewer slots to add.
-constexpr int32_t BCS_MINRUN = 8;
+// Slices per warp at least, when fewer than all warps suffice (the tail, when
+// few instances are left): measured 18.42 ms with 1 or 2, 18.94 ms with 8.
+#ifndef ALPB_BCS_MINRUN
+#define ALPB_BCS_MINRUN 2
+#endif
+constexpr int32_t BCS_MINRUN = ALPB_BCS_MINRUN;
 
 struct BcsArgs {
 	const int64_t *seg_rows;       // [nseg+1]
@@ -834,6 +838,10 @@ struct BcsShared {
 	double sigma[BCG_LIST_MAX], gamma[BCG_LIST_MAX], tol_abs[BCG_LIST_MAX];
 	uint8_t done[BCG_LIST_MAX];
 	int32_t scan[32];
+	// partials of the first and the last instance of each warp's run (the
+	// ones a neighbouring warp may share), combined per block in warp order
+	int32_t edge_j[BCS_WARPS][2];
+	double2 edge_v[BCS_WARPS][2];
 };
 
 // first item of warp g's run
@@ -843,6 +851,11 @@ __device__ __forceinline__ int64_t bcs_kb(int64_t ntot, int64_t g, int64_t nw) {
 // warp whose run holds item k: the largest g with bcs_kb(g) <= k
 __device__ __forceinline__ int64_t bcs_warp_of(int64_t ntot, int64_t k, int64_t nw) {
 	return ((k + 1) * nw - 1) / ntot;
+}
+
+// block whose warps' runs hold item k
+__device__ __forceinline__ int64_t bcs_block_of(int64_t ntot, int64_t k, int64_t nw) {
+	return bcs_warp_of(ntot, k, nw) / BCS_WARPS;
 }
 
 // block-wide exclusive scan of one int per thread (thread order); returns
@@ -904,21 +917,21 @@ __device__ __noinline__ void bcs_build_list(BcsShared &S, int64_t nseg, int64_t 
 		S.nwe = nw < want ? nw : want;
 	}
 	__syncthreads();
-	// slots: warps whose runs touch instance j (every active instance has at
-	// least one slice, so at least one warp; with nwe warps every run holds at
-	// least one item, so each warp from the instance's first to its last
-	// writes its slot)
+	// slots: one per block whose warps touch instance j (every active
+	// instance has at least one slice, so at least one warp; with nwe warps
+	// every run holds at least one item, so each block from the instance's
+	// first to its last writes its slot)
 	nw = S.nwe;
 	const int pj = (ni + nth - 1) / nth;
 	const int j0 = tid * pj, j1 = j0 + pj < ni ? j0 + pj : ni;
 	int32_t cs = 0;
 	for (int j = j0; j < j1; ++j)
-		cs += int32_t(bcs_warp_of(ntot, S.off[j + 1] - 1, nw) - bcs_warp_of(ntot, S.off[j], nw) + 1);
+		cs += int32_t(bcs_block_of(ntot, S.off[j + 1] - 1, nw) - bcs_block_of(ntot, S.off[j], nw) + 1);
 	int32_t nslots;
 	int32_t ps = bcs_scan(cs, S.scan, &nslots);
 	for (int j = j0; j < j1; ++j) {
 		S.slot0[j] = ps;
-		ps += int32_t(bcs_warp_of(ntot, S.off[j + 1] - 1, nw) - bcs_warp_of(ntot, S.off[j], nw) + 1);
+		ps += int32_t(bcs_block_of(ntot, S.off[j + 1] - 1, nw) - bcs_block_of(ntot, S.off[j], nw) + 1);
 	}
 	if (tid == 0) S.slot0[ni] = nslots;
 	__syncthreads();
@@ -1098,6 +1111,78 @@ __device__ __forceinline__ void bcs_instance_step(const BcsArgs &a, BcsShared &S
 	}
 }
 
+// The warp's run with one partial (or a pair of partials) per instance
+// segment, fn(j, s, k, e) -> double2, reduced to one slot per (block,
+// instance): an instance inside a warp's run (no other warp touches it) is
+// written by the warp; the first and the last instance of each run go to the
+// block's edge table, and thread 0 sums them in warp order.  Slot of
+// (instance j, block b): slot0[j] + b - (first block of j).  ya: slots of
+// the first partials, yb: of the second (null: none).  Every thread of the
+// block calls this.
+template <class F>
+__device__ __forceinline__ void bcs_walk_slots(BcsShared &S, int64_t g, int lane, double *ya,
+	double *yb, F &&fn) {
+	const int w = threadIdx.x >> 5;
+	const int64_t b = blockIdx.x;
+	const auto slot = [&](int j) {
+		return S.slot0[j] + int32_t(b - bcs_block_of(S.ntot, S.off[j], S.nwe));
+	};
+	// lane 0 keeps the latest segment in edge slot 1 until the next one shows
+	// that it lay inside the run
+	if (lane == 0) {
+		S.edge_j[w][0] = -1;
+		S.edge_j[w][1] = -1;
+	}
+	bool first = true;
+	bcs_walk(S, g, [&](int j, int s, int64_t k, int64_t e) {
+		const double2 v = fn(j, s, k, e);
+		if (lane == 0) {
+			if (first) {
+				S.edge_j[w][0] = j;
+				S.edge_v[w][0] = v;
+			} else {
+				const int jp = S.edge_j[w][1];
+				if (jp >= 0) {
+					const int32_t sl = slot(jp);
+					ya[sl] = S.edge_v[w][1].x;
+					if (yb) yb[sl] = S.edge_v[w][1].y;
+				}
+				S.edge_j[w][1] = j;
+				S.edge_v[w][1] = v;
+			}
+		}
+		first = false;
+	});
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		int jc = -1;
+		double2 acc = make_double2(0.0, 0.0);
+		for (int u = 0; u < BCS_WARPS; ++u)
+			for (int q = 0; q < 2; ++q) {
+				const int j = S.edge_j[u][q];
+				if (j < 0) continue;
+				const double2 v = S.edge_v[u][q];
+				if (j != jc) {
+					if (jc >= 0) {
+						const int32_t sl = slot(jc);
+						ya[sl] = acc.x;
+						if (yb) yb[sl] = acc.y;
+					}
+					jc = j;
+					acc = v;
+				} else {
+					acc.x += v.x;
+					acc.y += v.y;
+				}
+			}
+		if (jc >= 0) {
+			const int32_t sl = slot(jc);
+			ya[sl] = acc.x;
+			if (yb) yb[sl] = acc.y;
+		}
+	}
+}
+
 __global__ void __launch_bounds__(32 * BCS_WARPS, ALPB_BCS_MINB) k_bcg_sliced(BcsArgs a) {
 	__shared__ BcsShared S;
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1118,7 +1203,7 @@ __global__ void __launch_bounds__(32 * BCS_WARPS, ALPB_BCS_MINB) k_bcg_sliced(Bc
 	bcs_build_list(S, a.nseg, nw);
 
 	// prelude: r = b - A x, pairs (r, 0); partials r.r -> slot_a, b.b -> slot_b
-	bcs_walk(S, g, [&](int j, int s, int64_t k, int64_t e) {
+	bcs_walk_slots(S, g, lane, a.slot_a, a.slot_b, [&](int j, int s, int64_t k, int64_t e) {
 		const int64_t q0 = k - S.off[j];
 		const int64_t R0 = __ldg(a.seg_rows + s), R1 = __ldg(a.seg_rows + s + 1);
 		double rr = 0.0, bb = 0.0;
@@ -1131,12 +1216,7 @@ __global__ void __launch_bounds__(32 * BCS_WARPS, ALPB_BCS_MINB) k_bcg_sliced(Bc
 				rr += ri * ri;
 				bb += bi * bi;
 			});
-		const double s1 = warp_sum(rr), s2 = warp_sum(bb);
-		if (lane == 0) {
-			const int32_t sl = S.slot0[j] + int32_t(g - bcs_warp_of(S.ntot, S.off[j], S.nwe));
-			a.slot_a[sl] = s1;
-			a.slot_b[sl] = s2;
-		}
+		return make_double2(warp_sum(rr), warp_sum(bb));
 	});
 	if (!grid_sync(a.gs)) return;
 	for (int j0 = w * BCS_SU; j0 < S.n; j0 += BCS_WARPS * BCS_SU) {
@@ -1157,7 +1237,7 @@ __global__ void __launch_bounds__(32 * BCS_WARPS, ALPB_BCS_MINB) k_bcg_sliced(Bc
 		const double2 *pc = a.pair[cur];
 		double2 *pn = a.pair[cur ^ 1];
 		// phase A: temp = A p, partials p.(A p) -> slot_a
-		bcs_walk(S, g, [&](int j, int s, int64_t k, int64_t e) {
+		bcs_walk_slots(S, g, lane, a.slot_a, nullptr, [&](int j, int s, int64_t k, int64_t e) {
 			const int64_t q0 = k - S.off[j];
 			const int64_t R0 = __ldg(a.seg_rows + s), R1 = __ldg(a.seg_rows + s + 1);
 			const double gamma = S.gamma[s];
@@ -1173,13 +1253,12 @@ __global__ void __launch_bounds__(32 * BCS_WARPS, ALPB_BCS_MINB) k_bcg_sliced(Bc
 					const double un = p.x + gamma * p.y;
 					acc += v * un;
 				});
-			const double part = warp_sum(acc);
-			if (lane == 0) a.slot_a[S.slot0[j] + int32_t(g - bcs_warp_of(S.ntot, S.off[j], S.nwe))] = part;
+			return make_double2(warp_sum(acc), 0.0);
 		});
 		if (!grid_sync(a.gs)) return;
 		// phase B: alpha from the instance's slots; x += alpha p, r -= alpha A p,
 		// the next pairs; partials r.r -> slot_b
-		bcs_walk(S, g, [&](int j, int s, int64_t k, int64_t e) {
+		bcs_walk_slots(S, g, lane, a.slot_b, nullptr, [&](int j, int s, int64_t k, int64_t e) {
 			const double alpha = S.sigma[s] / bcs_slot_sum(a.slot_a, S.slot0[j], S.slot0[j + 1], lane);
 			const double gamma = S.gamma[s];
 			const int64_t q0 = k - S.off[j];
@@ -1212,8 +1291,7 @@ __global__ void __launch_bounds__(32 * BCS_WARPS, ALPB_BCS_MINB) k_bcg_sliced(Bc
 					}
 				}
 			}
-			part = warp_sum(part);
-			if (lane == 0) a.slot_b[S.slot0[j] + int32_t(g - bcs_warp_of(S.ntot, S.off[j], S.nwe))] = part;
+			return make_double2(warp_sum(part), 0.0);
 		});
 		if (!grid_sync(a.gs)) return;
 		// scalar step, in every block: r.r, convergence, gamma, sigma; a warp
