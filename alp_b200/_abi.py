@@ -116,6 +116,7 @@ PROTOS: dict[str, list] = {
     "alpb_vec_reduce_dom": [P, I32, U64, I32, U32, I32, I64, P, I32, P, P, I32, P, P, P, I32,
                             I32, P],
     "alpb_count_assigned": [P, I64, PI64, P],
+    "alpb_vec_chain": [I32, I64, I32, P, P, I32, P, P, P],
     "alpb_vec_reduce": [PD, I32, D, I32, U32, I64, P, I32, P, P, I32, P, P, P, I32, I32, P],
     "alpb_cg_solve": [I64, P, P, P, P, P, I64, D, PI64, PD, P, P, P],
     "alpb_pagerank": [I64, P, P, P, P, P, P, P, I32, D, D, I64, PI64, PD, P],
@@ -131,6 +132,16 @@ PROTOS: dict[str, list] = {
     "alpb_batched_cg_results": [P, P, P, P, P],
 }
 _RESTYPE = {"alpb_last_error": C.c_char_p, "alpb_launch_count": C.c_int64}
+
+VEC_SET, VEC_FOLDL, VEC_FOLDR, VEC_APPLY, VEC_MULADD, VEC_REDUCE = 0, 1, 2, 3, 4, 5
+
+
+class VecStep(C.Structure):
+    """struct alpb_vec_step of alp_b200.h (one step of alpb_vec_chain)."""
+    _fields_ = [("kind", C.c_int32), ("op", C.c_int32), ("mul_op", C.c_int32),
+                ("descr", C.c_uint32), ("z", C.c_int32), ("x", C.c_int32), ("y", C.c_int32),
+                ("reserved", C.c_int32), ("alpha", C.c_uint64), ("beta", C.c_uint64),
+                ("identity", C.c_uint64)]
 
 _lib = None
 

@@ -376,6 +376,158 @@ static int vec_op_run(int kind, int op, int monoid, uint64_t identity, int mul_o
 	return ALPB_SUCCESS;
 }
 
+// ------------------------------------------------------ fused chains --
+// Steps of alpb_vec_chain, with the domain's values decoded; slot values live
+// in a per-thread array for the element being processed.
+template <class T>
+struct ChainStep {
+	int32_t kind, op, mul_op, use_index, z, x, y;
+	T alpha, beta;
+};
+template <class T>
+struct ChainArgs {
+	int64_t n;
+	int nslots, nsteps;
+	uint32_t load, store;          // slots read before written / written
+	void *val[ALPB_CHAIN_SLOTS];
+	int type[ALPB_CHAIN_SLOTS];
+	ChainStep<T> step[ALPB_CHAIN_STEPS];
+	int reduce;                    // the last step is a reduction
+	int radd, rmul, rx, ry;
+	T rident;
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) k_vec_chain(ChainArgs<T> c, T *partials) {
+	__shared__ T sm[32];
+	T acc = c.rident;
+	bool any = false;
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < c.n;
+		 i += int64_t(gridDim.x) * blockDim.x) {
+		T v[ALPB_CHAIN_SLOTS];
+#pragma unroll
+		for (int q = 0; q < ALPB_CHAIN_SLOTS; ++q)
+			if (q < c.nslots && ((c.load >> q) & 1)) v[q] = ld_as<T>(c.val[q], c.type[q], i);
+		for (int k = 0; k < c.nsteps; ++k) {
+			const ChainStep<T> &o = c.step[k];
+			const T xv = o.x >= 0 ? v[o.x] : o.alpha;
+			const T yv = o.y >= 0 ? v[o.y] : o.beta;
+			switch (o.kind) {
+			case ALPB_VEC_SET: v[o.z] = o.use_index ? T(i) : xv; break;
+			case ALPB_VEC_FOLDL: v[o.z] = opv(o.op, v[o.z], xv); break;
+			case ALPB_VEC_FOLDR: v[o.z] = opv(o.op, xv, v[o.z]); break;
+			default: v[o.z] = opv(o.op, v[o.z], opv(o.mul_op, xv, yv)); break;  // MULADD
+			}
+		}
+		if (c.reduce) {   // as k_vec_dot on dense operands
+			const T t = c.ry >= 0 ? opv(c.rmul, v[c.rx], v[c.ry]) : v[c.rx];
+			acc = any ? opv(c.radd, acc, t) : opv(c.radd, c.rident, t);
+			any = true;
+		}
+#pragma unroll
+		for (int q = 0; q < ALPB_CHAIN_SLOTS; ++q)
+			if (q < c.nslots && ((c.store >> q) & 1)) st_as<T>(c.val[q], c.type[q], i, v[q]);
+	}
+	if (!c.reduce) return;
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	for (int o = 16; o > 0; o >>= 1) acc = opv(c.radd, acc, shfl_down_t(acc, o));
+	if (lane == 0) sm[wid] = acc;
+	__syncthreads();
+	if (wid == 0) {
+		T w = lane < int(blockDim.x >> 5) ? sm[lane] : c.rident;
+		for (int o = 16; o > 0; o >>= 1) w = opv(c.radd, w, shfl_down_t(w, o));
+		if (lane == 0) partials[blockIdx.x] = w;
+	}
+}
+
+static bool domain_type(int domain, int type) {
+	return type == domain || (domain == ALPB_UINT64 && type == ALPB_INT64) ||
+		(domain == ALPB_INT64 && type == ALPB_UINT64);
+}
+
+template <class T>
+static int vec_chain_run(int domain, int64_t n, int nslots, void *const *values,
+	const int *types, int nsteps, const alpb_vec_step *steps, void *result, cudaStream_t s) {
+	ChainArgs<T> c{};
+	c.n = n;
+	c.nslots = nslots;
+	uint32_t written = 0;
+	for (int q = 0; q < nslots; ++q) {
+		ALPB_CHECK(values[q] != nullptr, ALPB_ILLEGAL, "alpb_vec_chain: null vector in slot %d", q);
+		ALPB_CHECK(domain_type(domain, types[q]), ALPB_UNSUPPORTED,
+			"alpb_vec_chain: slot %d has type %d, not the domain's", q, types[q]);
+		c.val[q] = values[q];
+		c.type[q] = types[q];
+	}
+	const auto slot_ok = [&](int q, bool scalar_ok) { return (scalar_ok && q == -1) || (q >= 0 && q < nslots); };
+	const auto read = [&](int q) { if (q >= 0 && !((written >> q) & 1)) c.load |= 1u << q; };
+	for (int k = 0; k < nsteps; ++k) {
+		const alpb_vec_step &o = steps[k];
+		const bool last = k + 1 == nsteps;
+		if (o.kind == ALPB_VEC_REDUCE) {
+			ALPB_CHECK(last && result != nullptr, ALPB_ILLEGAL,
+				"alpb_vec_chain: a reduction must be the last step, with a result");
+			ALPB_CHECK(slot_ok(o.x, false) && (o.y == -1 || slot_ok(o.y, false)), ALPB_ILLEGAL,
+				"alpb_vec_chain: reduction operands");
+			ALPB_CHECK(o.op >= ALPB_OP_ADD && o.op <= ALPB_OP_LAND && o.mul_op >= ALPB_OP_ADD &&
+				o.mul_op <= ALPB_OP_GEQ && o.mul_op != ALPB_OP_LEFT_ASSIGN_IF, ALPB_UNSUPPORTED,
+				"alpb_vec_chain: reduction ops %d %d", o.op, o.mul_op);
+			read(o.x);
+			read(o.y);
+			c.reduce = 1;
+			c.radd = o.op;
+			c.rmul = o.mul_op;
+			c.rx = o.x;
+			c.ry = o.y;
+			c.rident = from_bits<T>(o.identity);
+			continue;
+		}
+		ALPB_CHECK(o.kind >= ALPB_VEC_SET && o.kind <= ALPB_VEC_MULADD && o.kind != ALPB_VEC_APPLY,
+			ALPB_ILLEGAL, "alpb_vec_chain: step kind %d", o.kind);
+		ALPB_CHECK(o.op >= ALPB_OP_ADD && o.op <= ALPB_OP_GEQ && o.op != ALPB_OP_LEFT_ASSIGN_IF &&
+			(o.kind != ALPB_VEC_MULADD || (o.mul_op >= ALPB_OP_ADD && o.mul_op <= ALPB_OP_GEQ &&
+			o.mul_op != ALPB_OP_LEFT_ASSIGN_IF)), ALPB_UNSUPPORTED, "alpb_vec_chain: step ops");
+		ALPB_CHECK(slot_ok(o.z, false) && slot_ok(o.x, true) &&
+			(o.kind != ALPB_VEC_MULADD || slot_ok(o.y, true)), ALPB_ILLEGAL,
+			"alpb_vec_chain: step %d slots", k);
+		read(o.x);
+		if (o.kind == ALPB_VEC_MULADD) read(o.y);
+		if (o.kind != ALPB_VEC_SET) read(o.z);
+		written |= 1u << o.z;
+		ChainStep<T> &d = c.step[c.nsteps++];
+		d.kind = o.kind;
+		d.op = o.op;
+		d.mul_op = o.mul_op;
+		d.use_index = o.kind == ALPB_VEC_SET && (o.descr & ALPB_DESC_USE_INDEX) ? 1 : 0;
+		d.z = o.z;
+		d.x = o.x;
+		d.y = o.kind == ALPB_VEC_MULADD ? o.y : -1;
+		d.alpha = from_bits<T>(o.alpha);
+		d.beta = from_bits<T>(o.beta);
+	}
+	c.store = written;
+	if (!c.reduce) {
+		k_vec_chain<T><<<grid_for(n, 256), 256, 0, s>>>(c, nullptr);
+		ALPB_LAUNCHED();
+		return ALPB_SUCCESS;
+	}
+	// the reduction's grid and order are those of alpb_vec_reduce_dom
+	int64_t g64 = (n + 256 * 8 - 1) / (256 * 8);
+	if (g64 > int64_t(sm_count()) * 4) g64 = int64_t(sm_count()) * 4;
+	const int g = int(g64 < 1 ? 1 : g64);
+	T *part = nullptr;
+	ALPB_CUDA(cudaMallocAsync(&part, size_t(g + 1) * sizeof(T), s));
+	k_vec_chain<T><<<g, 256, 0, s>>>(c, part);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cudaMemcpyAsync(part + g, result, sizeof(T), cudaMemcpyHostToDevice, s));
+	k_vec_dot_finish<T><<<1, 32, 0, s>>>(c.radd, part, g, part + g);
+	ALPB_LAUNCHED();
+	ALPB_CUDA(cudaMemcpyAsync(result, part + g, sizeof(T), cudaMemcpyDeviceToHost, s));
+	ALPB_CUDA(cudaFreeAsync(part, s));
+	ALPB_CUDA(cudaStreamSynchronize(s));
+	return ALPB_SUCCESS;
+}
+
 static uint64_t bits_of(double v) {
 	uint64_t b;
 	memcpy(&b, &v, 8);
@@ -477,6 +629,28 @@ int alpb_vec_op(int kind, int op, int monoid, double identity, int mul_op, uint3
 	return alpb_vec_op_dom(kind, op, monoid, bits_of(identity), mul_op, descr, ALPB_FP64, n, z,
 		z_type, z_assigned, z_nnz, mask, mask_assigned, mask_type, masked, x, x_type, x_assigned,
 		bits_of(alpha), y, y_type, y_assigned, bits_of(beta), stream);
+}
+
+int alpb_vec_chain(int domain, int64_t n, int nslots, void *const *values, const int *types,
+	int nsteps, const alpb_vec_step *steps, void *result, void *stream) {
+	ALPB_CHECK(nslots >= 0 && nslots <= ALPB_CHAIN_SLOTS && nsteps >= 0 &&
+		nsteps <= ALPB_CHAIN_STEPS, ALPB_ILLEGAL, "alpb_vec_chain: %d slots, %d steps (at most %d, %d)",
+		nslots, nsteps, ALPB_CHAIN_SLOTS, ALPB_CHAIN_STEPS);
+	ALPB_CHECK(nsteps == 0 || (values != nullptr && types != nullptr && steps != nullptr),
+		ALPB_ILLEGAL, "alpb_vec_chain: null arrays");
+	ALPB_CHECK(domain == ALPB_FP64 || domain == ALPB_INT64 || domain == ALPB_UINT64 ||
+		domain == ALPB_INT32 || domain == ALPB_UINT32, ALPB_UNSUPPORTED,
+		"alpb_vec_chain: domain %d", domain);
+	if (n < 0) return ALPB_ILLEGAL;
+	if (n == 0 || nsteps == 0) return ALPB_SUCCESS;
+	cudaStream_t s = as_stream(stream);
+	switch (domain) {
+	case ALPB_FP64: return vec_chain_run<double>(domain, n, nslots, values, types, nsteps, steps, result, s);
+	case ALPB_INT64: return vec_chain_run<int64_t>(domain, n, nslots, values, types, nsteps, steps, result, s);
+	case ALPB_INT32: return vec_chain_run<int32_t>(domain, n, nslots, values, types, nsteps, steps, result, s);
+	case ALPB_UINT32: return vec_chain_run<uint32_t>(domain, n, nslots, values, types, nsteps, steps, result, s);
+	default: return vec_chain_run<uint64_t>(domain, n, nslots, values, types, nsteps, steps, result, s);
+	}
 }
 
 int alpb_count_assigned(const uint8_t *assigned, int64_t n, int64_t *count, void *stream) {

@@ -448,6 +448,36 @@ ALPB_API int alpb_vec_reduce_dom(void *result, int add_op, uint64_t identity, in
 	uint32_t descr, int domain, int64_t n, const void *x, int x_type,
 	const uint8_t *x_assigned, const void *y, int y_type, const uint8_t *y_assigned,
 	const void *mask, const uint8_t *mask_assigned, int mask_type, int masked, void *stream);
+
+/* Several dense level-1 steps over the same n entries in ONE device pass
+ * (the fusion of chains of grb::set / foldl / foldr / eWiseMul / eWiseMulAdd
+ * calls that the C++ backend records, plus a closing grb::dot or fold to a
+ * scalar).  No counterpart in the reference's C interface: its nonblocking
+ * backend fuses such chains on the CPU (include/graphblas/nonblocking/).
+ * values[s], types[s] (s < nslots <= ALPB_CHAIN_SLOTS): the dense vectors the
+ * steps name by slot number; each is read from memory once (if a step reads
+ * it before any step writes it) and written once (if a step writes it).  The
+ * steps apply alpb_vec_op_dom's dense semantics in order, element by element,
+ * in the given domain; every type must be the domain's own (FP64 for ALPB_FP64,
+ * INT64/UINT64/INT32/UINT32 for theirs), so no value is rounded between steps.
+ * A last step of kind ALPB_VEC_REDUCE folds x (*) y (y = -1: x alone) with op
+ * into *result exactly as alpb_vec_reduce_dom does (same order: bit-identical).
+ * left_assign_if is not accepted (it may leave entries unassigned). */
+#define ALPB_VEC_REDUCE 5
+#define ALPB_CHAIN_SLOTS 8
+#define ALPB_CHAIN_STEPS 16
+typedef struct alpb_vec_step {
+	int32_t kind;      /* ALPB_VEC_SET, _FOLDL, _FOLDR, _MULADD, or ALPB_VEC_REDUCE (last) */
+	int32_t op;        /* the operator (MULADD, REDUCE: the additive one); SET: unused */
+	int32_t mul_op;    /* MULADD and REDUCE with y: the multiplicative operator */
+	uint32_t descr;    /* SET: ALPB_DESC_USE_INDEX writes the index */
+	int32_t z, x, y;   /* slots; x or y = -1: the scalar alpha or beta instead */
+	int32_t reserved;
+	uint64_t alpha, beta;  /* bits of domain values */
+	uint64_t identity;     /* REDUCE: bits of the additive identity */
+} alpb_vec_step;
+ALPB_API int alpb_vec_chain(int domain, int64_t n, int nslots, void *const *values,
+	const int *types, int nsteps, const alpb_vec_step *steps, void *result, void *stream);
 /* number of assigned entries (synchronises). */
 ALPB_API int alpb_count_assigned(const uint8_t *assigned, int64_t n, int64_t *count,
 	void *stream);

@@ -64,14 +64,30 @@ namespace grb {
 				const int mt = masked ? type_code< M >::value : ALPB_VOID;
 				if( zt < 0 || xt < 0 || yt < 0 || mt < 0 ) { return UNSUPPORTED; }
 				if( n == 0 ) { return SUCCESS; }
+				// the operands' domain: integer operators compute exactly on the device
+				constexpr int dom = domain_of< Z, X, Y >::value;
+				// dense, unmasked steps join the pending chain (run at the next flush)
+				const bool y_used = kind == ALPB_VEC_MULADD || kind == ALPB_VEC_APPLY;
+				if( fusion_enabled() && !masked && kind != ALPB_VEC_APPLY && z.b200_dense() &&
+					( !x || x->b200_dense() ) && ( !y_used || !y || y->b200_dense() ) &&
+					op != ALPB_OP_LEFT_ASSIGN_IF &&
+					( kind != ALPB_VEC_MULADD || ( mul_op >= 0 && mul_op != ALPB_OP_LEFT_ASSIGN_IF ) ) &&
+					chain_type_ok( dom, zt ) && ( !x || chain_type_ok( dom, xt ) ) &&
+					( !y_used || !y || chain_type_ok( dom, yt ) )
+				) {
+					z.b200_device_ready();   // host-written pages back (this may flush)
+					if( x ) { x->b200_device_ready(); }
+					if( y_used && y ) { y->b200_device_ready(); }
+					if( record_step( kind, op, kind == ALPB_VEC_MULADD ? mul_op : ALPB_OP_ADD, descr, dom,
+						n, z.b200_values(), zt, x ? x->b200_values() : nullptr, xt, alpha,
+						( y_used && y ) ? y->b200_values() : nullptr, yt, beta ) ) { return SUCCESS; }
+				}
 				z.b200_device_ready();
 				if( x ) { x->b200_device_ready(); }
 				if( y ) { y->b200_device_ready(); }
 				if( masked ) { mask->b200_device_ready(); }
 				// a dense output stays dense unless eWiseApply may drop entries
 				const bool out_sparse = !z.b200_dense() || kind == ALPB_VEC_APPLY;
-				// the operands' domain: integer operators compute exactly on the device
-				constexpr int dom = domain_of< Z, X, Y >::value;
 				const RC rc = check( alpb_vec_op_dom( kind, op, monoid ? 1 : 0,
 					domain_bits( identity, dom ), mul_op, descr, dom, n,
 					z.b200_values(), zt, out_sparse ? z.b200_flags() : nullptr,
@@ -108,12 +124,50 @@ namespace grb {
 				const int mt = masked ? type_code< M >::value : ALPB_VOID;
 				if( xt < 0 || yt < 0 || mt < 0 ) { return UNSUPPORTED; }
 				if( n == 0 ) { return SUCCESS; }
-				x.b200_device_ready();
-				if( y ) { y->b200_device_ready(); }
-				if( masked ) { mask->b200_device_ready(); }
 				// folded on the device in the operands' domain, exactly for integers
 				constexpr int dom = domain_of< OutT, X, Y >::value;
 				uint64_t r = domain_bits( static_cast< scalar_t >( out ), dom );
+				// a dense, unmasked reduction closes a pending chain of its domain in
+				// the same device pass (same grid and order as alpb_vec_reduce_dom)
+				Chain &c = chain();
+				if( c.nsteps > 0 && c.domain == dom && c.n == static_cast< int64_t >( n ) &&
+					!masked && x.b200_dense() && ( !y || y->b200_dense() ) &&
+					mul_op != ALPB_OP_LEFT_ASSIGN_IF && chain_type_ok( dom, xt ) &&
+					( !y || chain_type_ok( dom, yt ) )
+				) {
+					x.b200_device_ready();   // may flush (host-written pages)
+					if( y ) { y->b200_device_ready(); }
+					const int xs = c.nsteps > 0 ? chain_slot( c, x.b200_values(), xt ) : -1;
+					const int ys = ( c.nsteps > 0 && y ) ? chain_slot( c, y->b200_values(), yt ) : -1;
+					if( c.nsteps > 0 && xs >= 0 && ( !y || ys >= 0 ) ) {
+						alpb_vec_step &st = c.step[ c.nsteps ];
+						st.kind = ALPB_VEC_REDUCE;
+						st.op = add_op;
+						st.mul_op = y ? mul_op : ALPB_OP_ADD;
+						st.descr = descr;
+						st.z = 0;
+						st.x = xs;
+						st.y = ys;
+						st.reserved = 0;
+						st.alpha = 0;
+						st.beta = 0;
+						st.identity = domain_bits( identity, dom );
+						const int steps = c.nsteps + 1;
+						c.nsteps = 0;   // the chain is consumed here, whatever the outcome
+						const RC rc = check( alpb_vec_chain( dom, c.n, c.nslots, c.val, c.type, steps,
+							c.step, &r, nullptr ), "reduce (fused)" );
+						++c.runs;
+						c.fused_steps += steps;
+						c.nslots = 0;
+						c.domain = -1;
+						c.n = 0;
+						if( rc == SUCCESS ) { out = from_domain_bits< OutT >( r, dom ); }
+						return rc;
+					}
+				}
+				x.b200_device_ready();
+				if( y ) { y->b200_device_ready(); }
+				if( masked ) { mask->b200_device_ready(); }
 				const RC rc = check( alpb_vec_reduce_dom( &r, add_op, domain_bits( identity, dom ),
 					mul_op, descr, dom, n, x.b200_values(), xt, x.b200_flags_or_dense(),
 					y ? y->b200_values() : nullptr, yt, y ? y->b200_flags_or_dense() : nullptr,

@@ -19,8 +19,16 @@ namespace grb {
 		return internal::b200rt::check( alpb_init( dev ? std::atoi( dev ) : 0 ), "grb::init" );
 	}
 
+	/** Runs pending fused level-1 steps; with ALPB_TRACE set, one line on
+	 *  stderr with the fusion count and the kernels launched. */
 	template<>
 	inline RC finalize< b200 >() {
+		(void) alpb_stream_sync( internal::b200rt::stream() );
+		if( std::getenv( "ALPB_TRACE" ) != nullptr ) {
+			const internal::b200rt::Chain &c = internal::b200rt::chain();
+			std::cerr << "grb::b200: fused level-1 passes " << c.runs << " for " << c.fused_steps
+				<< " steps, kernel launches " << alpb_launch_count() << "\n";
+		}
 		return internal::b200rt::check( alpb_finalize(), "grb::finalize" );
 	}
 

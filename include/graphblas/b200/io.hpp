@@ -147,6 +147,13 @@ namespace grb {
 				}
 				// a 64-bit integer value does not fit a double: it takes the typed path
 				constexpr int dom = domain_of< DataType, T >::value;
+				// a dense vector set to a value joins the pending level-1 chain
+				if( !mask && x.b200_dense() && fusion_enabled() && chain_type_ok( dom, zt ) &&
+					record_step( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, ALPB_OP_ADD, descr, dom, n,
+						x.b200_values(), zt, nullptr, zt, static_cast< scalar_t >( val ), nullptr, zt, 0 )
+				) {
+					return SUCCESS;
+				}
 				if( !mask && !( descr & descriptors::use_index ) &&
 					!( std::is_integral< DataType >::value && sizeof( DataType ) == 8 )
 				) {
@@ -231,6 +238,14 @@ namespace grb {
 		if( zt < 0 || yt < 0 ) { return UNSUPPORTED; }
 		x.b200_device_ready();
 		y.b200_device_ready();
+		// dense to dense: a step of the pending level-1 chain
+		constexpr int dom = domain_of< OutputType, InputType >::value;
+		if( x.b200_dense() && y.b200_dense() && fusion_enabled() && chain_type_ok( dom, zt ) &&
+			chain_type_ok( dom, yt ) && record_step( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN,
+				ALPB_OP_ADD, descr, dom, n, x.b200_values(), zt, y.b200_values(), yt, 0, nullptr, zt, 0 )
+		) {
+			return SUCCESS;
+		}
 		RC rc = clear( x );
 		if( rc != SUCCESS ) { return rc; }
 		rc = check( alpb_vec_op_dom( ALPB_VEC_SET, ALPB_OP_RIGHT_ASSIGN, 0, 0, 0, descr,

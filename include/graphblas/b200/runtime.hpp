@@ -12,6 +12,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <iostream>
 #include <limits>
@@ -31,8 +32,62 @@ namespace grb {
 
 		namespace b200rt {
 
-			/** Stream all primitives are ordered on (NULL: the legacy default stream). */
-			inline void * stream() noexcept { return nullptr; }
+			/**
+			 * Pending chain of dense level-1 steps (alpb_vec_chain): set, foldl,
+			 * foldr, eWiseMul and eWiseMulAdd calls on dense vectors without a mask
+			 * are recorded instead of run, and the chain runs as ONE device pass
+			 * when anything else needs the device or a vector's values -- a dot or
+			 * fold to a scalar closes it inside that pass.  This is the lazy fusion
+			 * of ALP's nonblocking backend (include/graphblas/nonblocking/), done
+			 * on the device; results are those of the steps run one by one, bit
+			 * for bit.  ALPB_FUSE=0 in the environment runs every step at once.
+			 */
+			struct Chain {
+				int domain = -1;
+				int64_t n = 0;
+				int nslots = 0, nsteps = 0;
+				void * val[ ALPB_CHAIN_SLOTS ];
+				int type[ ALPB_CHAIN_SLOTS ];
+				alpb_vec_step step[ ALPB_CHAIN_STEPS ];
+				int enabled = -1;   // -1: ALPB_FUSE not read yet
+				long runs = 0, fused_steps = 0;   // passes run, steps they held
+			};
+			inline Chain & chain() noexcept { static Chain c; return c; }
+
+			inline bool fusion_enabled() noexcept {
+				Chain &c = chain();
+				if( c.enabled < 0 ) {
+					const char * const e = std::getenv( "ALPB_FUSE" );
+					c.enabled = ( e && e[ 0 ] == '0' ) ? 0 : 1;
+				}
+				return c.enabled == 1;
+			}
+
+			/** Runs the pending chain, if any (enqueued on the default stream). */
+			inline void flush() noexcept {
+				Chain &c = chain();
+				if( c.nsteps == 0 ) { return; }
+				const int rc = alpb_vec_chain( c.domain, c.n, c.nslots, c.val, c.type, c.nsteps,
+					c.step, nullptr, nullptr );
+				++c.runs;
+				c.fused_steps += c.nsteps;
+				c.nsteps = 0;
+				c.nslots = 0;
+				c.domain = -1;
+				c.n = 0;
+				if( rc != ALPB_SUCCESS ) {
+#ifndef _GRB_NO_STDIO
+					std::cerr << "grb::b200: fused level-1 chain: " << alpb_last_error() << "\n";
+#endif
+				}
+			}
+
+			/** Stream all primitives are ordered on (NULL: the legacy default
+			 *  stream); asking for it runs the pending chain first. */
+			inline void * stream() noexcept {
+				flush();
+				return nullptr;
+			}
 
 			/** The C-ABI returns grb::RC numbering; map it and keep the message. */
 			inline RC check( const int rc, const char * const where ) {
@@ -267,7 +322,70 @@ namespace grb {
 			}
 
 			inline void release( void * p ) noexcept {
-				if( p ) { (void) alpb_free( p ); }
+				if( p ) {
+					flush();   // the pending chain may name this buffer
+					(void) alpb_free( p );
+				}
+			}
+
+			/** Whether a vector of type code t joins a chain in domain dom (the
+			 *  domain's own type: no value is rounded between fused steps). */
+			inline bool chain_type_ok( const int dom, const int t ) noexcept {
+				return t == dom || ( dom == ALPB_UINT64 && t == ALPB_INT64 ) ||
+					( dom == ALPB_INT64 && t == ALPB_UINT64 );
+			}
+
+			/** Slot of buffer p in the pending chain (added if new); -1 when full. */
+			inline int chain_slot( Chain &c, void * const p, const int t ) noexcept {
+				for( int q = 0; q < c.nslots; ++q ) {
+					if( c.val[ q ] == p ) { return q; }
+				}
+				if( c.nslots == ALPB_CHAIN_SLOTS ) { return -1; }
+				c.val[ c.nslots ] = p;
+				c.type[ c.nslots ] = t;
+				return c.nslots++;
+			}
+
+			/**
+			 * Appends a step on dense vectors (z; x and y, or NULL for the
+			 * scalars alpha and beta) to the pending chain, after running what is
+			 * pending if the domain or length differs or the chain is full.  The
+			 * caller has checked that the step is one alpb_vec_chain accepts and
+			 * that every vector is dense and of the domain's type.
+			 */
+			inline bool record_step( const int kind, const int op, const int mul_op,
+				const uint32_t descr, const int dom, const size_t n, void * const z, const int zt,
+				void * const x, const int xt, const scalar_t alpha, void * const y, const int yt,
+				const scalar_t beta
+			) {
+				Chain &c = chain();
+				if( c.nsteps > 0 && ( c.domain != dom || c.n != static_cast< int64_t >( n ) ||
+					c.nsteps >= ALPB_CHAIN_STEPS - 1 ) ) { flush(); }
+				for( int attempt = 0; attempt < 2; ++attempt ) {
+					const int zs = chain_slot( c, z, zt );
+					const int xs = x ? chain_slot( c, x, xt ) : -1;
+					const int ys = y ? chain_slot( c, y, yt ) : -1;
+					if( zs < 0 || ( x && xs < 0 ) || ( y && ys < 0 ) ) {
+						flush();   // out of slots: run what is pending, then start anew
+						continue;
+					}
+					alpb_vec_step &st = c.step[ c.nsteps++ ];
+					st.kind = kind;
+					st.op = op;
+					st.mul_op = mul_op;
+					st.descr = descr;
+					st.z = zs;
+					st.x = xs;
+					st.y = ys;
+					st.reserved = 0;
+					st.alpha = domain_bits( alpha, dom );
+					st.beta = domain_bits( beta, dom );
+					st.identity = 0;
+					c.domain = dom;
+					c.n = static_cast< int64_t >( n );
+					return true;
+				}
+				return false;
 			}
 
 		} // namespace b200rt

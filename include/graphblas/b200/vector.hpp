@@ -200,10 +200,12 @@ namespace grb {
 			}
 
 			lambda_reference operator[]( const size_t i ) {
+				if( internal::b200rt::chain().nsteps ) { b200_host_ready(); }  // fused steps pending
 				_host_touched = true;
 				return reinterpret_cast< D * >( _val )[ i ];
 			}
 			lambda_reference operator[]( const size_t i ) const {
+				if( internal::b200rt::chain().nsteps ) { b200_host_ready(); }
 				_host_touched = true;
 				return reinterpret_cast< D * >( _val )[ i ];
 			}
