@@ -314,8 +314,7 @@ __global__ void __launch_bounds__(256) k_pr_fix(PrStepArgs a, int parity) {
 		const int64_t t = base + lane;
 		const int32_t n = t < mt.ntiles ? mt.span_len[t] : 0;
 		if (n > 0 && n <= 32) {
-			double v = 0.0;
-			for (int64_t k = t; k < t + n - 1; ++k) v += load_bits<double>(mt.tail_val + k);
+			double v = wm_sum_slots<RF>(0.0, mt.tail_val, t, t + n - 1);
 			v += load_bits<double>(mt.head_val + t + n - 1);
 			epi.row(mt.tile_row[t + 1], v, true);
 		}

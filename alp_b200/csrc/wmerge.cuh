@@ -328,6 +328,25 @@ __device__ __forceinline__ bool warp_tile_ordered(int64_t t, const WmMeta &g,
 	return true;
 }
 
+// v (+)= slots[k] for k = k0, k0+1, ..., k1-1, in that order, eight loads in
+// flight (a row spanning many tiles then costs a few round trips, not one
+// per tile).
+template <class R>
+__device__ __forceinline__ typename R::T wm_sum_slots(typename R::T v, const uint64_t *slots,
+	int64_t k0, int64_t k1) {
+	using T = typename R::T;
+	int64_t k = k0;
+	for (; k + 8 <= k1; k += 8) {
+		T b[8];
+#pragma unroll
+		for (int u = 0; u < 8; ++u) b[u] = wm_load_slot<T>(slots + k + u);
+#pragma unroll
+		for (int u = 0; u < 8; ++u) v = R::add(v, b[u]);
+	}
+	for (; k < k1; ++k) v = R::add(v, wm_load_slot<T>(slots + k));
+	return v;
+}
+
 // Second pass: every row that crosses tiles, y_r = y_r (+) its slots summed
 // in tile order (tail slots of its first..last-1 tiles, head slot of its last
 // tile).  One lane per first tile for spans up to 32 tiles; the whole warp
@@ -342,8 +361,7 @@ __global__ void __launch_bounds__(256) k_wm_fixup(MergeTables mt, Epi epi) {
 		const int64_t t = base + lane;
 		const int32_t n = t < mt.ntiles ? mt.span_len[t] : 0;
 		if (n > 0 && n <= 32) {
-			T v = R::zero();
-			for (int64_t k = t; k < t + n - 1; ++k) v = R::add(v, wm_load_slot<T>(mt.tail_val + k));
+			T v = wm_sum_slots<R>(R::zero(), mt.tail_val, t, t + n - 1);
 			v = R::add(v, wm_load_slot<T>(mt.head_val + t + n - 1));
 			epi.row(mt.tile_row[t + 1], v, true);
 		}
