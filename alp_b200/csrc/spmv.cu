@@ -331,7 +331,8 @@ k_spmv_wmerge_hot(MergeTables mt, const int64_t *__restrict__ offsets,
 	WmMeta g = wm_meta(mt, t);
 	while (t < mt.ntiles) {
 		const WmMeta next = wm_meta(mt, t + nw);
-		warp_tile<R>(t, g, mt, offsets, hot_idx, values, xl, epi, left, mine);
+		warp_tile<R, HotX<T>, HotAccumulateY<R>, WarpSmemCompact<R>, false>(t, g, mt, offsets,
+			hot_idx, values, xl, epi, left, mine);
 		t += nw;
 		g = next;
 	}

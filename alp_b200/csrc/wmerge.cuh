@@ -89,7 +89,13 @@ __device__ __forceinline__ T wm_load_slot(const uint64_t *p) {
 // end in the tile (its shared-memory writes are visible to epi.row).  Leaves in every lane:
 // head_v/head_h (the partial of row i0 up to its end, in the lane whose first
 // finished row is row 0) and sv/sh (lane 31: the partial of the tail row).
-template <class R, class XL, class Epi, class SM>
+//
+// kLoadsFirst issues the tile's loads (the offsets of its first 64 rows, its
+// column indices and values, then epi.begin_tile's) before any shared-memory
+// store, so that their round trips overlap; it holds 4 more registers while
+// they are in flight, which a kernel at the 64-register limit cannot spare
+// (the hot-column SpMV turns it off).
+template <class R, class XL, class Epi, class SM, bool kLoadsFirst = true>
 __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
 	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
@@ -110,6 +116,52 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 	const int64_t j0 = d0 - i0, j1 = d1 - i1;
 	const int nrows = int(i1 - i0);
 	const int nnzt = int(j1 - j0);
+	if constexpr (kLoadsFirst) {
+		int64_t ro[2];
+#pragma unroll
+		for (int h = 0; h < 2; ++h) {
+			const int k = lane + 32 * h;
+			const int64_t r = i0 + k;
+			ro[h] = k <= nrows + 1 && r <= m ? offsets[r] : j1 + 1;
+		}
+		uint32_t col[WM_IPT];
+		T a[WM_IPT];
+#pragma unroll
+		for (int u = 0; u < WM_IPT; ++u) {
+			const int k = lane + 32 * u;
+			if (k < nnzt) {
+				col[u] = __ldcs(indices + j0 + k);
+				a[u] = values ? __ldcs(values + j0 + k) : R::one();
+			}
+		}
+		epi.begin_tile(i0, nrows, lane);
+		// row ends, relative to j0, clamped as below
+#pragma unroll
+		for (int h = 0; h < 2; ++h) {
+			const int k = lane + 32 * h;
+			if (k <= nrows + 1) {
+				int64_t v = ro[h] - j0;
+				if (v > WM_TILE + 1) v = WM_TILE + 1;
+				if (v < -1) v = -1;
+				sm.row_end[k] = static_cast<typename SM::End>(v);
+			}
+		}
+		for (int k = lane + 64; k <= nrows + 1; k += 32) {
+			const int64_t r = i0 + k;
+			int64_t v = (r <= m ? offsets[r] : j1 + 1) - j0;
+			if (v > WM_TILE + 1) v = WM_TILE + 1;
+			if (v < -1) v = -1;
+			sm.row_end[k] = static_cast<typename SM::End>(v);
+		}
+#pragma unroll
+		for (int u = 0; u < WM_IPT; ++u) {
+			const int k = lane + 32 * u;
+			if (k < nnzt) {
+				const T xv = xl(col[u]);
+				sm.prod[wm_pad(k)] = left ? R::mull(xv, a[u]) : R::mulr(a[u], xv);
+			}
+		}
+	} else {
 	epi.begin_tile(i0, nrows, lane);
 
 	// row ends, relative to j0; clamped to the tile (the walk compares them
@@ -144,6 +196,7 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 				sm.prod[wm_pad(k)] = left ? R::mull(xv, a[u]) : R::mulr(a[u], xv);
 			}
 		}
+	}
 	}
 	__syncwarp();
 
@@ -243,7 +296,7 @@ __device__ __forceinline__ WmMeta wm_meta(const MergeTables &mt, int64_t t) {
 // head_val[t] (the row ends here) or tail_val[t] (it continues), and
 // k_wm_fixup finishes it.  A spanning row always holds nonzeroes, so its
 // partials need no presence flag: an empty partial is the additive identity.
-template <class R, class XL, class Epi, class SM>
+template <class R, class XL, class Epi, class SM, bool kLoadsFirst = true>
 __device__ __forceinline__ void warp_tile(int64_t t, const WmMeta &g, const MergeTables &mt,
 	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
 	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
@@ -253,8 +306,8 @@ __device__ __forceinline__ void warp_tile(int64_t t, const WmMeta &g, const Merg
 	int first_row;
 	T head_v, sv;
 	bool head_h, sh;
-	wm_core<R>(t, mt, offsets, indices, values, xl, epi, left, sm, g.i0, g.i1, g.hf, first_row,
-		head_v, head_h, sv, sh);
+	wm_core<R, XL, Epi, SM, kLoadsFirst>(t, mt, offsets, indices, values, xl, epi, left, sm, g.i0,
+		g.i1, g.hf, first_row, head_v, head_h, sv, sh);
 	if (g.hf >= 0 && first_row == 0) store_bits<T>(mt.head_val + t, head_v);
 	if (g.tf >= 0 && lane == 31) store_bits<T>(mt.tail_val + t, sv);
 }
@@ -283,7 +336,7 @@ constexpr long long kWmSpinLimit = 1ll << 23;
 // a cycle.  Epi: begin_tile and row(r, sum, has), from any lane.  Returns
 // false if a wait gave up or *err was set elsewhere (a timeout sets *err = 1;
 // the caller leaves at its next grid barrier, which checks the same flag).
-template <class R, class XL, class Epi>
+template <class R, class XL, class Epi, bool kLoadsFirst = true>
 __device__ __forceinline__ bool warp_tile_ordered(int64_t t, const WmMeta &g,
 	const MergeTables &mt, const int64_t *__restrict__ offsets,
 	const uint32_t *__restrict__ indices, const typename R::T *__restrict__ values,
@@ -293,8 +346,8 @@ __device__ __forceinline__ bool warp_tile_ordered(int64_t t, const WmMeta &g,
 	int first_row;
 	T head_v, sv;
 	bool head_h, sh;
-	wm_core<R>(t, mt, offsets, indices, values, xl, epi, left, sm, g.i0, g.i1, g.hf, first_row,
-		head_v, head_h, sv, sh);
+	wm_core<R, XL, Epi, WarpSmem<R>, kLoadsFirst>(t, mt, offsets, indices, values, xl, epi, left,
+		sm, g.i0, g.i1, g.hf, first_row, head_v, head_h, sv, sh);
 	if (g.tf >= 0 && lane == 31) {
 		store_bits<T>(mt.tail_val + t, sv);
 		wm_st_release(mt.ready + t, epoch);  // orders the store above before the flag
