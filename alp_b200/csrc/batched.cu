@@ -517,7 +517,7 @@ k_batched_cg(BcgArgs a) {
 		for (int64_t t = gw; t < nt; t += nw) {
 			BcgPrelude epi{&a, &sm[w]};
 			const WmMeta g = wm_meta(a.mt, t);
-			if (!warp_tile_ordered<RF, PlainX<double>, BcgPrelude, false>(t, g, a.mt, a.offsets,
+			if (!warp_tile_ordered<RF, PlainX<double>, BcgPrelude, 0>(t, g, a.mt, a.offsets,
 					a.indices, a.values, xl, epi, 0, sm[w].tile, epoch, err))
 				break;
 			const double s1 = warp_sum(epi.acc_rr), s2 = warp_sum(epi.acc_bb);
@@ -579,7 +579,7 @@ k_batched_cg(BcgArgs a) {
 				} else {
 					BcgIter epi{&a, &sm[w], u_old, u_new, gamma};
 					BcgGather xl{a.r, u_old, gamma};
-					if (!warp_tile_ordered<RF, BcgGather, BcgIter, false>(t, g, a.mt, a.offsets,
+					if (!warp_tile_ordered<RF, BcgGather, BcgIter, 0>(t, g, a.mt, a.offsets,
 							a.indices, a.values, xl, epi, 0, sm[w].tile, epoch, err))
 						break;
 					part = warp_sum(epi.acc);
@@ -602,7 +602,7 @@ k_batched_cg(BcgArgs a) {
 				if (!cur.done) {
 					BcgIter epi{&a, &sm[w], u_old, u_new, cur.scalar};
 					BcgGather xl{a.r, u_old, cur.scalar};
-					if (!warp_tile_ordered<RF, BcgGather, BcgIter, false>(t, g, a.mt, a.offsets,
+					if (!warp_tile_ordered<RF, BcgGather, BcgIter, 0>(t, g, a.mt, a.offsets,
 							a.indices, a.values, xl, epi, 0, sm[w].tile, epoch, err))
 						break;
 					const double part = warp_sum(epi.acc);

@@ -230,7 +230,8 @@ k_spmv_wmerge(MergeTables mt, const int64_t *__restrict__ offsets,
 	WmMeta g = wm_meta(mt, t);
 	while (t < mt.ntiles) {
 		const WmMeta next = wm_meta(mt, t + nw);
-		warp_tile<R>(t, g, mt, offsets, indices, values, xl, epi, left, sm[w]);
+		warp_tile<R, XL, WarpAccumulateY<R>, WarpSmem<R>, WM_LOADS_FIRST | WM_WALK_AHEAD>(t, g, mt,
+			offsets, indices, values, xl, epi, left, sm[w]);
 		t += nw;
 		g = next;
 	}
@@ -331,7 +332,7 @@ k_spmv_wmerge_hot(MergeTables mt, const int64_t *__restrict__ offsets,
 	WmMeta g = wm_meta(mt, t);
 	while (t < mt.ntiles) {
 		const WmMeta next = wm_meta(mt, t + nw);
-		warp_tile<R, HotX<T>, HotAccumulateY<R>, WarpSmemCompact<R>, false>(t, g, mt, offsets,
+		warp_tile<R, HotX<T>, HotAccumulateY<R>, WarpSmemCompact<R>, WM_WALK_AHEAD>(t, g, mt, offsets,
 			hot_idx, values, xl, epi, left, mine);
 		t += nw;
 		g = next;

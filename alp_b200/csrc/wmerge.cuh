@@ -34,6 +34,10 @@ constexpr unsigned WM_FULL = 0xffffffffu;
 // (lane L) and the walk reads k ~ 8L + c; XOR-ing the low four bits with bits
 // 3..6 makes both patterns hit sixteen distinct 8-byte bank pairs per
 // half-warp (a bijection of k within each aligned block of 128 entries).
+// wm_core options
+constexpr int WM_LOADS_FIRST = 1;
+constexpr int WM_WALK_AHEAD = 2;
+
 __device__ __forceinline__ int wm_pad(int k) { return k ^ ((k >> 3) & 15); }
 
 template <class R>
@@ -90,12 +94,15 @@ __device__ __forceinline__ T wm_load_slot(const uint64_t *p) {
 // head_v/head_h (the partial of row i0 up to its end, in the lane whose first
 // finished row is row 0) and sv/sh (lane 31: the partial of the tail row).
 //
-// kLoadsFirst issues the tile's loads (the offsets of its first 64 rows, its
-// column indices and values, then epi.begin_tile's) before any shared-memory
-// store, so that their round trips overlap; it holds 4 more registers while
-// they are in flight, which a kernel at the 64-register limit cannot spare
-// (the hot-column SpMV turns it off).
-template <class R, class XL, class Epi, class SM, bool kLoadsFirst = true>
+// Opts (WM_LOADS_FIRST | WM_WALK_AHEAD):
+// WM_LOADS_FIRST issues the tile's loads (the offsets of its first 64 rows,
+// its column indices and values, then epi.begin_tile's) before any
+// shared-memory store, so that their round trips overlap; it holds 4 more
+// registers while they are in flight, which a kernel at the 64-register
+// limit cannot spare (the hot-column SpMV leaves it out).
+// WM_WALK_AHEAD reads the walk's next product and next row end one step
+// ahead (measured: the SpMV kernels gain 1-2 %, PageRank's loses 2 %).
+template <class R, class XL, class Epi, class SM, int Opts = WM_LOADS_FIRST>
 __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
 	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
@@ -116,7 +123,7 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 	const int64_t j0 = d0 - i0, j1 = d1 - i1;
 	const int nrows = int(i1 - i0);
 	const int nnzt = int(j1 - j0);
-	if constexpr (kLoadsFirst) {
+	if constexpr ((Opts & WM_LOADS_FIRST) != 0) {
 		int64_t ro[2];
 #pragma unroll
 		for (int h = 0; h < 2; ++h) {
@@ -162,41 +169,41 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 			}
 		}
 	} else {
-	epi.begin_tile(i0, nrows, lane);
+		epi.begin_tile(i0, nrows, lane);
 
-	// row ends, relative to j0; clamped to the tile (the walk compares them
-	// with positions <= nnzt only)
-	for (int k = lane; k <= nrows + 1; k += 32) {
-		int64_t v;
-		if (k == 0) v = offsets[i0] - j0;
-		else {
-			const int64_t r = i0 + k;
-			v = (r <= m ? offsets[r] : j1 + 1) - j0;
+		// row ends, relative to j0; clamped to the tile (the walk compares them
+		// with positions <= nnzt only)
+		for (int k = lane; k <= nrows + 1; k += 32) {
+			int64_t v;
+			if (k == 0) v = offsets[i0] - j0;
+			else {
+				const int64_t r = i0 + k;
+				v = (r <= m ? offsets[r] : j1 + 1) - j0;
+			}
+			if (v > WM_TILE + 1) v = WM_TILE + 1;
+			if (v < -1) v = -1;
+			sm.row_end[k] = static_cast<typename SM::End>(v);
 		}
-		if (v > WM_TILE + 1) v = WM_TILE + 1;
-		if (v < -1) v = -1;
-		sm.row_end[k] = static_cast<typename SM::End>(v);
-	}
-	{
-		uint32_t col[WM_IPT];
-		T a[WM_IPT];
+		{
+			uint32_t col[WM_IPT];
+			T a[WM_IPT];
 #pragma unroll
-		for (int u = 0; u < WM_IPT; ++u) {
-			const int k = lane + 32 * u;
-			if (k < nnzt) {
-				col[u] = __ldcs(indices + j0 + k);
-				a[u] = values ? __ldcs(values + j0 + k) : R::one();
+			for (int u = 0; u < WM_IPT; ++u) {
+				const int k = lane + 32 * u;
+				if (k < nnzt) {
+					col[u] = __ldcs(indices + j0 + k);
+					a[u] = values ? __ldcs(values + j0 + k) : R::one();
+				}
+			}
+#pragma unroll
+			for (int u = 0; u < WM_IPT; ++u) {
+				const int k = lane + 32 * u;
+				if (k < nnzt) {
+					const T xv = xl(col[u]);
+					sm.prod[wm_pad(k)] = left ? R::mull(xv, a[u]) : R::mulr(a[u], xv);
+				}
 			}
 		}
-#pragma unroll
-		for (int u = 0; u < WM_IPT; ++u) {
-			const int k = lane + 32 * u;
-			if (k < nnzt) {
-				const T xv = xl(col[u]);
-				sm.prod[wm_pad(k)] = left ? R::mull(xv, a[u]) : R::mulr(a[u], xv);
-			}
-		}
-	}
 	}
 	__syncwarp();
 
@@ -223,23 +230,56 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 	T first_val = R::zero();
 	bool first_has = false;
 	int re = sm.row_end[ti + 1];  // end of the row being walked
-	for (int d = dl; d < dend; ++d) {
-		if (tj < re) {
-			acc = R::add(acc, sm.prod[wm_pad(tj)]);
-			has = true;
-			++tj;
-		} else {
-			if (first_row < 0) {
-				first_row = ti;
-				first_val = acc;
-				first_has = has;
-			} else {
-				epi.row(i0 + ti, acc, has);
+	if constexpr ((Opts & WM_WALK_AHEAD) != 0) {
+		// the next product and the next row end are read one step ahead, so no
+		// step waits on a shared-memory load issued by the step before (the reads
+		// past the tile's last product or row are clamped into the arrays and
+		// their values never used)
+		int re2 = sm.row_end[ti + 2 <= nrows + 1 ? ti + 2 : nrows + 1];
+		T pv = sm.prod[wm_pad(tj < WM_TILE ? tj : WM_TILE - 1)];
+#pragma unroll
+		for (int s = 0; s < WM_IPT; ++s) {
+			if (dl + s < dend) {
+				if (tj < re) {
+					acc = R::add(acc, pv);
+					has = true;
+					++tj;
+					pv = sm.prod[wm_pad(tj < WM_TILE ? tj : WM_TILE - 1)];
+				} else {
+					if (first_row < 0) {
+						first_row = ti;
+						first_val = acc;
+						first_has = has;
+					} else {
+						epi.row(i0 + ti, acc, has);
+					}
+					acc = R::zero();
+					has = false;
+					++ti;
+					re = re2;
+					re2 = sm.row_end[ti + 2 <= nrows + 1 ? ti + 2 : nrows + 1];
+				}
 			}
-			acc = R::zero();
-			has = false;
-			++ti;
-			re = sm.row_end[ti + 1];
+		}
+	} else {
+		for (int d = dl; d < dend; ++d) {
+			if (tj < re) {
+				acc = R::add(acc, sm.prod[wm_pad(tj)]);
+				has = true;
+				++tj;
+			} else {
+				if (first_row < 0) {
+					first_row = ti;
+					first_val = acc;
+					first_has = has;
+				} else {
+					epi.row(i0 + ti, acc, has);
+				}
+				acc = R::zero();
+				has = false;
+				++ti;
+				re = sm.row_end[ti + 1];
+			}
 		}
 	}
 
@@ -296,7 +336,7 @@ __device__ __forceinline__ WmMeta wm_meta(const MergeTables &mt, int64_t t) {
 // head_val[t] (the row ends here) or tail_val[t] (it continues), and
 // k_wm_fixup finishes it.  A spanning row always holds nonzeroes, so its
 // partials need no presence flag: an empty partial is the additive identity.
-template <class R, class XL, class Epi, class SM, bool kLoadsFirst = true>
+template <class R, class XL, class Epi, class SM, int Opts = WM_LOADS_FIRST>
 __device__ __forceinline__ void warp_tile(int64_t t, const WmMeta &g, const MergeTables &mt,
 	const int64_t *__restrict__ offsets, const uint32_t *__restrict__ indices,
 	const typename R::T *__restrict__ values, const XL &xl, Epi &epi, int left,
@@ -306,7 +346,7 @@ __device__ __forceinline__ void warp_tile(int64_t t, const WmMeta &g, const Merg
 	int first_row;
 	T head_v, sv;
 	bool head_h, sh;
-	wm_core<R, XL, Epi, SM, kLoadsFirst>(t, mt, offsets, indices, values, xl, epi, left, sm, g.i0,
+	wm_core<R, XL, Epi, SM, Opts>(t, mt, offsets, indices, values, xl, epi, left, sm, g.i0,
 		g.i1, g.hf, first_row, head_v, head_h, sv, sh);
 	if (g.hf >= 0 && first_row == 0) store_bits<T>(mt.head_val + t, head_v);
 	if (g.tf >= 0 && lane == 31) store_bits<T>(mt.tail_val + t, sv);
@@ -336,7 +376,7 @@ constexpr long long kWmSpinLimit = 1ll << 23;
 // a cycle.  Epi: begin_tile and row(r, sum, has), from any lane.  Returns
 // false if a wait gave up or *err was set elsewhere (a timeout sets *err = 1;
 // the caller leaves at its next grid barrier, which checks the same flag).
-template <class R, class XL, class Epi, bool kLoadsFirst = true>
+template <class R, class XL, class Epi, int Opts = WM_LOADS_FIRST>
 __device__ __forceinline__ bool warp_tile_ordered(int64_t t, const WmMeta &g,
 	const MergeTables &mt, const int64_t *__restrict__ offsets,
 	const uint32_t *__restrict__ indices, const typename R::T *__restrict__ values,
@@ -346,7 +386,7 @@ __device__ __forceinline__ bool warp_tile_ordered(int64_t t, const WmMeta &g,
 	int first_row;
 	T head_v, sv;
 	bool head_h, sh;
-	wm_core<R, XL, Epi, WarpSmem<R>, kLoadsFirst>(t, mt, offsets, indices, values, xl, epi, left,
+	wm_core<R, XL, Epi, WarpSmem<R>, Opts>(t, mt, offsets, indices, values, xl, epi, left,
 		sm, g.i0, g.i1, g.hf, first_row, head_v, head_h, sv, sh);
 	if (g.tf >= 0 && lane == 31) {
 		store_bits<T>(mt.tail_val + t, sv);
