@@ -285,17 +285,19 @@ __device__ __forceinline__ void wm_core(int64_t t, const MergeTables &mt,
 
 	// segmented inclusive scan of the carries, keyed by the row each lane
 	// stops in (rows are non-decreasing over lanes)
+	// (rows are non-decreasing over lanes, so the lanes that stop in this
+	// lane's row are the run [seg0, lane]: one match replaces a shuffle of
+	// the row per step, and the presence flags are OR-ed from one ballot)
 	sv = acc;
-	sh = has;
+	const int seg0 = __ffs(__match_any_sync(WM_FULL, ti)) - 1;
 #pragma unroll
 	for (int off = 1; off < 32; off <<= 1) {
 		const T v = wm_shfl_up(sv, off);
-		const bool h = wm_shfl_up(sh, off);
-		const int r = __shfl_up_sync(WM_FULL, ti, off);
-		if (lane >= off && r == ti) {
-			sv = R::add(v, sv);
-			sh = sh || h;
-		}
+		if (lane - off >= seg0) sv = R::add(v, sv);
+	}
+	{
+		const unsigned upto = lane == 31 ? 0xffffffffu : (1u << (lane + 1)) - 1u;
+		sh = (__ballot_sync(WM_FULL, has) & upto & ~((1u << seg0) - 1u)) != 0;
 	}
 	// carry into this lane: the scan of lane-1, whose stop row is this lane's
 	// start row
