@@ -324,8 +324,7 @@ __global__ void __launch_bounds__(256) k_pr_fix(PrStepArgs a, int parity) {
 			long_rows &= long_rows - 1;
 			const int64_t f = base + src;
 			const int32_t nn = __shfl_sync(0xffffffffu, n, src);
-			double v = 0.0;
-			for (int64_t k = f + lane; k < f + nn - 1; k += 32) v += load_bits<double>(mt.tail_val + k);
+			double v = wm_sum_slots32<RF>(0.0, mt.tail_val, f + lane, f + nn - 1);
 			for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
 			if (lane == 0) {
 				v += load_bits<double>(mt.head_val + f + nn - 1);
@@ -344,14 +343,51 @@ __global__ void __launch_bounds__(256) k_pr_fix(PrStepArgs a, int parity) {
 // residual and dangling mass in a fixed order; the next teleport term; stop
 // after an iteration whose residual is <= conv (:490) or at max_iter.
 // setup != 0: only the first term (no iteration has run).
+// The four sums of k_pr_finish in one pass: a thread's loads of all four
+// arrays are in flight together, and each sum keeps block_sum_array's order
+// (the thread's elements in stride order, then block_sum's tree), so the
+// values are those of four block_sum_array calls bit for bit.
+__device__ __forceinline__ void pr_finish_sums(const PrStepArgs &a, int setup,
+	double (*smem)[33], double out[4]) {
+	double v[4] = {0.0, 0.0, 0.0, 0.0};
+	for (int64_t k = threadIdx.x; k < a.grid; k += blockDim.x) {
+		v[0] += a.blk[k];
+		v[1] += a.blk[a.grid + k];
+	}
+	if (!setup)
+		for (int64_t k = threadIdx.x; k < a.fix_grid; k += blockDim.x) {
+			v[2] += a.fix[k];
+			v[3] += a.fix[a.fix_grid + k];
+		}
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+	for (int q = 0; q < 4; ++q)
+		for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+	if (lane == 0)
+		for (int q = 0; q < 4; ++q) smem[q][wid] = v[q];
+	__syncthreads();
+	if (wid == 0) {
+		const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+		for (int q = 0; q < 4; ++q) {
+			double w = lane < nw ? smem[q][lane] : 0.0;
+			for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+			if (lane == 0) smem[q][32] = w;
+		}
+	}
+	__syncthreads();
+	for (int q = 0; q < 4; ++q) out[q] = smem[q][32];
+}
+
 __global__ void __launch_bounds__(256) k_pr_finish(PrStepArgs a, int setup) {
-	__shared__ double red[33];
+	__shared__ double red[4][33];
 	PrStepState *st = a.st;
 	if (st->done) return;
-	const double r1 = block_sum_array(a.blk, a.grid, red);
-	const double d1 = block_sum_array(a.blk + a.grid, a.grid, red);
-	const double r2 = setup ? 0.0 : block_sum_array(a.fix, a.fix_grid, red);
-	const double d2 = setup ? 0.0 : block_sum_array(a.fix + a.fix_grid, a.fix_grid, red);
+	double sums[4];
+	pr_finish_sums(a, setup, red, sums);
+	const double r1 = sums[0], d1 = sums[1];
+	const double r2 = setup ? 0.0 : sums[2];
+	const double d2 = setup ? 0.0 : sums[3];
 	if (threadIdx.x == 0) {
 		const double dang = d1 + d2;
 		st->d = (a.alpha * dang + 1 - a.alpha) / double(a.n);     // (:390)

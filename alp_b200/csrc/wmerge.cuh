@@ -30,14 +30,14 @@ constexpr int WM_IPT = ALPB_WM_IPT;    // merge items per lane
 constexpr int WM_TILE = 32 * WM_IPT;   // merge items per warp tile
 constexpr unsigned WM_FULL = 0xffffffffu;
 
-// Position of product k in shared memory.  The staging writes k = 32u + L
-// (lane L) and the walk reads k ~ 8L + c; XOR-ing the low four bits with bits
-// 3..6 makes both patterns hit sixteen distinct 8-byte bank pairs per
-// half-warp (a bijection of k within each aligned block of 128 entries).
 // wm_core options
 constexpr int WM_LOADS_FIRST = 1;
 constexpr int WM_WALK_AHEAD = 2;
 
+// Position of product k in shared memory.  The staging writes k = 32u + L
+// (lane L) and the walk reads k ~ 8L + c; XOR-ing the low four bits with bits
+// 3..6 makes both patterns hit sixteen distinct 8-byte bank pairs per
+// half-warp (a bijection of k within each aligned block of 128 entries).
 __device__ __forceinline__ int wm_pad(int k) { return k ^ ((k >> 3) & 15); }
 
 template <class R>
@@ -442,6 +442,24 @@ __device__ __forceinline__ typename R::T wm_sum_slots(typename R::T v, const uin
 	return v;
 }
 
+// v (+)= slots[k] for k = k0, k0 + 32, k0 + 64, ... < k1, in that order,
+// eight loads in flight (one lane's share of a row spanning many tiles).
+template <class R>
+__device__ __forceinline__ typename R::T wm_sum_slots32(typename R::T v, const uint64_t *slots,
+	int64_t k0, int64_t k1) {
+	using T = typename R::T;
+	int64_t k = k0;
+	for (; k + 7 * 32 < k1; k += 8 * 32) {
+		T b[8];
+#pragma unroll
+		for (int u = 0; u < 8; ++u) b[u] = wm_load_slot<T>(slots + k + 32 * u);
+#pragma unroll
+		for (int u = 0; u < 8; ++u) v = R::add(v, b[u]);
+	}
+	for (; k < k1; k += 32) v = R::add(v, wm_load_slot<T>(slots + k));
+	return v;
+}
+
 // Second pass: every row that crosses tiles, y_r = y_r (+) its slots summed
 // in tile order (tail slots of its first..last-1 tiles, head slot of its last
 // tile).  One lane per first tile for spans up to 32 tiles; the whole warp
@@ -466,9 +484,7 @@ __global__ void __launch_bounds__(256) k_wm_fixup(MergeTables mt, Epi epi) {
 			long_rows &= long_rows - 1;
 			const int64_t f = base + src;
 			const int32_t nn = __shfl_sync(WM_FULL, n, src);
-			T v = R::zero();
-			for (int64_t k = f + lane; k < f + nn - 1; k += 32)
-				v = R::add(v, wm_load_slot<T>(mt.tail_val + k));
+			T v = wm_sum_slots32<R>(R::zero(), mt.tail_val, f + lane, f + nn - 1);
 #pragma unroll
 			for (int o = 16; o > 0; o >>= 1) {
 				const T vo = wm_shfl_xor(v, o);
